@@ -1,0 +1,117 @@
+/*
+ * pssgpu.h -- C ABI of the B200 string sample sort (libpssgpu.so).
+ *
+ * The library sorts NUL-terminated byte strings on one NVIDIA B200 and
+ * optionally emits the LCP array. Its results equal those of the reference
+ * pS5 (bingmann/parallel-string-sorting, "pS5-Unroll",
+ * src/parallel/bingmann-parallel_sample_sort.cpp:31-42): the same sorted
+ * string sequence and the same LCP array; only the order of pointers to
+ * equal strings may differ.
+ *
+ * String model (the reference's UCharStringSet, src/tools/stringset.hpp):
+ * a string is the bytes from its start up to its first NUL; comparison is
+ * unsigned bytewise (strcmp). LCP convention (src/tools/stringptr.hpp:
+ * 977-1046): lcp[i] = number of chars shared by sorted strings i-1 and i,
+ * for i >= 1; lcp[0] is never written.
+ *
+ * All entry points are thread-safe. Errors are returned as a status code;
+ * pssgpu_last_error() gives the message of the calling thread's last error.
+ * The drop-in pointer-array entry points (the psstest contestant signatures)
+ * have no error channel in the reference, so they abort() with the message on
+ * stderr, which psstest --fork reports as status=aborted
+ * (src/psstest.cpp:341-369).
+ */
+#ifndef PSSGPU_H
+#define PSSGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define PSSGPU_OK 0
+#define PSSGPU_EINVAL 1   /* bad argument: sizes, alignment, unterminated arena */
+#define PSSGPU_ENOMEM 2   /* device or host allocation failed */
+#define PSSGPU_ECUDA 3    /* a CUDA runtime call failed */
+#define PSSGPU_ETIMEOUT 4 /* a bounded device-side wait gave up */
+#define PSSGPU_ENODEV 5   /* no usable CUDA device */
+#define PSSGPU_EBUDGET 6  /* request exceeds the configured memory budget */
+
+/* Device arenas must stay readable this many bytes past their last char. */
+#define PSSGPU_ARENA_PAD 16
+
+/* Largest string count one call accepts (ids are 32-bit). */
+#define PSSGPU_MAX_STRINGS 0xFFFFFFF0u
+
+const char* pssgpu_last_error(void);
+const char* pssgpu_version(void);
+
+/* ---- contexts ------------------------------------------------------------
+ * A context owns a CUDA stream and a device workspace that grows to the
+ * largest sort seen and is reused. Calls on one context are serialised by
+ * its mutex; separate contexts run concurrently. */
+typedef struct pssgpu_ctx pssgpu_ctx;
+
+int pssgpu_ctx_create(int device, pssgpu_ctx** out);
+void pssgpu_ctx_destroy(pssgpu_ctx* ctx);
+/* Bytes of device workspace a sort of n strings needs (excluding inputs and
+ * outputs). */
+uint64_t pssgpu_workspace_bytes(uint64_t n);
+
+/* Statistics of the last sort on a context (all counts, device ms). */
+typedef struct pssgpu_stats {
+    uint32_t passes;          /* big-segment sample-sort passes */
+    uint32_t kernel_launches; /* kernels launched by the last sort */
+    uint64_t big_elements;    /* sum over passes of strings in big segments */
+    uint64_t small_segments;  /* segments finished by the small-sort kernel */
+    uint64_t boundaries;      /* split boundaries whose LCP was set at the end */
+    float device_ms;          /* device time of the last sort (events) */
+} pssgpu_stats;
+int pssgpu_ctx_stats(pssgpu_ctx* ctx, pssgpu_stats* out);
+
+/* ---- arena sorts ---------------------------------------------------------
+ * chars[0, nchars) holds the strings; string i starts at chars + offs[i] and
+ * ends at its first NUL, which must lie inside the arena (chars[nchars-1]
+ * must be 0). Outputs: perm[r] = id of the r-th smallest string; lcp (may be
+ * NULL) as in the LCP convention above (lcp[0] untouched).
+ *
+ * pssgpu_sort_host: host buffers; the call copies the arena and offsets to
+ * the device, sorts, and copies perm/lcp back. Replaces the body of a
+ * psstest contestant run (src/psstest.cpp:387-403) for an arena input.
+ *
+ * pssgpu_sort_device: device buffers on the context's device. d_chars must
+ * be 8-byte aligned and readable for nchars + PSSGPU_ARENA_PAD bytes;
+ * `stream` is a cudaStream_t or NULL for the context's stream. The call
+ * returns after the sort has completed. */
+int pssgpu_sort_host(pssgpu_ctx* ctx, const uint8_t* chars, uint64_t nchars,
+                     const uint64_t* offs, uint64_t n, uint32_t* perm,
+                     uint32_t* lcp);
+int pssgpu_sort_device(pssgpu_ctx* ctx, const uint8_t* d_chars,
+                       uint64_t nchars, const uint64_t* d_offs, uint64_t n,
+                       uint32_t* d_perm, uint32_t* d_lcp, void* stream);
+
+/* ---- psstest Contest drop-ins --------------------------------------------
+ * The three contestant signatures of Contestant_UCArray
+ * (src/tools/contest.hpp:88-91). Each permutes `strings` in place into
+ * sorted order exactly as the reference's
+ * parallel_sample_sortBTCUI (bingmann-parallel_sample_sort.cpp:31-37) and
+ * parallel_sample_sort_lcp_base (bingmann-parallel_sample_sort.hpp:1733-1748)
+ * do, never writes the characters, and uses the default context of device 0.
+ * lcp[0] is left untouched; cache[i] = strings[i][lcp[i]] for i >= 1
+ * (verify_lcp_cache, src/tools/stringptr.hpp:977-1033). On failure they
+ * abort(). The _status variants return the status code instead. */
+void pssgpu_sort_strings(unsigned char** strings, size_t n);
+void pssgpu_sort_strings_lcp(unsigned char** strings, uintptr_t* lcp, size_t n);
+void pssgpu_sort_strings_lcp_cache(uint8_t** strings, uintptr_t* lcp,
+                                   uint8_t* cache, size_t n);
+int pssgpu_sort_strings_status(unsigned char** strings, uintptr_t* lcp,
+                               uint8_t* cache, size_t n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PSSGPU_H */

@@ -1,0 +1,139 @@
+"""Python host API of the B200 string sample sort.
+
+It mirrors the reference's entry points for this path
+(src/parallel/bingmann-parallel_sample_sort.hpp:1685-1757 and the psstest
+contestant signatures of src/tools/contest.hpp:88-91):
+
+* ``parallel_sample_sort(strings)`` sorts a list of byte strings
+  (the role of ``parallel_sample_sort_base``),
+* ``parallel_sample_sort_lcp(strings)`` also returns the LCP array
+  (``parallel_sample_sort_lcp_base``; ``lcp[0]`` is reported as 0),
+* ``Context.sort_host`` / ``Context.sort_device`` sort an arena
+  (chars + offsets) from host or device memory,
+* ``sort_pointer_array`` calls the C drop-in ``pssgpu_sort_strings*`` on a
+  raw ``unsigned char**`` array, exactly as psstest would.
+
+Errors raise ``SortError`` carrying the library's status code. Nothing here
+falls back to the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _native
+from ._native import PssStats, STATUS_NAMES
+
+
+class SortError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        msg = _native.gpu().pssgpu_last_error()
+        raise SortError(rc, msg.decode() if msg else "")
+
+
+def _ptr(a) -> Optional[int]:
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return a.data_ptr()  # torch tensor
+
+
+class Context:
+    """A device context: one CUDA stream and a reusable workspace."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        _check(_native.gpu().pssgpu_ctx_create(device, C.byref(h)))
+        self._h = h
+        self.device = device
+
+    def close(self) -> None:
+        if self._h:
+            _native.gpu().pssgpu_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def stats(self) -> dict:
+        s = PssStats()
+        _check(_native.gpu().pssgpu_ctx_stats(self._h, C.byref(s)))
+        return {f: getattr(s, f) for f, _ in PssStats._fields_}
+
+    def sort_host(self, chars: np.ndarray, offs: np.ndarray, lcp: bool = True):
+        """Sort the arena strings; returns (perm u32[n], lcp u32[n] or None)."""
+        chars = np.ascontiguousarray(chars, dtype=np.uint8)
+        offs = np.ascontiguousarray(offs, dtype=np.uint64)
+        n = offs.shape[0]
+        perm = np.empty(n, dtype=np.uint32)
+        lcp_a = np.zeros(n, dtype=np.uint32) if lcp else None
+        _check(_native.gpu().pssgpu_sort_host(self._h, _ptr(chars), chars.shape[0], _ptr(offs), n,
+                                              _ptr(perm), _ptr(lcp_a)))
+        return perm, lcp_a
+
+    def sort_device(self, chars, nchars: int, offs, perm, lcp=None, stream=None) -> None:
+        """Sort an arena resident on this context's device (torch tensors or
+        raw device pointers). ``chars`` must hold nchars + 16 bytes."""
+        def addr(t):
+            if t is None:
+                return None
+            return t if isinstance(t, int) else t.data_ptr()
+        n = offs.shape[0] if hasattr(offs, "shape") else int(perm)
+        s = None if stream is None else (stream if isinstance(stream, int) else stream.cuda_stream)
+        _check(_native.gpu().pssgpu_sort_device(self._h, addr(chars), nchars, addr(offs), n,
+                                                addr(perm), addr(lcp), s))
+
+
+_default: Optional[Context] = None
+
+
+def default_context() -> Context:
+    global _default
+    if _default is None:
+        _default = Context(0)
+    return _default
+
+
+def pack_strings(strings: Sequence[bytes]):
+    """Pack byte strings (no NULs inside) into a NUL-terminated arena."""
+    lens = np.fromiter((len(s) for s in strings), dtype=np.uint64, count=len(strings))
+    offs = np.zeros(len(strings), dtype=np.uint64)
+    if len(strings):
+        np.cumsum(lens[:-1] + 1, out=offs[1:])
+    chars = np.frombuffer(b"".join(s + b"\0" for s in strings), dtype=np.uint8).copy()
+    return chars, offs
+
+
+def parallel_sample_sort(strings: Sequence[bytes]) -> list:
+    chars, offs = pack_strings(strings)
+    if len(strings) == 0:
+        return []
+    perm, _ = default_context().sort_host(chars, offs, lcp=False)
+    return [strings[i] for i in perm]
+
+
+def parallel_sample_sort_lcp(strings: Sequence[bytes]):
+    chars, offs = pack_strings(strings)
+    if len(strings) == 0:
+        return [], np.zeros(0, dtype=np.uint32)
+    perm, lcp = default_context().sort_host(chars, offs, lcp=True)
+    lcp[0] = 0
+    return [strings[i] for i in perm], lcp
+
+
+def sort_pointer_array(ptrs, n: int, lcp=None, cache=None) -> int:
+    """Call the contestant drop-in on a ctypes ``unsigned char*`` array.
+    Returns the status code (the void drop-ins abort on failure instead)."""
+    return _native.gpu().pssgpu_sort_strings_status(ptrs, lcp, cache, n)

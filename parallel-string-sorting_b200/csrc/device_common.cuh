@@ -1,0 +1,97 @@
+// device_common.cuh -- shared device helpers of the B200 string sample sort.
+//
+// Key model (the reference's get_char_uint64_simple, src/tools/stringset.hpp:
+// 201-231): the 8 chars at s + depth packed big-endian into a u64, every byte
+// from the first NUL on set to zero. lcpKeyType / lcpKeyDepth restate
+// src/parallel/bingmann-parallel_sample_sort.hpp:225-237.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace pssgpu {
+
+// Error bits OR-ed into the device error word and mapped to status codes.
+enum : uint32_t {
+    ERR_OFFSET = 1u,     // a string offset lies outside the arena
+    ERR_TIMEOUT = 2u,    // a look-back wait exceeded its iteration cap
+    ERR_OVERFLOW = 4u,   // a work list exceeded its capacity
+    ERR_INTERNAL = 8u,   // an internal invariant failed (index out of range)
+};
+
+struct Seg {
+    uint32_t begin;  // first position in the permutation arrays
+    uint32_t size;   // number of strings
+    uint32_t depth;  // chars known to be shared (FINAL: the LCP inside)
+    uint32_t meta;   // bit0 buffer, bit1 keys valid, bit2 final (all equal)
+};
+static_assert(sizeof(Seg) == 16, "Seg layout");
+
+enum : uint32_t { META_BUF = 1u, META_VALID = 2u, META_FINAL = 4u };
+
+__device__ __forceinline__ uint64_t bswap64(uint64_t x)
+{
+    uint32_t lo = (uint32_t)x, hi = (uint32_t)(x >> 32);
+    uint32_t a = __byte_perm(lo, 0, 0x0123);
+    uint32_t b = __byte_perm(hi, 0, 0x0123);
+    return ((uint64_t)a << 32) | b;
+}
+
+// Big-endian key of the 8 chars at byte position p of the arena; positions at
+// or beyond nchars read as NUL. The arena is 8-byte aligned and readable for
+// nchars + 16 bytes, so both aligned words are in bounds whenever p < nchars.
+__device__ __forceinline__ uint64_t load_key(const uint8_t* __restrict__ chars,
+                                             uint64_t nchars, uint64_t p)
+{
+    if (p >= nchars) return 0;
+    const uint64_t* w = reinterpret_cast<const uint64_t*>(chars + (p & ~7ull));
+    const unsigned sh = (unsigned)(p & 7) * 8u;
+    uint64_t raw = __ldg(w) >> sh;
+    if (sh) raw |= __ldg(w + 1) << (64u - sh);
+    // lowest zero byte (little-endian order = string order)
+    const uint64_t z = (raw - 0x0101010101010101ull) & ~raw & 0x8080808080808080ull;
+    if (z) {
+        const unsigned nb = (unsigned)(__ffsll((long long)z) - 1) >> 3;
+        raw = nb ? (raw & (~0ull >> (64u - 8u * nb))) : 0ull;
+    }
+    return bswap64(raw);
+}
+
+__device__ __forceinline__ uint64_t gather_key(const uint8_t* __restrict__ chars,
+                                               uint64_t nchars,
+                                               const uint64_t* __restrict__ offs,
+                                               uint32_t id, uint32_t depth)
+{
+    return load_key(chars, nchars, __ldg(offs + id) + depth);
+}
+
+// chars shared by two keys (8 when equal)
+__device__ __forceinline__ uint32_t lcp_key_type(uint64_t a, uint64_t b)
+{
+    const uint64_t x = a ^ b;
+    return x ? (uint32_t)__clzll((long long)x) >> 3 : 8u;
+}
+
+// number of non-NUL chars in a key
+__device__ __forceinline__ uint32_t lcp_key_depth(uint64_t a)
+{
+    return a ? 8u - ((uint32_t)(__ffsll((long long)a) - 1) >> 3) : 0u;
+}
+
+__device__ __forceinline__ bool key_terminated(uint64_t k) { return (k & 0xFFu) == 0; }
+
+__device__ __forceinline__ uint64_t mix64(uint64_t x)
+{
+    // splitmix64 finaliser: deterministic sample positions
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+__device__ __forceinline__ void set_error(uint32_t* err, uint32_t bit)
+{
+    atomicOr(err, bit);
+}
+
+}  // namespace pssgpu

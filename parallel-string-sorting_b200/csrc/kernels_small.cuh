@@ -1,0 +1,337 @@
+// kernels_small.cuh -- finishes segments of at most SMALL_MAX strings in one
+// block, including every deeper character round and the LCP array. This is
+// the device counterpart of pS5's base cases: sort_mkqs_cache /
+// insertion_sort_cache on 8-byte caches (src/parallel/
+// bingmann-parallel_sample_sort.hpp:805-861, 1056-1178), inssort_generic
+// (src/sequential/inssort.hpp:63-95) and lcp_insertion_sort
+// (src/sequential/bingmann-lcp_inssort.hpp:38-189).
+//
+// Phase A (block): sort (group, key, id) with a shared-memory bitonic sort;
+// runs of equal keys become groups one 8-byte round deeper. Groups larger
+// than a warp stay in phase A; smaller ones are parked.
+// Phase B (warp per parked group): the same rounds on <= 32 strings with
+// shuffles only. A group that stops splitting jumps to its common prefix with
+// a warp-wide 256-byte compare, so deep repeats cost O(LCP / 256) rounds.
+#pragma once
+
+#include "block_util.cuh"
+#include "work.cuh"
+
+namespace pssgpu {
+
+struct SmallSmem {
+    uint64_t key[SMALL_MAX];
+    uint32_t id[SMALL_MAX];
+    uint32_t gdep[SMALL_MAX];   // depth of the active group starting here
+    uint32_t ndep[SMALL_MAX];   // next depth, staged
+    uint16_t grp[SMALL_MAX];    // start index of the element's group
+    uint16_t rs[SMALL_MAX];     // start index of the element's run
+    uint16_t runlen[SMALL_MAX]; // run length, at the run start
+    uint8_t state[SMALL_MAX];   // 0 active (phase A), 1 done, 2 parked
+    uint16_t park_start[SMALL_MAX / 2];
+    uint16_t park_len[SMALL_MAX / 2];
+    uint32_t park_dep[SMALL_MAX / 2];
+    uint32_t tmp[32];
+    uint32_t npark;
+    uint32_t nactive;
+    uint32_t ngroups;
+    uint32_t g0;
+    uint32_t jump;
+};
+
+__device__ __forceinline__ bool tuple_less(uint32_t ga, uint64_t ka, uint32_t ia,
+                                           uint32_t gb, uint64_t kb, uint32_t ib)
+{
+    if (ga != gb) return ga < gb;
+    if (ka != kb) return ka < kb;
+    return ia < ib;
+}
+
+// Bitonic sort of sm.{grp,key,id}[0, npad) by (grp, key, id).
+__device__ void small_bitonic(SmallSmem& sm, uint32_t npad)
+{
+    for (uint32_t kk = 2; kk <= npad; kk <<= 1) {
+        for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = threadIdx.x; i < npad / 2; i += SMALL_THREADS) {
+                const uint32_t a = 2 * i - (i & (j - 1));
+                const uint32_t b = a + j;
+                const bool asc = (a & kk) == 0;
+                const uint32_t ga = sm.grp[a], gb = sm.grp[b];
+                const uint64_t ka = sm.key[a], kb = sm.key[b];
+                const uint32_t ia = sm.id[a], ib = sm.id[b];
+                if (tuple_less(gb, kb, ib, ga, ka, ia) == asc) {
+                    sm.grp[a] = (uint16_t)gb; sm.grp[b] = (uint16_t)ga;
+                    sm.key[a] = kb; sm.key[b] = ka;
+                    sm.id[a] = ib; sm.id[b] = ia;
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// Common-prefix extension (in 8-byte chunks from depth d) of a set of
+// strings against `base`: the first chunk where some string differs from
+// base or base ends. Used when a group stopped splitting.
+__device__ __forceinline__ uint32_t chunks_equal(const Work& w, uint32_t base, uint32_t other,
+                                                 uint32_t d, uint32_t limit)
+{
+    uint32_t c = 0;
+    const uint64_t ob = __ldg(w.offs + base) + d, oo = __ldg(w.offs + other) + d;
+    while (c < limit) {
+        const uint64_t ka = load_key(w.chars, w.nchars, ob + 8ull * c);
+        const uint64_t kb = load_key(w.chars, w.nchars, oo + 8ull * c);
+        if (ka != kb || key_terminated(ka)) break;
+        ++c;
+    }
+    return c;
+}
+
+// Warp-level rounds for one parked group of c <= 32 strings at depth d,
+// occupying sm.id[start, start + c) and positions begin + start + ...
+__device__ void warp_group_sort(const Work& w, SmallSmem& sm, uint32_t begin,
+                                uint32_t start, uint32_t c, uint32_t d)
+{
+    const uint32_t lane = threadIdx.x & 31;
+    const bool real = lane < c;
+    uint32_t myid = real ? sm.id[start + lane] : 0xFFFFFFFFu;
+    uint32_t mygrp = real ? 0u : 0xFFFFFFFFu;
+    uint32_t mydep = d;
+    uint32_t mystate = real ? 0u : 1u;  // 0 active, 1 done
+    uint64_t mykey = 0;
+    uint32_t prev_active = c;
+    bool stalled = false;
+    while (true) {
+        const uint32_t A = __ballot_sync(0xffffffffu, mystate == 0);
+        if (A == 0) break;
+        if (stalled) {
+            // exactly one active group: jump to its common prefix
+            const int f = __ffs(A) - 1;
+            const uint32_t base = __shfl_sync(0xffffffffu, myid, f);
+            const uint32_t dd = __shfl_sync(0xffffffffu, mydep, f);
+            uint32_t best = 0xFFFFFFFFu;
+            uint32_t rest = A & ~(1u << f);
+            const uint64_t ob = __ldg(w.offs + base) + dd;
+            while (rest) {
+                const int j = __ffs(rest) - 1;
+                rest &= rest - 1;
+                const uint32_t other = __shfl_sync(0xffffffffu, myid, j);
+                const uint64_t oo = __ldg(w.offs + other) + dd;
+                for (uint32_t t = 0; t * 32 < best; ++t) {
+                    const uint32_t ch = t * 32 + lane;
+                    const uint64_t ka = load_key(w.chars, w.nchars, ob + 8ull * ch);
+                    const uint64_t kb = load_key(w.chars, w.nchars, oo + 8ull * ch);
+                    const uint32_t bal = __ballot_sync(0xffffffffu, ka != kb || key_terminated(ka));
+                    if (bal) {
+                        best = min(best, t * 32 + (uint32_t)(__ffs(bal) - 1));
+                        break;
+                    }
+                }
+            }
+            if (mystate == 0) mydep = dd + 8u * best;
+        }
+        if (mystate == 0) mykey = gather_key(w.chars, w.nchars, w.offs, myid, mydep);
+        // bitonic sort of the 32 lanes by (grp, key, id), carrying dep/state
+#pragma unroll
+        for (uint32_t kk = 2; kk <= 32; kk <<= 1) {
+#pragma unroll
+            for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
+                const uint32_t og = __shfl_xor_sync(0xffffffffu, mygrp, j);
+                const uint64_t ok = __shfl_xor_sync(0xffffffffu, mykey, j);
+                const uint32_t oi = __shfl_xor_sync(0xffffffffu, myid, j);
+                const uint32_t od = __shfl_xor_sync(0xffffffffu, mydep, j);
+                const uint32_t os = __shfl_xor_sync(0xffffffffu, mystate, j);
+                const bool lower = (lane & j) == 0;
+                const bool asc = (lane & kk) == 0;
+                const bool other_less = tuple_less(og, ok, oi, mygrp, mykey, myid);
+                // lower lane keeps the smaller in an ascending pair
+                const bool take = (lower == asc) ? other_less : !other_less;
+                if (take) { mygrp = og; mykey = ok; myid = oi; mydep = od; mystate = os; }
+            }
+        }
+        const uint32_t pg = __shfl_up_sync(0xffffffffu, mygrp, 1);
+        const uint64_t pk = __shfl_up_sync(0xffffffffu, mykey, 1);
+        const bool ns = lane == 0 || mygrp != pg || mykey != pk;
+        const uint32_t NS = __ballot_sync(0xffffffffu, ns);
+        const uint32_t le = NS & (0xFFFFFFFFu >> (31 - lane));
+        const uint32_t rs = 31u - __clz(le);
+        const uint32_t gtm = lane == 31 ? 0u : (NS & (0xFFFFFFFFu << (lane + 1)));
+        const uint32_t nx = gtm ? (uint32_t)(__ffs(gtm) - 1) : 32u;
+        const uint32_t len = nx - rs;
+        if (mystate == 0) {
+            if (lane >= 1 && pg == mygrp && w.lcp) {
+                const uint32_t pos = begin + start + lane;
+                if (pk != mykey) w.lcp[pos] = mydep + lcp_key_type(pk, mykey);
+                else if (key_terminated(mykey)) w.lcp[pos] = mydep + lcp_key_depth(mykey);
+            }
+            if (len == 1 || key_terminated(mykey)) mystate = 1;
+            else mydep += 8;
+            mygrp = rs;
+        }
+        const uint32_t A2 = __ballot_sync(0xffffffffu, mystate == 0);
+        const uint32_t G2 = __ballot_sync(0xffffffffu, mystate == 0 && rs == lane);
+        const uint32_t na = __popc(A2);
+        stalled = (na == prev_active) && (__popc(G2) == 1);
+        prev_active = na;
+    }
+    if (real) sm.id[start + lane] = myid;
+}
+
+__global__ void __launch_bounds__(SMALL_THREADS) k_small(Work w, uint32_t nsmall)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SmallSmem& sm = *reinterpret_cast<SmallSmem*>(smem_raw);
+    const Seg sg = w.small[w.cur][blockIdx.x];
+    const uint32_t m = sg.size, begin = sg.begin;
+    const int buf = sg.meta & META_BUF;
+    const uint32_t* gids = w.ids[buf];
+    if (sg.meta & META_FINAL) {
+        for (uint32_t i = threadIdx.x; i < m; i += SMALL_THREADS) {
+            w.perm[begin + i] = gids[begin + i];
+            if (w.lcp && i) w.lcp[begin + i] = sg.depth;
+        }
+        return;
+    }
+    if (threadIdx.x == 0) {
+        sm.npark = 0;
+        atomicAdd(w.counters + C_SMALLSEGS, 1u);
+    }
+    for (uint32_t i = threadIdx.x; i < m; i += SMALL_THREADS) sm.id[i] = gids[begin + i];
+    __syncthreads();
+    if (m <= (uint32_t)WARP_GROUP_MAX) {
+        if (threadIdx.x == 0) {
+            sm.park_start[0] = 0; sm.park_len[0] = (uint16_t)m; sm.park_dep[0] = sg.depth;
+            sm.npark = 1;
+        }
+        __syncthreads();
+    } else {
+        // ---------------- phase A ----------------
+        uint32_t npad = 1;
+        while (npad < m) npad <<= 1;
+        const bool valid = sg.meta & META_VALID;
+        for (uint32_t i = threadIdx.x; i < npad; i += SMALL_THREADS) {
+            if (i < m) {
+                sm.key[i] = valid ? w.keys[buf][begin + i]
+                                  : gather_key(w.chars, w.nchars, w.offs, sm.id[i], sg.depth);
+                sm.grp[i] = 0;
+                sm.state[i] = 0;
+            } else {
+                sm.key[i] = ~0ull;
+                sm.id[i] = 0xFFFFFFFFu;
+                sm.grp[i] = 0xFFFF;
+                sm.state[i] = 1;
+            }
+        }
+        if (threadIdx.x == 0) sm.gdep[0] = sg.depth;
+        uint32_t prev_active = m;
+        bool stalled = false;
+        const uint32_t per = (m + SMALL_THREADS - 1) / SMALL_THREADS;
+        const uint32_t clo = min(threadIdx.x * per, m), chi = min(clo + per, m);
+        while (true) {
+            __syncthreads();
+            if (stalled) {
+                // one active group that did not split: jump to its common prefix
+                const uint32_t g0 = sm.g0;
+                const uint32_t d0 = sm.gdep[g0];
+                const uint32_t base = sm.id[g0];
+                if (threadIdx.x == 0) sm.jump = 0xFFFFFFFFu;
+                __syncthreads();
+                for (uint32_t i = threadIdx.x; i < m; i += SMALL_THREADS) {
+                    if (sm.state[i] != 0 || i == g0) continue;
+                    const uint32_t lim = *((volatile uint32_t*)&sm.jump);
+                    const uint32_t c = chunks_equal(w, base, sm.id[i], d0, lim);
+                    atomicMin(&sm.jump, c);
+                }
+                __syncthreads();
+                if (threadIdx.x == 0) sm.gdep[g0] = d0 + 8u * sm.jump;
+                __syncthreads();
+                for (uint32_t i = threadIdx.x; i < m; i += SMALL_THREADS)
+                    if (sm.state[i] == 0)
+                        sm.key[i] = gather_key(w.chars, w.nchars, w.offs, sm.id[i], sm.gdep[sm.grp[i]]);
+                __syncthreads();
+            }
+            small_bitonic(sm, npad);
+            // run starts: a run is a maximal stretch of equal (grp, key)
+            uint32_t last = 0;
+            for (uint32_t i = clo; i < chi; ++i) {
+                const bool ns = i == 0 || sm.grp[i] != sm.grp[i - 1] || sm.key[i] != sm.key[i - 1];
+                if (ns) last = i;
+            }
+            const bool any = clo < chi;
+            uint32_t carry = block_excl_max<SMALL_THREADS>(any ? last : 0u, sm.tmp);
+            for (uint32_t i = clo; i < chi; ++i) {
+                const bool ns = i == 0 || sm.grp[i] != sm.grp[i - 1] || sm.key[i] != sm.key[i - 1];
+                if (ns) carry = i;
+                sm.rs[i] = (uint16_t)carry;
+                const bool end = (i + 1 == m) || sm.grp[i + 1] != sm.grp[i] || sm.key[i + 1] != sm.key[i];
+                if (end) sm.runlen[carry] = (uint16_t)(i + 1 - carry);
+            }
+            if (threadIdx.x == 0) { sm.nactive = 0; sm.ngroups = 0; }
+            __syncthreads();
+            // resolve: LCPs, new states, parked groups (reads gdep only)
+            for (uint32_t i = threadIdx.x; i < m; i += SMALL_THREADS) {
+                if (sm.state[i] != 0) continue;
+                const uint64_t k = sm.key[i];
+                const uint32_t d = sm.gdep[sm.grp[i]];
+                if (i >= 1 && sm.grp[i - 1] == sm.grp[i] && w.lcp) {
+                    const uint64_t pk = sm.key[i - 1];
+                    if (pk != k) w.lcp[begin + i] = d + lcp_key_type(pk, k);
+                    else if (key_terminated(k)) w.lcp[begin + i] = d + lcp_key_depth(k);
+                }
+                const uint32_t r = sm.rs[i];
+                const uint32_t len = sm.runlen[r];
+                if (i == r && len > 1 && !key_terminated(k)) {
+                    if (len <= (uint32_t)WARP_GROUP_MAX) {
+                        const uint32_t at = atomicAdd(&sm.npark, 1u);
+                        sm.park_start[at] = (uint16_t)r;
+                        sm.park_len[at] = (uint16_t)len;
+                        sm.park_dep[at] = d + 8;
+                    } else {
+                        sm.ndep[r] = d + 8;
+                    }
+                }
+            }
+            __syncthreads();
+            for (uint32_t i = threadIdx.x; i < m; i += SMALL_THREADS) {
+                if (sm.state[i] != 0) continue;
+                const uint32_t r = sm.rs[i];
+                const uint32_t len = sm.runlen[r];
+                const uint64_t k = sm.key[i];
+                uint8_t ns;
+                if (len == 1 || key_terminated(k)) ns = 1;
+                else if (len <= (uint32_t)WARP_GROUP_MAX) ns = 2;
+                else ns = 0;
+                sm.grp[i] = (uint16_t)r;
+                sm.state[i] = ns;
+                if (ns == 0) {
+                    atomicAdd(&sm.nactive, 1u);
+                    if (i == r) {
+                        sm.gdep[r] = sm.ndep[r];
+                        atomicAdd(&sm.ngroups, 1u);
+                        sm.g0 = r;
+                    }
+                }
+            }
+            __syncthreads();
+            const uint32_t na = sm.nactive;
+            if (na == 0) break;
+            stalled = (na == prev_active) && (sm.ngroups == 1);
+            prev_active = na;
+            if (!stalled) {
+                for (uint32_t i = threadIdx.x; i < m; i += SMALL_THREADS)
+                    if (sm.state[i] == 0)
+                        sm.key[i] = gather_key(w.chars, w.nchars, w.offs, sm.id[i], sm.gdep[sm.grp[i]]);
+            }
+        }
+        __syncthreads();
+    }
+    // ---------------- phase B ----------------
+    const uint32_t warp = threadIdx.x >> 5;
+    const uint32_t np = sm.npark;
+    for (uint32_t g = warp; g < np; g += SMALL_THREADS / 32)
+        warp_group_sort(w, sm, begin, sm.park_start[g], sm.park_len[g], sm.park_dep[g]);
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < m; i += SMALL_THREADS) w.perm[begin + i] = sm.id[i];
+}
+
+}  // namespace pssgpu

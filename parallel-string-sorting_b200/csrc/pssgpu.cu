@@ -1,0 +1,498 @@
+// pssgpu.cu -- host driver and C ABI of the B200 string sample sort.
+//
+// The driver replaces pS5's job queue (src/tools/jobqueue.hpp:74-261) and
+// Enqueue (src/parallel/bingmann-parallel_sample_sort.hpp:1613-1634) with
+// level-synchronous passes: every pass runs one sample-sort step over all
+// segments larger than SMALL_MAX strings (kernels_big.cuh) and finishes all
+// smaller segments in shared memory (kernels_small.cuh). One 24-byte
+// device-to-host read per pass sizes the next pass's grids.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/pssgpu.h"
+#include "kernels_big.cuh"
+#include "kernels_small.cuh"
+
+namespace pssgpu {
+
+static thread_local std::string g_last_error;
+
+static int fail(int code, const std::string& msg)
+{
+    g_last_error = msg;
+    return code;
+}
+
+#define PSS_CUDA(call)                                                              \
+    do {                                                                            \
+        cudaError_t e_ = (call);                                                    \
+        if (e_ != cudaSuccess)                                                      \
+            return fail(e_ == cudaErrorMemoryAllocation ? PSSGPU_ENOMEM : PSSGPU_ECUDA, \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));       \
+    } while (0)
+
+__global__ void k_init(Work w)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < w.n; i += gridDim.x * blockDim.x) {
+        w.ids[0][i] = i;
+        if (w.offs[i] >= w.nchars) set_error(w.counters + C_ERR, ERR_OFFSET);
+    }
+}
+
+__global__ void k_root(Work w)
+{
+    push_seg(w, 0, Seg{0u, w.n, 0u, 0u});
+}
+
+struct Sizes {
+    uint64_t n, big_cap, small_cap, tile_cap;
+};
+
+static Sizes sizes_for(uint64_t n)
+{
+    Sizes s;
+    s.n = std::max<uint64_t>(n, 1);
+    s.big_cap = s.n / (SMALL_MAX + 1) + 2;
+    s.small_cap = s.n / 2 + 2;
+    s.tile_cap = s.n / TILE + s.big_cap + 1;
+    return s;
+}
+
+static uint64_t align256(uint64_t b) { return (b + 255) & ~255ull; }
+
+static uint64_t workspace_bytes(const Sizes& s)
+{
+    uint64_t b = 0;
+    b += 2 * align256(4 * s.n);                    // ids
+    b += 2 * align256(8 * s.n);                    // keys
+    b += align256(2 * s.n);                        // bucket ids
+    b += align256(8 * s.n);                        // boundary list
+    b += 2 * align256(16 * s.big_cap);             // big lists
+    b += 2 * align256(16 * s.small_cap);           // small lists
+    b += align256(4 * (s.big_cap + 1));            // tile starts
+    b += 2 * align256(s.big_cap);                  // tree bits, one-bucket flags
+    b += 2 * align256(8ull * 1024 * s.big_cap);    // trees, splitters
+    b += 2 * align256(4ull * MAX_BKT * s.big_cap); // bucket counts, starts
+    b += align256(8ull * MAX_BKT * s.tile_cap);    // look-back status
+    b += align256(4 * C_COUNT);                    // counters
+    return b;
+}
+
+struct Ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::mutex mu;
+    // workspace
+    unsigned char* ws = nullptr;
+    uint64_t ws_bytes = 0;
+    Sizes cap{0, 0, 0, 0};
+    Work base{};
+    uint32_t epoch = 0;
+    uint32_t* host_counters = nullptr;  // pinned
+    // staging for the host entry points
+    unsigned char* io = nullptr;
+    uint64_t io_bytes = 0;
+    pssgpu_stats stats{};
+};
+
+static int ensure_workspace(Ctx* c, uint64_t n)
+{
+    if (c->ws && n <= c->cap.n) return PSSGPU_OK;
+    if (c->ws) {
+        cudaFree(c->ws);
+        c->ws = nullptr;
+    }
+    const Sizes s = sizes_for(std::max<uint64_t>(n, 1024));
+    const uint64_t bytes = workspace_bytes(s);
+    PSS_CUDA(cudaMalloc(&c->ws, bytes));
+    c->ws_bytes = bytes;
+    c->cap = s;
+    unsigned char* p = c->ws;
+    auto take = [&](uint64_t b) { unsigned char* r = p; p += align256(b); return r; };
+    Work& w = c->base;
+    w = Work{};
+    for (int i = 0; i < 2; ++i) w.ids[i] = (uint32_t*)take(4 * s.n);
+    for (int i = 0; i < 2; ++i) w.keys[i] = (uint64_t*)take(8 * s.n);
+    w.bkt = (uint16_t*)take(2 * s.n);
+    w.bnd = (uint2*)take(8 * s.n);
+    w.bnd_cap = (uint32_t)s.n;
+    for (int i = 0; i < 2; ++i) w.big[i] = (Seg*)take(16 * s.big_cap);
+    for (int i = 0; i < 2; ++i) w.small[i] = (Seg*)take(16 * s.small_cap);
+    w.big_cap = (uint32_t)s.big_cap;
+    w.small_cap = (uint32_t)s.small_cap;
+    w.tile_start = (uint32_t*)take(4 * (s.big_cap + 1));
+    w.tree_bits = (uint8_t*)take(s.big_cap);
+    w.bflags = (uint8_t*)take(s.big_cap);
+    w.tree = (uint64_t*)take(8ull * 1024 * s.big_cap);
+    w.spl = (uint64_t*)take(8ull * 1024 * s.big_cap);
+    w.bcount = (uint32_t*)take(4ull * MAX_BKT * s.big_cap);
+    w.bstart = (uint32_t*)take(4ull * MAX_BKT * s.big_cap);
+    w.status = (uint64_t*)take(8ull * MAX_BKT * s.tile_cap);
+    w.tile_cap = (uint32_t)s.tile_cap;
+    w.counters = (uint32_t*)take(4 * C_COUNT);
+    PSS_CUDA(cudaMemsetAsync(w.status, 0, 8ull * MAX_BKT * s.tile_cap, c->stream));
+    c->epoch = 0;
+    return PSSGPU_OK;
+}
+
+static int setup_kernels()
+{
+    static int done = 0;
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lk(mu);
+    if (done) return PSSGPU_OK;
+    PSS_CUDA(cudaFuncSetAttribute(k_small, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sizeof(SmallSmem)));
+    PSS_CUDA(cudaFuncSetAttribute(k_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sizeof(ScatterSmem)));
+    done = 1;
+    return PSSGPU_OK;
+}
+
+static int map_device_error(uint32_t err)
+{
+    if (err & ERR_OFFSET) return fail(PSSGPU_EINVAL, "a string offset lies outside the arena");
+    if (err & ERR_TIMEOUT) return fail(PSSGPU_ETIMEOUT, "a look-back wait exceeded its iteration cap");
+    if (err & ERR_OVERFLOW) return fail(PSSGPU_ECUDA, "an internal work list overflowed");
+    return fail(PSSGPU_ECUDA, "internal device error");
+}
+
+// Sort n strings already resident on the device. Caller holds c->mu.
+static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_t* offs,
+                    uint32_t n, uint32_t* perm, uint32_t* lcp, cudaStream_t st)
+{
+    int rc = ensure_workspace(c, n);
+    if (rc) return rc;
+    if ((rc = setup_kernels())) return rc;
+    Work w = c->base;
+    w.chars = chars;
+    w.nchars = nchars;
+    w.offs = offs;
+    w.n = n;
+    w.perm = perm;
+    w.lcp = lcp;
+    pssgpu_stats stats{};
+    PSS_CUDA(cudaEventRecord(c->ev0, st));
+    PSS_CUDA(cudaMemsetAsync(w.counters, 0, 4 * C_COUNT, st));
+    k_init<<<1184, 256, 0, st>>>(w);
+    k_root<<<1, 1, 0, st>>>(w);
+    stats.kernel_launches += 2;
+    uint32_t* hc = c->host_counters;
+    PSS_CUDA(cudaMemcpyAsync(hc, w.counters, 4 * C_COUNT, cudaMemcpyDeviceToHost, st));
+    PSS_CUDA(cudaStreamSynchronize(st));
+    uint32_t nbig = hc[C_NBIG], nsmall = hc[C_NSMALL], ntiles = hc[C_NTILES];
+    uint32_t err = hc[C_ERR];
+    int cur = 0;
+    while (!err && (nbig || nsmall)) {
+        const int nxt = cur ^ 1;
+        w.cur = cur;
+        if (nbig) {
+            if (++c->epoch >= 0xFFFFu) {
+                PSS_CUDA(cudaMemsetAsync(w.status, 0, 8ull * MAX_BKT * c->cap.tile_cap, st));
+                c->epoch = 1;
+            }
+            w.epoch = c->epoch;
+        }
+        PSS_CUDA(cudaMemsetAsync(w.counters + 3 * nxt, 0, 12, st));
+        PSS_CUDA(cudaMemsetAsync(w.counters + C_TICKET, 0, 4, st));
+        if (nsmall) {
+            k_small<<<nsmall, SMALL_THREADS, sizeof(SmallSmem), st>>>(w, nsmall);
+            stats.kernel_launches += 1;
+        }
+        if (nbig) {
+            if (ntiles > c->cap.tile_cap) return fail(PSSGPU_ECUDA, "tile capacity exceeded");
+            k_tile_scan<<<1, 1024, 0, st>>>(w, nbig);
+            k_sample<<<nbig, 1024, 0, st>>>(w);
+            k_classify<<<ntiles, TILE_THREADS, 0, st>>>(w, nbig);
+            k_bstart<<<nbig, 1024, 0, st>>>(w);
+            k_scatter<<<ntiles, TILE_THREADS, sizeof(ScatterSmem), st>>>(w, nbig);
+            k_children<<<nbig, 1024, 0, st>>>(w);
+            stats.kernel_launches += 6;
+            stats.passes += 1;
+            stats.big_elements += (uint64_t)ntiles * TILE;
+        }
+        PSS_CUDA(cudaGetLastError());
+        PSS_CUDA(cudaMemcpyAsync(hc, w.counters, 4 * C_COUNT, cudaMemcpyDeviceToHost, st));
+        PSS_CUDA(cudaStreamSynchronize(st));
+        nbig = hc[3 * nxt + C_NBIG];
+        nsmall = hc[3 * nxt + C_NSMALL];
+        ntiles = hc[3 * nxt + C_NTILES];
+        err = hc[C_ERR];
+        cur = nxt;
+    }
+    if (!err && lcp) {
+        k_boundary_lcp<<<1184, 256, 0, st>>>(w);
+        stats.kernel_launches += 1;
+    }
+    PSS_CUDA(cudaEventRecord(c->ev1, st));
+    PSS_CUDA(cudaMemcpyAsync(hc, w.counters, 4 * C_COUNT, cudaMemcpyDeviceToHost, st));
+    PSS_CUDA(cudaStreamSynchronize(st));
+    PSS_CUDA(cudaGetLastError());
+    err = hc[C_ERR];
+    stats.small_segments = hc[C_SMALLSEGS];
+    stats.boundaries = hc[C_NBND];
+    cudaEventElapsedTime(&stats.device_ms, c->ev0, c->ev1);
+    c->stats = stats;
+    if (err) return map_device_error(err);
+    return PSSGPU_OK;
+}
+
+static int ctx_create(int device, Ctx** out)
+{
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+        return fail(PSSGPU_ENODEV, "no CUDA device available");
+    if (device < 0 || device >= count) return fail(PSSGPU_EINVAL, "device index out of range");
+    PSS_CUDA(cudaSetDevice(device));
+    Ctx* c = new Ctx;
+    c->device = device;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+        cudaHostAlloc((void**)&c->host_counters, 4 * C_COUNT, cudaHostAllocDefault) != cudaSuccess) {
+        delete c;
+        return fail(PSSGPU_ECUDA, "stream/event/pinned allocation failed");
+    }
+    *out = c;
+    return PSSGPU_OK;
+}
+
+static void ctx_destroy(Ctx* c)
+{
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->ws) cudaFree(c->ws);
+    if (c->io) cudaFree(c->io);
+    if (c->host_counters) cudaFreeHost(c->host_counters);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+static int ensure_io(Ctx* c, uint64_t bytes)
+{
+    if (c->io && bytes <= c->io_bytes) return PSSGPU_OK;
+    if (c->io) {
+        cudaFree(c->io);
+        c->io = nullptr;
+    }
+    PSS_CUDA(cudaMalloc(&c->io, bytes));
+    c->io_bytes = bytes;
+    return PSSGPU_OK;
+}
+
+static int check_args(uint64_t nchars, uint64_t n)
+{
+    if (n > PSSGPU_MAX_STRINGS) return fail(PSSGPU_EINVAL, "too many strings for one call");
+    if (n > 0 && nchars == 0) return fail(PSSGPU_EINVAL, "empty arena with strings");
+    return PSSGPU_OK;
+}
+
+// Host buffers in, host buffers out. Caller holds c->mu.
+static int sort_host_locked(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_t* offs,
+                            uint64_t n, uint32_t* perm, uint32_t* lcp)
+{
+    int rc = check_args(nchars, n);
+    if (rc) return rc;
+    if (n == 0) return PSSGPU_OK;
+    if (chars[nchars - 1] != 0) return fail(PSSGPU_EINVAL, "arena does not end with NUL");
+    PSS_CUDA(cudaSetDevice(c->device));
+    const uint64_t b_chars = align256(nchars + PSSGPU_ARENA_PAD);
+    const uint64_t b_offs = align256(8 * n);
+    const uint64_t b_perm = align256(4 * n);
+    const uint64_t b_lcp = lcp ? align256(4 * n) : 0;
+    if ((rc = ensure_io(c, b_chars + b_offs + b_perm + b_lcp))) return rc;
+    uint8_t* d_chars = c->io;
+    uint64_t* d_offs = (uint64_t*)(c->io + b_chars);
+    uint32_t* d_perm = (uint32_t*)(c->io + b_chars + b_offs);
+    uint32_t* d_lcp = lcp ? (uint32_t*)(c->io + b_chars + b_offs + b_perm) : nullptr;
+    cudaStream_t st = c->stream;
+    PSS_CUDA(cudaMemcpyAsync(d_chars, chars, nchars, cudaMemcpyHostToDevice, st));
+    PSS_CUDA(cudaMemsetAsync(d_chars + nchars, 0, b_chars - nchars, st));
+    PSS_CUDA(cudaMemcpyAsync(d_offs, offs, 8 * n, cudaMemcpyHostToDevice, st));
+    if ((rc = run_sort(c, d_chars, nchars, d_offs, (uint32_t)n, d_perm, d_lcp, st))) return rc;
+    PSS_CUDA(cudaMemcpyAsync(perm, d_perm, 4 * n, cudaMemcpyDeviceToHost, st));
+    if (lcp && n > 1)
+        PSS_CUDA(cudaMemcpyAsync(lcp + 1, d_lcp + 1, 4 * (n - 1), cudaMemcpyDeviceToHost, st));
+    PSS_CUDA(cudaStreamSynchronize(st));
+    return PSSGPU_OK;
+}
+
+// Default contexts for the pointer-array drop-ins, one per device.
+static Ctx* default_ctx(int device, int* rc)
+{
+    static std::mutex mu;
+    static std::vector<Ctx*> ctxs;
+    std::lock_guard<std::mutex> lk(mu);
+    if ((int)ctxs.size() <= device) ctxs.resize(device + 1, nullptr);
+    if (!ctxs[device]) {
+        Ctx* c = nullptr;
+        *rc = ctx_create(device, &c);
+        if (*rc) return nullptr;
+        ctxs[device] = c;
+    }
+    *rc = PSSGPU_OK;
+    return ctxs[device];
+}
+
+// Pack a pointer array into (arena, offsets): a dense copy of the span the
+// strings occupy when it is compact (the psstest arena, suffix pointers),
+// else a gather of every string.
+static int sort_pointer_array(unsigned char** strings, uintptr_t* lcp_out, uint8_t* cache,
+                              size_t n)
+{
+    if (n > PSSGPU_MAX_STRINGS) return fail(PSSGPU_EINVAL, "too many strings for one call");
+    if (n <= 1) return PSSGPU_OK;
+    int rc;
+    Ctx* c = default_ctx(0, &rc);
+    if (!c) return rc;
+    std::lock_guard<std::mutex> lk(c->mu);
+    uintptr_t lo = UINTPTR_MAX, hi = 0;
+    for (size_t i = 0; i < n; ++i) {
+        const uintptr_t p = (uintptr_t)strings[i];
+        lo = std::min(lo, p);
+        hi = std::max(hi, p);
+    }
+    const uint64_t hi_end = hi + strlen((const char*)hi) + 1 - lo;
+    std::vector<uint64_t> offs(n);
+    std::vector<uint8_t> packed;
+    const uint8_t* arena;
+    uint64_t nchars;
+    if (hi_end <= 8ull * n + (64ull << 20)) {
+        arena = (const uint8_t*)lo;
+        nchars = hi_end;
+        for (size_t i = 0; i < n; ++i) offs[i] = (uintptr_t)strings[i] - lo;
+    } else {
+        uint64_t total = 0;
+        std::vector<uint64_t> len(n);
+        for (size_t i = 0; i < n; ++i) {
+            len[i] = strlen((const char*)strings[i]) + 1;
+            offs[i] = total;
+            total += len[i];
+        }
+        packed.resize(total);
+        for (size_t i = 0; i < n; ++i) memcpy(packed.data() + offs[i], strings[i], len[i]);
+        arena = packed.data();
+        nchars = total;
+    }
+    std::vector<uint32_t> perm(n);
+    std::vector<uint32_t> lcp32(lcp_out ? n : 0);
+    rc = sort_host_locked(c, arena, nchars, offs.data(), n, perm.data(),
+                          lcp_out ? lcp32.data() : nullptr);
+    if (rc) return rc;
+    std::vector<unsigned char*> orig(strings, strings + n);
+    for (size_t i = 0; i < n; ++i) strings[i] = orig[perm[i]];
+    if (lcp_out)
+        for (size_t i = 1; i < n; ++i) lcp_out[i] = lcp32[i];
+    if (cache && lcp_out)
+        for (size_t i = 1; i < n; ++i) cache[i] = strings[i][lcp_out[i]];
+    return PSSGPU_OK;
+}
+
+}  // namespace pssgpu
+
+using namespace pssgpu;
+
+
+
+extern "C" {
+
+const char* pssgpu_last_error(void) { return g_last_error.c_str(); }
+
+const char* pssgpu_version(void) { return "pssgpu 0.1 sm_100a"; }
+
+int pssgpu_ctx_create(int device, pssgpu_ctx** out)
+{
+    if (!out) return fail(PSSGPU_EINVAL, "null output pointer");
+    Ctx* c = nullptr;
+    int rc = ctx_create(device, &c);
+    if (rc) return rc;
+    *out = reinterpret_cast<pssgpu_ctx*>(c);
+    return PSSGPU_OK;
+}
+
+void pssgpu_ctx_destroy(pssgpu_ctx* ctx) { ctx_destroy(reinterpret_cast<Ctx*>(ctx)); }
+
+uint64_t pssgpu_workspace_bytes(uint64_t n)
+{
+    return workspace_bytes(sizes_for(std::max<uint64_t>(n, 1024)));
+}
+
+int pssgpu_ctx_stats(pssgpu_ctx* ctx, pssgpu_stats* out)
+{
+    if (!ctx || !out) return fail(PSSGPU_EINVAL, "null argument");
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    std::lock_guard<std::mutex> lk(c->mu);
+    *out = c->stats;
+    return PSSGPU_OK;
+}
+
+int pssgpu_sort_host(pssgpu_ctx* ctx, const uint8_t* chars, uint64_t nchars,
+                     const uint64_t* offs, uint64_t n, uint32_t* perm, uint32_t* lcp)
+{
+    if (!ctx) return fail(PSSGPU_EINVAL, "null context");
+    if (n && (!chars || !offs || !perm)) return fail(PSSGPU_EINVAL, "null buffer");
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    std::lock_guard<std::mutex> lk(c->mu);
+    return sort_host_locked(c, chars, nchars, offs, n, perm, lcp);
+}
+
+int pssgpu_sort_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nchars,
+                       const uint64_t* d_offs, uint64_t n, uint32_t* d_perm, uint32_t* d_lcp,
+                       void* stream)
+{
+    if (!ctx) return fail(PSSGPU_EINVAL, "null context");
+    int rc = check_args(nchars, n);
+    if (rc) return rc;
+    if (n == 0) return PSSGPU_OK;
+    if (!d_chars || !d_offs || !d_perm) return fail(PSSGPU_EINVAL, "null buffer");
+    if (((uintptr_t)d_chars & 7) != 0) return fail(PSSGPU_EINVAL, "arena not 8-byte aligned");
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    std::lock_guard<std::mutex> lk(c->mu);
+    PSS_CUDA(cudaSetDevice(c->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    uint8_t last = 1;
+    PSS_CUDA(cudaMemcpyAsync(&last, d_chars + nchars - 1, 1, cudaMemcpyDeviceToHost, st));
+    PSS_CUDA(cudaStreamSynchronize(st));
+    if (last != 0) return fail(PSSGPU_EINVAL, "arena does not end with NUL");
+    return run_sort(c, d_chars, nchars, d_offs, (uint32_t)n, d_perm, d_lcp, st);
+}
+
+int pssgpu_sort_strings_status(unsigned char** strings, uintptr_t* lcp, uint8_t* cache, size_t n)
+{
+    if (n && !strings) return fail(PSSGPU_EINVAL, "null string array");
+    return sort_pointer_array(strings, lcp, cache, n);
+}
+
+static void die_on(int rc)
+{
+    if (rc) {
+        fprintf(stderr, "pssgpu: sort failed (status %d): %s\n", rc, g_last_error.c_str());
+        abort();
+    }
+}
+
+void pssgpu_sort_strings(unsigned char** strings, size_t n)
+{
+    die_on(pssgpu_sort_strings_status(strings, nullptr, nullptr, n));
+}
+
+void pssgpu_sort_strings_lcp(unsigned char** strings, uintptr_t* lcp, size_t n)
+{
+    die_on(pssgpu_sort_strings_status(strings, lcp, nullptr, n));
+}
+
+void pssgpu_sort_strings_lcp_cache(uint8_t** strings, uintptr_t* lcp, uint8_t* cache, size_t n)
+{
+    die_on(pssgpu_sort_strings_status(strings, lcp, cache, n));
+}
+
+}  // extern "C"

@@ -1,0 +1,110 @@
+"""Seeded synthetic workloads with the shapes of the reference's benchmark
+configurations (no public dataset is available offline; every generator is
+deterministic and documented).
+
+* ``digits(seed=1)``            -- strings of length U[1,40] over '0'..'9',
+  packed to 10 MiB of chars (a psstest ``random10``-style plain sort).
+* ``prefixes(n=64 Mi, seed=2)``  -- one of 4096 random 48-char prefixes
+  ('a'..'z', Zipf s=1.1 by rank) + a suffix of length U[8,24]; mean LCP ~50.
+* ``dna_suffixes(seed=3)``       -- a 32 MiB ACGT text with 5% overwritten by
+  copies of earlier 1-10 KiB blocks; all 33,554,433 suffixes.
+* ``random_strings(...)``        -- generic test inputs.
+
+Arenas are (chars u8[nchars + 16], offs u64[n], nchars): NUL-terminated
+strings, 16 zero bytes of padding after the last char. ``out`` allocators let
+callers place the arena in pinned host memory.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Callable, Optional
+
+import numpy as np
+
+from . import _native
+
+PAD = 16
+
+
+def _alloc_np(nbytes: int, dtype) -> np.ndarray:
+    return np.empty(nbytes // np.dtype(dtype).itemsize, dtype=dtype)
+
+
+def random_strings(n: int, lmin: int, lmax: int, alphabet: bytes, seed: int,
+                   alloc: Callable = _alloc_np):
+    w = _native.work()
+    offs = alloc(8 * n, np.uint64) if n else np.zeros(0, np.uint64)
+    nchars = w.pssw_random_offsets(seed, n, lmin, lmax, offs.ctypes.data if n else None)
+    chars = alloc(nchars + PAD, np.uint8)
+    chars[nchars:] = 0
+    alpha = np.frombuffer(alphabet, dtype=np.uint8).copy()
+    if n:
+        w.pssw_random_fill(seed, n, offs.ctypes.data, nchars, alpha.ctypes.data, len(alpha),
+                           chars.ctypes.data)
+    return chars, offs, int(nchars)
+
+
+def digits(seed: int = 1, budget: int = 10 * 1024 * 1024, alloc: Callable = _alloc_np):
+    w = _native.work()
+    nch = C.c_uint64()
+    n = w.pssw_digits_count(seed, budget, C.byref(nch))
+    offs = alloc(8 * n, np.uint64)
+    chars = alloc(nch.value + PAD, np.uint8)
+    chars[nch.value:] = 0
+    w.pssw_digits_fill(seed, n, offs.ctypes.data, chars.ctypes.data)
+    return chars, offs, int(nch.value)
+
+
+def prefixes(n: int = 64 * 1024 * 1024, seed: int = 2, zipf_s: float = 1.1,
+             alloc: Callable = _alloc_np, with_ids: bool = False):
+    w = _native.work()
+    offs = alloc(8 * n, np.uint64)
+    nchars = w.pssw_prefix_offsets(seed, n, offs.ctypes.data)
+    chars = alloc(nchars + PAD, np.uint8)
+    chars[nchars:] = 0
+    ids = np.empty(n, np.uint16) if with_ids else None
+    w.pssw_prefix_fill(seed, n, offs.ctypes.data, zipf_s, chars.ctypes.data,
+                       ids.ctypes.data if with_ids else None)
+    if with_ids:
+        return chars, offs, int(nchars), ids
+    return chars, offs, int(nchars)
+
+
+def dna_text(length: int = 32 * 1024 * 1024, seed: int = 3, copy_frac: float = 0.05,
+             alloc: Callable = _alloc_np):
+    """The text plus its terminating NUL and padding: chars[length] == 0."""
+    chars = alloc(length + 1 + PAD, np.uint8)
+    chars[length:] = 0
+    _native.work().pssw_dna_text(seed, length, copy_frac, chars.ctypes.data)
+    return chars
+
+
+def dna_suffixes(length: int = 32 * 1024 * 1024, seed: int = 3, copy_frac: float = 0.05,
+                 alloc: Callable = _alloc_np):
+    """All length + 1 suffixes of the text (the last one is empty), as the
+    reference's psstest --suffix builds them (src/psstest.cpp:502-518)."""
+    chars = dna_text(length, seed, copy_frac, alloc)
+    offs = alloc(8 * (length + 1), np.uint64)
+    offs[:] = np.arange(length + 1, dtype=np.uint64)
+    return chars, offs, length + 1
+
+
+def alg_bytes(lcp: np.ndarray, T: int = 32) -> dict:
+    """Algorithmic bytes of the sample-sort method for a sorted LCP array."""
+    lcp = np.ascontiguousarray(lcp, dtype=np.uint32)
+    tot, rb, bb = C.c_uint64(), C.c_uint64(), C.c_uint64()
+    mr = C.c_uint32()
+    _native.work().pssw_alg_bytes(lcp.ctypes.data, lcp.shape[0], T, C.byref(tot), C.byref(rb),
+                                  C.byref(bb), C.byref(mr))
+    return {"total": tot.value, "rounds": rb.value, "base": bb.value, "max_round": mr.value}
+
+
+def strings_of(chars: np.ndarray, offs: np.ndarray, ids: Optional[np.ndarray] = None) -> list:
+    """Python bytes of the strings (small inputs only)."""
+    raw = chars.tobytes()
+    idx = range(len(offs)) if ids is None else ids
+    out = []
+    for i in idx:
+        o = int(offs[i])
+        out.append(raw[o:raw.index(b"\0", o)])
+    return out

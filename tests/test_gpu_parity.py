@@ -1,0 +1,194 @@
+"""GPU parity tests: the CUDA path, called through the C ABI, against the
+golden fixtures from the reference pS5, against the oracle restatement on
+seeded inputs, and through size-independent properties (order, permutation,
+LCP rescan) at full workload sizes. Integer work: everything is bit-exact."""
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from golden_util import canonical_ids
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = sorted((Path(__file__).parent / "golden").glob("*.npz"))
+
+
+def check_against_oracle(orc, chars, offs, perm, lcp):
+    ids, rlcp = orc.sort_ids_lcp(chars, offs)
+    assert orc.check_permutation(perm)
+    assert np.array_equal(canonical_ids(chars, offs, perm, lcp),
+                          canonical_ids(chars, offs, ids, rlcp))
+    assert np.array_equal(lcp[1:].astype(np.uint64), rlcp[1:])
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[p.stem for p in GOLDEN])
+def test_golden(ctx, path):
+    z = np.load(path)
+    chars, offs, gids, glcp = z["chars"], z["offs"], z["ids"], z["lcp"]
+    perm, lcp = ctx.sort_host(chars, offs, lcp=True)
+    assert np.array_equal(canonical_ids(chars, offs, perm, lcp), gids)
+    assert np.array_equal(lcp[1:].astype(np.uint64), glcp[1:])
+
+
+@pytest.mark.parametrize("n,lmin,lmax,alpha,seed", [
+    (2, 0, 3, b"ab", 1),
+    (31, 0, 5, b"ab", 2),
+    (33, 0, 9, b"ab", 3),
+    (2048, 0, 12, b"abc", 4),
+    (2049, 0, 12, b"abc", 5),
+    (5000, 0, 40, b"0123456789", 6),
+    (100000, 0, 30, b"ab", 7),
+    (300000, 1, 64, bytes(range(32, 127)), 8),
+    (1000000, 0, 20, b"ACGT", 9),
+])
+def test_random_vs_oracle(pkg, orc, ctx, n, lmin, lmax, alpha, seed):
+    chars, offs, _ = pkg.workloads.random_strings(n, lmin, lmax, alpha, seed)
+    perm, lcp = ctx.sort_host(chars, offs, lcp=True)
+    check_against_oracle(orc, chars, offs, perm, lcp)
+
+
+@pytest.mark.parametrize("strings", [
+    [],
+    [b"only"],
+    [b"b", b"a"],
+    [b""] * 5000,
+    [b"same"] * 10000,
+    [b"\xff" * 40] * 3000 + [b"\xff" * 39],
+    [b"a" * k for k in range(0, 3000, 7)],
+    [b"z" * 2000 + bytes([97 + i % 26]) + b"q" * (i % 5) for i in range(5000)],
+], ids=["empty", "one", "two", "all_empty", "all_equal", "ff_bytes", "prefix_chain",
+        "deep_shared_prefix"])
+def test_edge_cases(pkg, orc, ctx, strings):
+    chars, offs = pkg.pack_strings(strings)
+    if len(strings) == 0:
+        perm, lcp = ctx.sort_host(np.zeros(1, np.uint8), np.zeros(0, np.uint64), lcp=True)
+        assert perm.shape == (0,)
+        return
+    perm, lcp = ctx.sort_host(chars, offs, lcp=True)
+    check_against_oracle(orc, chars, offs, perm, lcp)
+
+
+def test_deep_repeats_suffixes(pkg, orc, ctx):
+    # a periodic text: suffix LCPs up to the text length
+    text = (b"abcab" * 4000)[:19999] + b"\0"
+    chars = np.frombuffer(text, dtype=np.uint8).copy()
+    offs = np.arange(len(text), dtype=np.uint64)
+    perm, lcp = ctx.sort_host(chars, offs, lcp=True)
+    check_against_oracle(orc, chars, offs, perm, lcp)
+
+
+def test_lcp_optional(pkg, ctx):
+    chars, offs, _ = pkg.workloads.random_strings(20000, 0, 10, b"abc", 11)
+    p1, _ = ctx.sort_host(chars, offs, lcp=False)
+    p2, l2 = ctx.sort_host(chars, offs, lcp=True)
+    assert np.array_equal(canonical_ids(chars, offs, p1, l2), canonical_ids(chars, offs, p2, l2))
+
+
+def test_digits_config_full(pkg, orc, ctx):
+    chars, offs, nchars = pkg.workloads.digits(seed=1)
+    perm, lcp = ctx.sort_host(chars[:nchars], offs, lcp=True)
+    check_against_oracle(orc, chars[:nchars], offs, perm, lcp)
+
+
+def test_dna_suffix_config_full(pkg, orc, ctx):
+    chars, offs, n = pkg.workloads.dna_suffixes()
+    perm, lcp = ctx.sort_host(chars[: n], offs, lcp=True)
+    assert orc.check_permutation(perm)
+    assert orc.check_order(chars, offs, perm) == -1
+    assert orc.check_lcp32(chars, offs, perm, lcp) == -1
+
+
+def test_prefix_config_properties(pkg, orc, ctx):
+    # the 64 Mi-string workload at a quarter of its size keeps the test short;
+    # bench.py sorts the full size
+    chars, offs, nchars = pkg.workloads.prefixes(n=16 * 1024 * 1024)
+    perm, lcp = ctx.sort_host(chars[:nchars], offs, lcp=True)
+    assert orc.check_permutation(perm)
+    assert orc.check_order(chars, offs, perm) == -1
+    assert orc.check_lcp32(chars, offs, perm, lcp) == -1
+
+
+def test_prefix_small_vs_oracle(pkg, orc, ctx):
+    chars, offs, nchars = pkg.workloads.prefixes(n=400000, seed=12)
+    perm, lcp = ctx.sort_host(chars[:nchars], offs, lcp=True)
+    check_against_oracle(orc, chars[:nchars], offs, perm, lcp)
+
+
+def test_device_api(pkg, orc, ctx):
+    import torch
+    chars, offs, nchars = pkg.workloads.random_strings(50000, 0, 16, b"abcd", 13)
+    dc = torch.from_numpy(chars).cuda()
+    do = torch.from_numpy(offs.view(np.int64)).cuda()
+    dp = torch.empty(len(offs), dtype=torch.int32, device="cuda")
+    dl = torch.zeros(len(offs), dtype=torch.int32, device="cuda")
+    ctx.sort_device(dc, nchars, do, dp, dl)
+    perm = dp.cpu().numpy().view(np.uint32)
+    lcp = dl.cpu().numpy().view(np.uint32)
+    check_against_oracle(orc, chars, offs, perm, lcp)
+
+
+def test_pointer_array_dropins(pkg, orc):
+    """The three psstest contestant signatures on a raw pointer array."""
+    lib = pkg._native.gpu()
+    chars, offs, nchars = pkg.workloads.random_strings(30000, 0, 12, b"abc", 14)
+    buf = (C.c_ubyte * len(chars)).from_buffer_copy(chars.tobytes())
+    base = C.addressof(buf)
+    n = len(offs)
+    ptr_t = C.c_void_p * n
+    ids, rlcp = orc.sort_ids_lcp(chars, offs)
+    want = orc.sorted_strings(chars, offs, ids)
+
+    def got_sequence(ptrs):
+        got_offs = np.array([p - base for p in ptrs], dtype=np.uint64)
+        assert len(set(got_offs.tolist())) == n  # a permutation of the pointers
+        return orc.sorted_strings(chars, got_offs, np.arange(n))
+
+    ptrs = ptr_t(*[base + int(o) for o in offs])
+    lib.pssgpu_sort_strings(ptrs, n)
+    assert got_sequence(ptrs) == want
+
+    ptrs = ptr_t(*[base + int(o) for o in offs])
+    lcp = (C.c_size_t * n)()
+    lcp[0] = 42
+    lib.pssgpu_sort_strings_lcp(ptrs, lcp, n)
+    assert got_sequence(ptrs) == want
+    assert lcp[0] == 42
+    assert np.array_equal(np.array(lcp[1:], dtype=np.uint64), rlcp[1:])
+
+    ptrs = ptr_t(*[base + int(o) for o in offs])
+    lcp = (C.c_size_t * n)()
+    cache = (C.c_ubyte * n)()
+    lib.pssgpu_sort_strings_lcp_cache(ptrs, lcp, cache, n)
+    raw = chars.tobytes()
+    for i in range(1, n, 97):
+        assert cache[i] == raw[ptrs[i] - base + lcp[i]]
+
+
+def test_suffix_pointer_array_dense_span(pkg, orc):
+    """Overlapping suffix pointers (psstest --suffix) take the dense-span path."""
+    lib = pkg._native.gpu()
+    text = pkg.workloads.dna_text(length=20000, seed=15)
+    buf = (C.c_ubyte * len(text)).from_buffer_copy(text.tobytes())
+    base = C.addressof(buf)
+    n = 20001
+    ptrs = (C.c_void_p * n)(*[base + i for i in range(n)])
+    assert pkg.sort_pointer_array(ptrs, n) == 0
+    sa = np.array([p - base for p in ptrs], dtype=np.uint64)
+    offs = np.arange(n, dtype=np.uint64)
+    assert orc.check_order(text, offs, sa.astype(np.uint32)) == -1
+
+
+def test_errors_are_status_codes(pkg, ctx):
+    chars = np.frombuffer(b"abc", dtype=np.uint8).copy()  # no terminating NUL
+    with pytest.raises(pkg.SortError) as e:
+        ctx.sort_host(chars, np.zeros(1, np.uint64))
+    assert e.value.status == 1
+    chars = np.frombuffer(b"ab\0", dtype=np.uint8).copy()
+    with pytest.raises(pkg.SortError) as e:
+        ctx.sort_host(chars, np.array([0, 7], np.uint64))  # offset outside the arena
+    assert e.value.status == 1
+    # the context stays usable after an error
+    perm, _ = ctx.sort_host(np.frombuffer(b"b\0a\0", np.uint8).copy(), np.array([0, 2], np.uint64))
+    assert perm.tolist() == [1, 0]

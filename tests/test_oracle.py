@@ -1,0 +1,95 @@
+"""CPU tests: the oracle restatement is pinned against the reference pS5
+(golden fixtures generated from it, and the compiled reference itself where
+it is present), unit oracles for key extraction and classification, and the
+checkers catch planted mistakes."""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from golden_util import canonical_ids
+
+GOLDEN = sorted((Path(__file__).parent / "golden").glob("*.npz"))
+
+
+def load(path):
+    z = np.load(path)
+    return z["chars"], z["offs"], z["ids"], z["lcp"]
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[p.stem for p in GOLDEN])
+def test_restatement_matches_golden(orc, path):
+    chars, offs, gids, glcp = load(path)
+    ids, lcp = orc.sort_ids_lcp(chars, offs)
+    assert np.array_equal(canonical_ids(chars, offs, ids, lcp), gids)
+    assert np.array_equal(lcp[1:], glcp[1:])
+    assert glcp[0] == 42  # the reference never writes lcp[0]
+
+
+def test_golden_set_present():
+    names = {p.stem for p in GOLDEN}
+    assert {"edge_mixed", "digits_256k", "alpha_ab", "prefix_30k", "dna_suffix_64k",
+            "highbyte_long"} <= names
+
+
+@pytest.mark.parametrize("seed,alpha,lmax", [(1, b"ab", 12), (2, b"0123456789", 40),
+                                             (3, bytes(range(1, 256)), 20)])
+def test_restatement_matches_reference_run(pkg, orc, seed, alpha, lmax):
+    if not orc.ref_available():
+        pytest.skip("reference pS5 not built here")
+    chars, offs, _ = pkg.workloads.random_strings(40000, 0, lmax, alpha, seed)
+    ids, lcp = orc.sort_ids_lcp(chars, offs)
+    rids, rlcp = orc.ref_sort(chars, offs, threads=4, lcp=True)
+    assert np.array_equal(canonical_ids(chars, offs, ids, lcp),
+                          canonical_ids(chars, offs, rids, rlcp))
+    assert np.array_equal(lcp[1:], rlcp[1:])
+    assert rlcp[0] == 42
+
+
+def test_key_extraction_matches_reference(pkg, orc):
+    if not orc.ref_available():
+        pytest.skip("reference pS5 not built here")
+    chars, offs, _ = pkg.workloads.random_strings(2000, 0, 30, b"\x01a\xff", seed=4)
+    rng = np.random.default_rng(0)
+    for i in rng.integers(0, len(offs), 500):
+        for depth in (0, 1, 3, 7, 8, 13):
+            ln = chars.tobytes().index(b"\0", int(offs[i])) - int(offs[i])
+            if depth > ln:
+                continue
+            assert orc.get_uint64(chars, offs[i], depth) == orc.ref_get_uint64(chars, offs[i], depth)
+
+
+def test_classification_matches_reference_find_bkt(orc):
+    if not orc.ref_available():
+        pytest.skip("reference pS5 not built here")
+    rng = np.random.default_rng(5)
+    spl = np.sort(rng.integers(0, 2**63, 1023, dtype=np.uint64) * np.uint64(2))
+    spl[100:110] = spl[100]  # duplicated splitters
+    keys = np.concatenate([rng.integers(0, 2**63, 5000, dtype=np.uint64) * np.uint64(2),
+                           spl[::7], spl[::11] + np.uint64(1), np.array([0, 2**64 - 1], np.uint64)])
+    assert np.array_equal(orc.classify(spl, keys), orc.ref_find_bkt(spl, keys))
+
+
+def test_checkers_catch_planted_mistakes(pkg, orc):
+    chars, offs, _ = pkg.workloads.random_strings(5000, 1, 10, b"abcd", seed=6)
+    ids, lcp = orc.sort_ids_lcp(chars, offs)
+    assert orc.check_order(chars, offs, ids) == -1
+    assert orc.check_permutation(ids)
+    assert orc.check_lcp32(chars, offs, ids, lcp.astype(np.uint32)) == -1
+    bad = ids.copy()
+    bad[[10, 4000]] = bad[[4000, 10]]
+    assert orc.check_order(chars, offs, bad) != -1
+    dup = ids.copy()
+    dup[3] = dup[4]
+    assert not orc.check_permutation(dup)
+    badl = lcp.astype(np.uint32).copy()
+    badl[77] += 1
+    assert orc.check_lcp32(chars, offs, ids, badl) == 77
+
+
+def test_distinguishing_prefix(pkg, orc):
+    chars, offs = pkg.pack_strings([b"abc", b"abd", b"b", b"ba"])
+    ids = orc.sort_ids(chars, offs)
+    d, s = orc.dprefix(chars, offs, ids)
+    assert s == 2 + 0 + 1  # lcp(abc,abd)=2, lcp(abd,b)=0, lcp(b,ba)=1
+    assert d > 0

@@ -1,0 +1,59 @@
+"""CPU tests of the host logic: the seeded workload generators have the
+documented shapes and are deterministic, and the algorithmic-byte model
+matches a hand count."""
+import numpy as np
+
+from golden_util import string_lengths
+
+
+def test_digits_shape(pkg):
+    chars, offs, nchars = pkg.workloads.digits(seed=1)
+    n = len(offs)
+    assert 480_000 < n < 495_000
+    assert nchars <= 10 * 1024 * 1024
+    lens = string_lengths(chars[:nchars + 1], offs)
+    assert lens.min() >= 1 and lens.max() <= 40
+    body = chars[:nchars]
+    assert set(np.unique(body).tolist()) <= set(range(48, 58)) | {0}
+    c2, o2, n2 = pkg.workloads.digits(seed=1)
+    assert n2 == nchars and np.array_equal(c2, chars) and np.array_equal(o2, offs)
+
+
+def test_prefix_shape(pkg):
+    chars, offs, nchars, ids = pkg.workloads.prefixes(n=200000, seed=2, with_ids=True)
+    lens = string_lengths(chars, offs)
+    assert lens.min() >= 56 and lens.max() <= 72
+    counts = np.bincount(ids, minlength=4096)
+    h = np.sum(np.arange(1, 4097, dtype=np.float64) ** -1.1)
+    assert abs(counts[0] / len(ids) - 1 / h) < 0.01
+    assert len(np.unique(ids)) > 3000
+
+
+def test_dna_text(pkg):
+    t = pkg.workloads.dna_text(length=1 << 20, seed=3)
+    assert t[1 << 20] == 0
+    assert set(np.unique(t[: 1 << 20]).tolist()) == {65, 67, 71, 84}
+    t2 = pkg.workloads.dna_text(length=1 << 20, seed=3)
+    assert np.array_equal(t, t2)
+
+
+def test_random_strings_deterministic(pkg):
+    a = pkg.workloads.random_strings(1000, 0, 9, b"xyz", seed=1)
+    b = pkg.workloads.random_strings(1000, 0, 9, b"xyz", seed=1)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
+def test_alg_bytes_hand_count(pkg):
+    # 40 strings tied at depth 0 (one group > 32) splitting into singletons
+    lcp = np.zeros(40, np.uint32)
+    r = pkg.workloads.alg_bytes(lcp, T=32)
+    assert r["rounds"] == 52 * 40
+    # every string enters the base case at depth 8 and needs 1 char: none left
+    assert r["base"] == 40 * 12
+    assert r["total"] == 52 * 40 + 40 * 12 + 8 * 40
+    # a group of 10 enters the base case at depth 0 and needs lcp+1 chars
+    lcp = np.array([0, 3, 3, 5, 0, 0, 0, 0, 0, 0], np.uint32)
+    r = pkg.workloads.alg_bytes(lcp, T=32)
+    need = [4, 4, 6, 6, 1, 1, 1, 1, 1, 1]
+    assert r["rounds"] == 0
+    assert r["base"] == sum(12 + x for x in need)

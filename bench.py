@@ -1,0 +1,340 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 string sample sort.
+
+Workload: 64 Mi strings, each one of 4096 random 48-char prefixes ('a'..'z',
+picked Zipf s=1.1 by rank) followed by a suffix of uniform length 8..24 over
+'a'..'z' (about 4.36 GB of chars, mean LCP ~50), generated seeded on the host.
+One step = one full plain sort (the pS5-Unroll contestant's job) of that
+instance.
+
+  value      sorted char GB/s with the arena resident in HBM (CUDA events on
+             the launching stream, max over ranks; inputs are 4.4 GB > L2)
+  e2e        the same metric through the C ABI with host buffers: the H2D copy
+             of arena + offsets from pinned memory and the D2H copy of the
+             permutation are inside every timed step
+  roofline   the kernel class with the largest device time: its algorithmic
+             bytes / its summed event time against the measured HBM copy
+             bandwidth; roofline_sort does the same for the whole sort with
+             the method's algorithmic bytes computed from the LCP array
+  cpu_baseline  the reference pS5 (compiled from the reference sources) on a
+             bounded sample of the same workload, all host threads
+
+--impl reference times the reference pS5 alone on the host cores (rank 0).
+With N GPUs (torchrun) every rank sorts its own instance (weak scaling; no
+collective is needed by the sort).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "sorted char GB/s"
+N_DEFAULT = 64 * 1024 * 1024
+SEED = 2
+CPU_SAMPLE = 8 * 1024 * 1024
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--n", type=int, default=N_DEFAULT, help="strings per instance")
+    p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--cpu-sample", type=int, default=CPU_SAMPLE)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def workload_config(n: int, nchars: int) -> dict:
+    return {"workload": "prefixes-64Mi" if n == N_DEFAULT else f"prefixes-{n}",
+            "strings": n, "chars": nchars, "prefixes": 4096, "prefix_len": 48,
+            "zipf_s": 1.1, "suffix_len": "U[8,24]", "alphabet": "a-z", "seed": SEED,
+            "l2": "inputs larger than L2 (126 MB)", "lcp_output": False}
+
+
+def measured_peak() -> tuple:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples of one GPU during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", str(self.device)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        sms, maxs, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sms.append(float(f[1]))
+                maxs.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sms) if sms else None,
+                "sm_max_mhz": max(maxs) if maxs else None,
+                "samples": len(sms), "reasons": sorted(reasons)}
+
+
+def pinned_alloc(torch):
+    def alloc(nbytes, dtype):
+        t = torch.empty(int(nbytes), dtype=torch.uint8, pin_memory=True)
+        return t.numpy().view(dtype)
+    return alloc
+
+
+def cpu_baseline(n_sample: int) -> dict:
+    """Reference pS5 (parallel_sample_sortBTCUI) on the first n_sample strings
+    of the same generator, all host threads, best of 3."""
+    from oracle import oracle as orc
+    import __graft_entry__
+    pkg = __graft_entry__.load_package()
+    if not orc.ref_available():
+        return {"value": None, "unit": "GB/s", "cores": os.cpu_count(), "kind": "reference",
+                "sample": "oracle/_ref/libps5ref.so not built"}
+    chars, offs, nchars = pkg.workloads.prefixes(n=n_sample, seed=SEED)
+    threads = os.cpu_count()
+    lib = orc.ref_lib()
+    lib.ps5ref_set_threads(threads)
+    base = orc.ref_pointer_array(chars, offs)
+    times = []
+    for _ in range(3):
+        ptrs = base.copy()
+        t0 = time.perf_counter()
+        lib.ps5ref_sort(ptrs.ctypes.data, n_sample)
+        times.append(time.perf_counter() - t0)
+    t = min(times)
+    return {"value": nchars / t / 1e9, "unit": "GB/s", "cores": threads, "kind": "reference",
+            "sample": f"first {n_sample} strings of the same generator ({nchars} chars), "
+                      f"pS5-Unroll (parallel_sample_sortBTCUI) best of 3: {t * 1e3:.1f} ms",
+            "strings_per_s": n_sample / t}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle as orc
+    import __graft_entry__
+    pkg = __graft_entry__.load_package()
+    n = args.cpu_sample
+    chars, offs, nchars = pkg.workloads.prefixes(n=n, seed=SEED)
+    if not orc.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/libps5ref.so (reference pS5 built from its sources) missing"}))
+        return
+    threads = os.cpu_count()
+    lib = orc.ref_lib()
+    lib.ps5ref_set_threads(threads)
+    base = orc.ref_pointer_array(chars, offs)
+    for _ in range(args.warmup):
+        ptrs = base.copy()
+        lib.ps5ref_sort(ptrs.ctypes.data, n)
+    times = []
+    for _ in range(args.steps):
+        ptrs = base.copy()
+        t0 = time.perf_counter()
+        lib.ps5ref_sort(ptrs.ctypes.data, n)
+        times.append(time.perf_counter() - t0)
+    t = sum(times) / len(times)
+    value = nchars / t / 1e9
+    cfg = workload_config(args.n, None)
+    cfg.update({"sample_strings": n, "sample_chars": nchars})
+    line = {
+        "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic", "config": cfg, "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": "GB/s", "cores": threads, "kind": "reference",
+                         "sample": f"first {n} strings of the workload generator ({nchars} chars), "
+                                   "pS5-Unroll (parallel_sample_sortBTCUI) from the reference "
+                                   "sources, every host thread"},
+        "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+    import __graft_entry__
+    pkg = __graft_entry__.load_package()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def allmax(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def allsum(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    n = args.n
+    alloc = pinned_alloc(torch)
+    h_chars, h_offs, nchars = pkg.workloads.prefixes(n=n, seed=SEED + rank, alloc=alloc)
+    ctx = pkg.Context(local)
+    stream = torch.cuda.current_stream()
+    d_chars = torch.from_numpy(h_chars).cuda(non_blocking=True)
+    d_offs = torch.from_numpy(h_offs.view(np.int64)).cuda(non_blocking=True)
+    d_perm = torch.empty(n, dtype=torch.int32, device="cuda")
+    d_lcp = torch.empty(n, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+
+    def step(lcp=None):
+        ctx.sort_device(d_chars, nchars, d_offs, d_perm, lcp, stream=stream)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    # untimed: one LCP-emitting sort for the method's algorithmic bytes
+    step(d_lcp)
+    lcp_host = d_lcp.cpu().numpy().view(np.uint32)
+    model = pkg.workloads.alg_bytes(lcp_host)
+
+    ctx.set_profile(True)
+    clocks = Clocks(local)
+    clocks.start()
+    time.sleep(0.3)
+    kstats = {}
+    launches = 0
+    barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+        for k in ctx.kernel_stats():
+            a = kstats.setdefault(k["name"], {"launches": 0, "strings": 0, "alg_bytes": 0, "ms": 0.0})
+            for f in ("launches", "strings", "alg_bytes", "ms"):
+                a[f] += k[f]
+        launches += ctx.stats()["kernel_launches"]
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ctx.set_profile(False)
+    ms = ev0.elapsed_time(ev1) / args.steps
+    ms_max = allmax(ms)
+    total_chars = allsum(float(nchars))
+    value = total_chars / (ms_max / 1e3) / 1e9
+
+    # end to end through the C ABI: host arena in, host permutation out
+    h_perm = alloc(4 * n, np.uint32)
+    ctx.sort_host(h_chars[:nchars], h_offs, lcp=False, out_perm=h_perm)  # warm
+    e2e_times = []
+    for _ in range(args.e2e_steps):
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.sort_host(h_chars[:nchars], h_offs, lcp=False, out_perm=h_perm)
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_s = allmax(sum(e2e_times) / max(len(e2e_times), 1))
+    e2e_value = total_chars / e2e_s / 1e9 if e2e_s > 0 else None
+    del h_perm
+
+    peak, peak_kind = measured_peak()
+    dom = max(kstats.items(), key=lambda kv: kv[1]["ms"])
+    dom_name, d = dom
+    achieved = d["alg_bytes"] / (d["ms"] / 1e3) / 1e9 if d["ms"] > 0 else 0.0
+    sort_achieved = model["total"] / (ms / 1e3) / 1e9
+    tot_ms = sum(v["ms"] for v in kstats.values())
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(min(args.cpu_sample, n))
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world,
+            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms_max,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic", "config": workload_config(n, nchars),
+            "strings_per_s": world * n / (ms_max / 1e3),
+            "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": nchars + 8 * n,
+                    "d2h_bytes_per_step": 4 * n, "ms_per_step": e2e_s * 1e3},
+            "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                         "peak_kind": peak_kind,
+                         "alg_bytes_per_launch": d["alg_bytes"] / max(d["launches"], 1),
+                         "ms_per_launch": d["ms"] / max(d["launches"], 1),
+                         "share_of_device_time": d["ms"] / tot_ms if tot_ms else None},
+            "roofline_sort": {"alg_bytes": model["total"], "achieved": sort_achieved,
+                              "frac": sort_achieved / peak, "max_round": model["max_round"]},
+            "kernels": {k: {"ms_per_step": v["ms"] / args.steps,
+                            "launches_per_step": v["launches"] / args.steps,
+                            "gb_s": v["alg_bytes"] / (v["ms"] / 1e3) / 1e9 if v["ms"] else None}
+                        for k, v in kstats.items()},
+            "gpu_launches": launches,
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

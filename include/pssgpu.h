@@ -72,6 +72,21 @@ typedef struct pssgpu_stats {
 } pssgpu_stats;
 int pssgpu_ctx_stats(pssgpu_ctx* ctx, pssgpu_stats* out);
 
+/* Per-kernel-class figures of the last sort: launches, strings processed,
+ * algorithmic bytes (per-string model: key gather 4 id + 8 chars + 8 key,
+ * classify 8 key, scatter 12 + 12, base case 12 + output) and, in profile
+ * mode, summed device time from CUDA events around each class. Returns the
+ * number of entries written (at most max), or a negative status. */
+typedef struct pssgpu_kernel_stats {
+    char name[16];
+    uint32_t launches;
+    uint64_t strings;
+    uint64_t alg_bytes;
+    double ms;
+} pssgpu_kernel_stats;
+int pssgpu_ctx_set_profile(pssgpu_ctx* ctx, int on);
+int pssgpu_ctx_kernel_stats(pssgpu_ctx* ctx, pssgpu_kernel_stats* out, int max);
+
 /* ---- arena sorts ---------------------------------------------------------
  * chars[0, nchars) holds the strings; string i starts at chars + offs[i] and
  * ends at its first NUL, which must lie inside the arena (chars[nchars-1]

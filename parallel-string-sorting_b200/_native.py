@@ -24,6 +24,8 @@ GPU_SIGNATURES = {
     "pssgpu_ctx_destroy": (None, [C.c_void_p]),
     "pssgpu_workspace_bytes": (C.c_uint64, [C.c_uint64]),
     "pssgpu_ctx_stats": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "pssgpu_ctx_set_profile": (C.c_int, [C.c_void_p, C.c_int]),
+    "pssgpu_ctx_kernel_stats": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     "pssgpu_sort_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64,
                                    C.c_void_p, C.c_void_p]),
     "pssgpu_sort_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64,
@@ -58,6 +60,16 @@ class PssStats(C.Structure):
         ("small_segments", C.c_uint64),
         ("boundaries", C.c_uint64),
         ("device_ms", C.c_float),
+    ]
+
+
+class PssKernelStats(C.Structure):
+    _fields_ = [
+        ("name", C.c_char * 16),
+        ("launches", C.c_uint32),
+        ("strings", C.c_uint64),
+        ("alg_bytes", C.c_uint64),
+        ("ms", C.c_double),
     ]
 
 

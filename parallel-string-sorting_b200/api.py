@@ -24,7 +24,7 @@ from typing import Optional, Sequence
 import numpy as np
 
 from . import _native
-from ._native import PssStats, STATUS_NAMES
+from ._native import PssKernelStats, PssStats, STATUS_NAMES
 
 
 class SortError(RuntimeError):
@@ -72,13 +72,33 @@ class Context:
         _check(_native.gpu().pssgpu_ctx_stats(self._h, C.byref(s)))
         return {f: getattr(s, f) for f, _ in PssStats._fields_}
 
-    def sort_host(self, chars: np.ndarray, offs: np.ndarray, lcp: bool = True):
-        """Sort the arena strings; returns (perm u32[n], lcp u32[n] or None)."""
+    def set_profile(self, on: bool) -> None:
+        """Time every kernel class with CUDA events (per-class totals in
+        kernel_stats())."""
+        _check(_native.gpu().pssgpu_ctx_set_profile(self._h, 1 if on else 0))
+
+    def kernel_stats(self) -> list:
+        arr = (PssKernelStats * 16)()
+        k = _native.gpu().pssgpu_ctx_kernel_stats(self._h, arr, 16)
+        if k < 0:
+            _check(-k)
+        return [{"name": arr[i].name.decode(), "launches": arr[i].launches,
+                 "strings": arr[i].strings, "alg_bytes": arr[i].alg_bytes, "ms": arr[i].ms}
+                for i in range(k)]
+
+    def sort_host(self, chars: np.ndarray, offs: np.ndarray, lcp: bool = True,
+                  out_perm: Optional[np.ndarray] = None, out_lcp: Optional[np.ndarray] = None):
+        """Sort the arena strings; returns (perm u32[n], lcp u32[n] or None).
+        out_perm / out_lcp may supply (pinned) result buffers."""
         chars = np.ascontiguousarray(chars, dtype=np.uint8)
         offs = np.ascontiguousarray(offs, dtype=np.uint64)
         n = offs.shape[0]
-        perm = np.empty(n, dtype=np.uint32)
-        lcp_a = np.zeros(n, dtype=np.uint32) if lcp else None
+        perm = np.empty(n, dtype=np.uint32) if out_perm is None else out_perm
+        if not lcp:
+            lcp_a = None
+        else:
+            lcp_a = np.zeros(n, dtype=np.uint32) if out_lcp is None else out_lcp
+        assert perm.dtype == np.uint32 and perm.shape[0] >= n and perm.flags.c_contiguous
         _check(_native.gpu().pssgpu_sort_host(self._h, _ptr(chars), chars.shape[0], _ptr(offs), n,
                                               _ptr(perm), _ptr(lcp_a)))
         return perm, lcp_a

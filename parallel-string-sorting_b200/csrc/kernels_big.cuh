@@ -62,8 +62,15 @@ __global__ void __launch_bounds__(1024) k_sample(Work w)
     uint32_t* bc = w.bcount + (size_t)s * MAX_BKT;
     for (int b = threadIdx.x; b < MAX_BKT; b += blockDim.x) bc[b] = 0;
     if (sg.meta & META_FINAL) {
-        if (threadIdx.x == 0) w.tree_bits[s] = 0;
+        if (threadIdx.x == 0) {
+            w.tree_bits[s] = 0;
+            atomicAdd(w.counters + C_P_FINAL, sg.size);
+        }
         return;
+    }
+    if (threadIdx.x == 0) {
+        atomicAdd(w.counters + C_P_BIG, sg.size);
+        if (!(sg.meta & META_VALID)) atomicAdd(w.counters + C_P_STALE, sg.size);
     }
     const uint32_t L = tree_bits_for(sg.size);
     const uint32_t k = (1u << L) - 1;
@@ -183,7 +190,10 @@ __global__ void __launch_bounds__(1024) k_bstart(Work w)
     block_scan_array<1024>(a, MAX_BKT, tmp);
     uint32_t* bs = w.bstart + (size_t)s * MAX_BKT;
     for (uint32_t b = threadIdx.x; b < MAX_BKT; b += 1024) bs[b] = a[b];
-    if (threadIdx.x == 0) w.bflags[s] = (uint8_t)one;
+    if (threadIdx.x == 0) {
+        w.bflags[s] = (uint8_t)one;
+        if (!one) atomicAdd(w.counters + C_P_SCATTER, sg.size);
+    }
 }
 
 // Decoupled look-back status word: epoch (16) | flag (2) | count (46).

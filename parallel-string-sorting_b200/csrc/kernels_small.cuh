@@ -185,6 +185,7 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_small(Work w, uint32_t nsmall
     const uint32_t m = sg.size, begin = sg.begin;
     const int buf = sg.meta & META_BUF;
     const uint32_t* gids = w.ids[buf];
+    if (threadIdx.x == 0) atomicAdd(w.counters + C_P_SMALL, m);
     if (sg.meta & META_FINAL) {
         for (uint32_t i = threadIdx.x; i < m; i += SMALL_THREADS) {
             w.perm[begin + i] = gids[begin + i];

@@ -85,6 +85,19 @@ static uint64_t workspace_bytes(const Sizes& s)
     return b;
 }
 
+// Kernel classes reported by pssgpu_ctx_kernel_stats.
+enum KClass { K_INIT = 0, K_SAMPLE, K_CLASSIFY, K_BSTART, K_SCATTER, K_CHILDREN, K_SMALL,
+              K_BOUNDARY, K_NCLASS };
+static const char* const kclass_name[K_NCLASS] = {
+    "init", "sample", "classify", "bstart", "scatter", "children", "small", "boundary"};
+
+struct KStat {
+    uint32_t launches = 0;
+    uint64_t strings = 0;
+    uint64_t alg_bytes = 0;
+    double ms = 0;
+};
+
 struct Ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -101,6 +114,37 @@ struct Ctx {
     unsigned char* io = nullptr;
     uint64_t io_bytes = 0;
     pssgpu_stats stats{};
+    // profile mode: events around every kernel class, per-class totals
+    bool profile = false;
+    cudaEvent_t kev[2 * K_NCLASS] = {};
+    KStat kstat[K_NCLASS];
+};
+
+// Record the start / end of a kernel class in profile mode.
+struct KTimer {
+    Ctx* c;
+    cudaStream_t st;
+    bool used[K_NCLASS] = {};
+    void begin(int k)
+    {
+        if (c->profile) { cudaEventRecord(c->kev[2 * k], st); used[k] = true; }
+    }
+    void end(int k)
+    {
+        if (c->profile) cudaEventRecord(c->kev[2 * k + 1], st);
+    }
+    // after a stream synchronisation
+    void collect()
+    {
+        if (!c->profile) return;
+        for (int k = 0; k < K_NCLASS; ++k) {
+            if (!used[k]) continue;
+            float ms = 0;
+            cudaEventElapsedTime(&ms, c->kev[2 * k], c->kev[2 * k + 1]);
+            c->kstat[k].ms += ms;
+            used[k] = false;
+        }
+    }
 };
 
 static int ensure_workspace(Ctx* c, uint64_t n)
@@ -180,14 +224,23 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
     w.perm = perm;
     w.lcp = lcp;
     pssgpu_stats stats{};
+    for (int k = 0; k < K_NCLASS; ++k) c->kstat[k] = KStat{};
+    KTimer kt{c, st};
+    const uint64_t out_bytes = lcp ? 8 : 4;  // perm (+ lcp) per string
     PSS_CUDA(cudaEventRecord(c->ev0, st));
     PSS_CUDA(cudaMemsetAsync(w.counters, 0, 4 * C_COUNT, st));
+    kt.begin(K_INIT);
     k_init<<<1184, 256, 0, st>>>(w);
     k_root<<<1, 1, 0, st>>>(w);
+    kt.end(K_INIT);
+    c->kstat[K_INIT].launches += 2;
+    c->kstat[K_INIT].strings += n;
+    c->kstat[K_INIT].alg_bytes += 12ull * n;  // offset read + id write
     stats.kernel_launches += 2;
     uint32_t* hc = c->host_counters;
     PSS_CUDA(cudaMemcpyAsync(hc, w.counters, 4 * C_COUNT, cudaMemcpyDeviceToHost, st));
     PSS_CUDA(cudaStreamSynchronize(st));
+    kt.collect();
     uint32_t nbig = hc[C_NBIG], nsmall = hc[C_NSMALL], ntiles = hc[C_NTILES];
     uint32_t err = hc[C_ERR];
     int cur = 0;
@@ -203,25 +256,60 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
         }
         PSS_CUDA(cudaMemsetAsync(w.counters + 3 * nxt, 0, 12, st));
         PSS_CUDA(cudaMemsetAsync(w.counters + C_TICKET, 0, 4, st));
+        PSS_CUDA(cudaMemsetAsync(w.counters + C_P_BIG, 0, 4 * (C_P_SMALL - C_P_BIG + 1), st));
         if (nsmall) {
+            kt.begin(K_SMALL);
             k_small<<<nsmall, SMALL_THREADS, sizeof(SmallSmem), st>>>(w, nsmall);
+            kt.end(K_SMALL);
+            c->kstat[K_SMALL].launches += 1;
             stats.kernel_launches += 1;
         }
         if (nbig) {
             if (ntiles > c->cap.tile_cap) return fail(PSSGPU_ECUDA, "tile capacity exceeded");
+            kt.begin(K_SAMPLE);
             k_tile_scan<<<1, 1024, 0, st>>>(w, nbig);
             k_sample<<<nbig, 1024, 0, st>>>(w);
+            kt.end(K_SAMPLE);
+            kt.begin(K_CLASSIFY);
             k_classify<<<ntiles, TILE_THREADS, 0, st>>>(w, nbig);
+            kt.end(K_CLASSIFY);
+            kt.begin(K_BSTART);
             k_bstart<<<nbig, 1024, 0, st>>>(w);
+            kt.end(K_BSTART);
+            kt.begin(K_SCATTER);
             k_scatter<<<ntiles, TILE_THREADS, sizeof(ScatterSmem), st>>>(w, nbig);
+            kt.end(K_SCATTER);
+            kt.begin(K_CHILDREN);
             k_children<<<nbig, 1024, 0, st>>>(w);
+            kt.end(K_CHILDREN);
+            c->kstat[K_SAMPLE].launches += 2;
+            c->kstat[K_CLASSIFY].launches += 1;
+            c->kstat[K_BSTART].launches += 1;
+            c->kstat[K_SCATTER].launches += 1;
+            c->kstat[K_CHILDREN].launches += 1;
             stats.kernel_launches += 6;
             stats.passes += 1;
-            stats.big_elements += (uint64_t)ntiles * TILE;
         }
         PSS_CUDA(cudaGetLastError());
         PSS_CUDA(cudaMemcpyAsync(hc, w.counters, 4 * C_COUNT, cudaMemcpyDeviceToHost, st));
         PSS_CUDA(cudaStreamSynchronize(st));
+        kt.collect();
+        {
+            // per-string algorithmic bytes of each kernel class: key gather
+            // 4 id + 8 chars + 8 key write; classify 8 key read; scatter
+            // 12 read + 12 write; base case 12 read + output
+            const uint64_t big = hc[C_P_BIG], stale = hc[C_P_STALE], fin = hc[C_P_FINAL];
+            const uint64_t sc = hc[C_P_SCATTER], sm = hc[C_P_SMALL];
+            stats.big_elements += big;
+            c->kstat[K_SAMPLE].strings += big;
+            c->kstat[K_CLASSIFY].strings += big + fin;
+            c->kstat[K_CLASSIFY].alg_bytes += 20 * stale + 8 * (big - stale) + (4 + out_bytes) * fin;
+            c->kstat[K_SCATTER].strings += sc;
+            c->kstat[K_SCATTER].alg_bytes += 24 * sc;
+            c->kstat[K_SMALL].strings += sm;
+            c->kstat[K_SMALL].alg_bytes += (12 + out_bytes) * sm;
+            c->kstat[K_CHILDREN].strings += big;
+        }
         nbig = hc[3 * nxt + C_NBIG];
         nsmall = hc[3 * nxt + C_NSMALL];
         ntiles = hc[3 * nxt + C_NTILES];
@@ -229,12 +317,21 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
         cur = nxt;
     }
     if (!err && lcp) {
+        kt.begin(K_BOUNDARY);
         k_boundary_lcp<<<1184, 256, 0, st>>>(w);
+        kt.end(K_BOUNDARY);
+        c->kstat[K_BOUNDARY].launches += 1;
         stats.kernel_launches += 1;
     }
     PSS_CUDA(cudaEventRecord(c->ev1, st));
     PSS_CUDA(cudaMemcpyAsync(hc, w.counters, 4 * C_COUNT, cudaMemcpyDeviceToHost, st));
     PSS_CUDA(cudaStreamSynchronize(st));
+    kt.collect();
+    if (lcp) {
+        // boundary (position, depth) 8 + two perm reads 8 + two keys 16 + lcp 4
+        c->kstat[K_BOUNDARY].strings += hc[C_NBND];
+        c->kstat[K_BOUNDARY].alg_bytes += 36ull * hc[C_NBND];
+    }
     PSS_CUDA(cudaGetLastError());
     err = hc[C_ERR];
     stats.small_segments = hc[C_SMALLSEGS];
@@ -245,6 +342,8 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
     return PSSGPU_OK;
 }
 
+static void ctx_destroy(Ctx* c);
+
 static int ctx_create(int device, Ctx** out)
 {
     int count = 0;
@@ -254,10 +353,13 @@ static int ctx_create(int device, Ctx** out)
     PSS_CUDA(cudaSetDevice(device));
     Ctx* c = new Ctx;
     c->device = device;
-    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
-        cudaHostAlloc((void**)&c->host_counters, 4 * C_COUNT, cudaHostAllocDefault) != cudaSuccess) {
-        delete c;
+    bool ok = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreate(&c->ev0) == cudaSuccess && cudaEventCreate(&c->ev1) == cudaSuccess &&
+              cudaHostAlloc((void**)&c->host_counters, 4 * C_COUNT, cudaHostAllocDefault) ==
+                  cudaSuccess;
+    for (int k = 0; ok && k < 2 * K_NCLASS; ++k) ok = cudaEventCreate(&c->kev[k]) == cudaSuccess;
+    if (!ok) {
+        ctx_destroy(c);
         return fail(PSSGPU_ECUDA, "stream/event/pinned allocation failed");
     }
     *out = c;
@@ -273,6 +375,8 @@ static void ctx_destroy(Ctx* c)
     if (c->host_counters) cudaFreeHost(c->host_counters);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
+    for (int k = 0; k < 2 * K_NCLASS; ++k)
+        if (c->kev[k]) cudaEventDestroy(c->kev[k]);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -433,6 +537,32 @@ int pssgpu_ctx_stats(pssgpu_ctx* ctx, pssgpu_stats* out)
     std::lock_guard<std::mutex> lk(c->mu);
     *out = c->stats;
     return PSSGPU_OK;
+}
+
+int pssgpu_ctx_set_profile(pssgpu_ctx* ctx, int on)
+{
+    if (!ctx) return fail(PSSGPU_EINVAL, "null context");
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->profile = on != 0;
+    return PSSGPU_OK;
+}
+
+int pssgpu_ctx_kernel_stats(pssgpu_ctx* ctx, pssgpu_kernel_stats* out, int max)
+{
+    if (!ctx || (!out && max > 0)) return -fail(PSSGPU_EINVAL, "null argument");
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    std::lock_guard<std::mutex> lk(c->mu);
+    int k = 0;
+    for (; k < K_NCLASS && k < max; ++k) {
+        memset(&out[k], 0, sizeof(out[k]));
+        strncpy(out[k].name, kclass_name[k], sizeof(out[k].name) - 1);
+        out[k].launches = c->kstat[k].launches;
+        out[k].strings = c->kstat[k].strings;
+        out[k].alg_bytes = c->kstat[k].alg_bytes;
+        out[k].ms = c->kstat[k].ms;
+    }
+    return k;
 }
 
 int pssgpu_sort_host(pssgpu_ctx* ctx, const uint8_t* chars, uint64_t nchars,

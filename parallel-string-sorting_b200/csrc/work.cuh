@@ -24,6 +24,12 @@ enum : int {
     C_TICKET = 7,     // scatter tile ticket
     C_ERR = 8,        // error bits
     C_SMALLSEGS = 9,  // statistics: segments finished by the small sorter
+    // per-pass statistics, reset every pass
+    C_P_BIG = 10,      // strings in big sample-sort segments
+    C_P_STALE = 11,    // of those, strings whose key was gathered this pass
+    C_P_FINAL = 12,    // strings copied out of big all-equal segments
+    C_P_SCATTER = 13,  // strings moved by the scatter
+    C_P_SMALL = 14,    // strings finished by the small sorter
     C_COUNT = 16
 };
 

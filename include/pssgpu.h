@@ -125,6 +125,29 @@ void pssgpu_sort_strings_lcp_cache(uint8_t** strings, uintptr_t* lcp,
 int pssgpu_sort_strings_status(unsigned char** strings, uintptr_t* lcp,
                                uint8_t* cache, size_t n);
 
+/* ---- allocation-free sort --------------------------------------------------
+ * No counterpart in the reference. Sorts at most PSSGPU_NOALLOC_MAX_STRINGS
+ * strings on the current device and allocates nothing: no cudaMalloc, no
+ * cudaFree, no allocating library call, no context. It exists for callers
+ * that cannot allocate device memory: a plugin inside a host application
+ * that owns all device memory through its own pool and forbids other
+ * allocations, a latency-critical path that cannot afford cudaMalloc's
+ * implicit device synchronisation, or a process whose device memory is
+ * already fully reserved. Inputs and outputs are caller-owned device buffers
+ * exactly as for pssgpu_sort_device; `stream` is a cudaStream_t (NULL: the
+ * default stream); the call returns after the sort has completed.
+ * Scratch is one file-scope device array of 8,272 bytes inside the library,
+ * held by every device that loads the library until the process exits. All
+ * calls share it: calls whose GPU work overlaps (other streams, other host
+ * threads) race on it, so the caller must serialise them. The first call on
+ * a device looks up the array's device address and raises the kernel's
+ * shared-memory limit; make that first call before any stream capture.
+ * More than PSSGPU_NOALLOC_MAX_STRINGS strings returns PSSGPU_EINVAL. */
+#define PSSGPU_NOALLOC_MAX_STRINGS 2048
+int pssgpu_sort_device_noalloc(const uint8_t* d_chars, uint64_t nchars,
+                               const uint64_t* d_offs, uint64_t n,
+                               uint32_t* d_perm, uint32_t* d_lcp, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -34,6 +34,8 @@ GPU_SIGNATURES = {
     "pssgpu_sort_strings_lcp": (None, [C.c_void_p, C.c_void_p, C.c_size_t]),
     "pssgpu_sort_strings_lcp_cache": (None, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t]),
     "pssgpu_sort_strings_status": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t]),
+    "pssgpu_sort_device_noalloc": (C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64,
+                                             C.c_void_p, C.c_void_p, C.c_void_p]),
 }
 
 WORK_SIGNATURES = {

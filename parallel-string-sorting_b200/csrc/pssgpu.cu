@@ -626,3 +626,105 @@ void pssgpu_sort_strings_lcp_cache(uint8_t** strings, uintptr_t* lcp, uint8_t* c
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free entry point.
+//
+// pssgpu_sort_device_noalloc sorts at most PSSGPU_NOALLOC_MAX_STRINGS strings
+// with the small-segment kernel and allocates nothing. Its scratch -- the id
+// buffer, the one segment descriptor and the counters that kernel uses -- is
+// the file-scope array below (8,272 bytes), which every device that loads this
+// library holds until the process exits. In host code the array's name is
+// only a host-side stand-in: kernels get the device address that
+// cudaGetSymbolAddress returns, looked up once per device with that device
+// current. Device code may name the array directly (k_noalloc_prep does).
+namespace pssgpu {
+
+struct NoAllocScratch {
+    uint32_t ids[PSSGPU_NOALLOC_MAX_STRINGS];
+    Seg seg;
+    uint32_t counters[C_COUNT];
+};
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocScratch)];
+
+// One block: clear the counters (the array keeps the previous call's
+// contents), write the identity ids and the single segment, check offsets.
+__global__ void k_noalloc_prep(const uint64_t* __restrict__ offs, uint64_t nchars, uint32_t n)
+{
+    NoAllocScratch* s = reinterpret_cast<NoAllocScratch*>(g_noalloc_scratch);
+    for (int i = threadIdx.x; i < C_COUNT; i += blockDim.x) s->counters[i] = 0;
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        s->ids[i] = i;
+        if (offs[i] >= nchars) atomicOr(&s->counters[C_ERR], ERR_OFFSET);
+    }
+    if (threadIdx.x == 0) s->seg = Seg{0u, n, 0u, 0u};
+}
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+static std::mutex g_noalloc_mu;
+static NoAllocScratch* g_noalloc_addr[NOALLOC_MAX_DEVICES];
+
+}  // namespace pssgpu
+
+// Error messages of this entry point are at most 15 characters, so setting
+// the thread's error string stays inside its inline buffer: failures do not
+// allocate either.
+extern "C" int pssgpu_sort_device_noalloc(const uint8_t* d_chars, uint64_t nchars,
+                                          const uint64_t* d_offs, uint64_t n, uint32_t* d_perm,
+                                          uint32_t* d_lcp, void* stream)
+{
+    if (n > PSSGPU_NOALLOC_MAX_STRINGS) return fail(PSSGPU_EINVAL, "n over max 2048");
+    if (n == 0) return PSSGPU_OK;
+    if (!d_chars || !d_offs || !d_perm) return fail(PSSGPU_EINVAL, "null buffer");
+    if (nchars == 0) return fail(PSSGPU_EINVAL, "empty arena");
+    if (((uintptr_t)d_chars & 7) != 0) return fail(PSSGPU_EINVAL, "unaligned arena");
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES)
+        return fail(PSSGPU_ENODEV, "no device");
+    NoAllocScratch* scratch;
+    {
+        // set-up, once per device, with that device current
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_addr[dev]) {
+            void* p = nullptr;
+            if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p)
+                return fail(PSSGPU_ECUDA, "symbol lookup");
+            if (cudaFuncSetAttribute(k_small, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sizeof(SmallSmem)) != cudaSuccess)
+                return fail(PSSGPU_ECUDA, "smem limit");
+            g_noalloc_addr[dev] = static_cast<NoAllocScratch*>(p);
+        }
+        scratch = g_noalloc_addr[dev];
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    uint8_t last = 1;
+    if (cudaMemcpyAsync(&last, d_chars + nchars - 1, 1, cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return fail(PSSGPU_ECUDA, "CUDA error");
+    if (last != 0) return fail(PSSGPU_EINVAL, "no NUL at end");
+    Work w{};
+    w.chars = d_chars;
+    w.nchars = nchars;
+    w.offs = d_offs;
+    w.n = (uint32_t)n;
+    w.ids[0] = w.ids[1] = scratch->ids;
+    w.perm = d_perm;
+    w.lcp = d_lcp;
+    w.counters = scratch->counters;
+    w.small[0] = w.small[1] = &scratch->seg;
+    w.cur = 0;
+    k_noalloc_prep<<<1, SMALL_THREADS, 0, st>>>(d_offs, nchars, (uint32_t)n);
+    k_small<<<1, SMALL_THREADS, sizeof(SmallSmem), st>>>(w, 1u);
+    uint32_t err = 0;
+    if (cudaGetLastError() != cudaSuccess ||
+        cudaMemcpyAsync(&err, scratch->counters + C_ERR, 4, cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return fail(PSSGPU_ECUDA, "CUDA error");
+    if (err & ERR_OFFSET) return fail(PSSGPU_EINVAL, "bad offset");
+    if (err) return fail(PSSGPU_ECUDA, "device error");
+    return PSSGPU_OK;
+}

@@ -136,7 +136,7 @@ int pssgpu_sort_strings_status(unsigned char** strings, uintptr_t* lcp,
  * already fully reserved. Inputs and outputs are caller-owned device buffers
  * exactly as for pssgpu_sort_device; `stream` is a cudaStream_t (NULL: the
  * default stream); the call returns after the sort has completed.
- * Scratch is one file-scope device array of 8,272 bytes inside the library,
+ * Scratch is one file-scope device array of 8,336 bytes inside the library,
  * held by every device that loads the library until the process exits. All
  * calls share it: calls whose GPU work overlaps (other streams, other host
  * threads) race on it, so the caller must serialise them. The first call on

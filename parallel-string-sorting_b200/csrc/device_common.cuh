@@ -23,11 +23,16 @@ struct Seg {
     uint32_t begin;  // first position in the permutation arrays
     uint32_t size;   // number of strings
     uint32_t depth;  // chars known to be shared (FINAL: the LCP inside)
-    uint32_t meta;   // bit0 buffer, bit1 keys valid, bit2 final (all equal)
+    uint32_t meta;   // META_* bits
 };
 static_assert(sizeof(Seg) == 16, "Seg layout");
 
-enum : uint32_t { META_BUF = 1u, META_VALID = 2u, META_FINAL = 4u };
+enum : uint32_t {
+    META_BUF = 1u,    // which ping-pong buffer holds the segment
+    META_VALID = 2u,  // keys at `depth` are cached in keys[buf]
+    META_FINAL = 4u,  // all strings equal: copy out, LCP inside = depth
+    META_NOTIE = 8u,  // skip the common-prefix jump (it made no progress)
+};
 
 __device__ __forceinline__ uint64_t bswap64(uint64_t x)
 {

@@ -11,6 +11,13 @@
 //                (hpp:1464-1490)
 //   k_children   distribute_finished: next segments, finished buckets, split
 //                boundaries for the LCP array (hpp:1492-1584, 311-396)
+//
+// A segment whose samples are all equal takes the common-prefix jump instead
+// of a classification: k_classify measures, for every string, the chars it
+// shares with the segment's first string beyond the current depth; the
+// segment then continues at depth + min (or is finished when all strings are
+// equal). pS5 advances such a tied group 8 bytes per step (hpp:1527-1528,
+// 1555-1556); the jump reaches the same depth in one pass.
 #pragma once
 
 #include "block_util.cuh"
@@ -31,15 +38,15 @@ __device__ __forceinline__ int find_tile_seg(const uint32_t* tile_start, int nbi
 
 __device__ __forceinline__ uint32_t tree_bits_for(uint32_t m)
 {
-    // about 32 strings per '<' bucket, at most pS5's 10 tree levels
+    // about 16 strings per '<' bucket, at most pS5's 10 tree levels
     const int lg = 31 - __clz((int)m);
-    return (uint32_t)min(MAX_TREE_BITS, max(1, lg - 5));
+    return (uint32_t)min(MAX_TREE_BITS, max(1, lg - 4));
 }
 
 __global__ void k_tile_scan(Work w, uint32_t nbig)
 {
     __shared__ uint32_t tmp[32];
-    const Seg* big = w.big[w.cur];
+    const Seg* big = w.list[L_BIG][w.cur];
     const uint32_t per = (nbig + blockDim.x - 1) / blockDim.x;
     const uint32_t lo = min(threadIdx.x * per, nbig), hi = min(lo + per, nbig);
     uint32_t s = 0;
@@ -58,7 +65,7 @@ __global__ void __launch_bounds__(1024) k_sample(Work w)
 {
     __shared__ uint64_t samp[2 << MAX_TREE_BITS];
     const int s = blockIdx.x;
-    const Seg sg = w.big[w.cur][s];
+    const Seg sg = w.list[L_BIG][w.cur][s];
     uint32_t* bc = w.bcount + (size_t)s * MAX_BKT;
     for (int b = threadIdx.x; b < MAX_BKT; b += blockDim.x) bc[b] = 0;
     if (sg.meta & META_FINAL) {
@@ -67,10 +74,6 @@ __global__ void __launch_bounds__(1024) k_sample(Work w)
             atomicAdd(w.counters + C_P_FINAL, sg.size);
         }
         return;
-    }
-    if (threadIdx.x == 0) {
-        atomicAdd(w.counters + C_P_BIG, sg.size);
-        if (!(sg.meta & META_VALID)) atomicAdd(w.counters + C_P_STALE, sg.size);
     }
     const uint32_t L = tree_bits_for(sg.size);
     const uint32_t k = (1u << L) - 1;
@@ -97,6 +100,20 @@ __global__ void __launch_bounds__(1024) k_sample(Work w)
             __syncthreads();
         }
     }
+    if (samp[0] == samp[S - 1] && !(sg.meta & META_NOTIE)) {
+        // all samples equal: most likely one tied group -> common-prefix jump
+        if (threadIdx.x == 0) {
+            w.tree_bits[s] = TREE_TIE;
+            w.jump_min[s] = 0xFFFFFFFFu;
+            w.jump_diff[s] = 0;
+            atomicAdd(w.counters + C_P_TIE, sg.size);
+        }
+        return;
+    }
+    if (threadIdx.x == 0) {
+        atomicAdd(w.counters + C_P_BIG, sg.size);
+        if (!valid) atomicAdd(w.counters + C_P_STALE, sg.size);
+    }
     // splitters: every second sample; level-order tree over them
     uint64_t* spl = w.spl + (size_t)s * 1024;
     uint64_t* tree = w.tree + (size_t)s * 1024;
@@ -110,27 +127,72 @@ __global__ void __launch_bounds__(1024) k_sample(Work w)
     if (threadIdx.x == 0) w.tree_bits[s] = (uint8_t)L;
 }
 
+// Chars string `id` shares with the base string (at arena offset boff, both
+// from depth d on); *differs is set when the two strings are not equal.
+// Gives up (returning a value > stop) once the shared length exceeds `stop`,
+// which then cannot lower the segment minimum.
+__device__ __forceinline__ uint32_t shared_chars(const Work& w, uint64_t boff, uint32_t id,
+                                                 uint32_t d, uint32_t stop, bool* differs)
+{
+    const uint64_t o = __ldg(w.offs + id) + d;
+    for (uint32_t c = 0;; ++c) {
+        if (8u * c > stop) return 8u * c;
+        const uint64_t ka = load_key(w.chars, w.nchars, boff + 8ull * c);
+        const uint64_t kb = load_key(w.chars, w.nchars, o + 8ull * c);
+        if (ka != kb) {
+            *differs = true;
+            return 8u * c + lcp_key_type(ka, kb);
+        }
+        if (key_terminated(ka)) return 8u * c + lcp_key_depth(ka);
+    }
+}
+
 // One block per tile of a big segment: gather keys if stale, classify,
 // store bucket ids, add the tile histogram into the segment's counts.
-// Tiles of finished (all-equal) segments copy ids and LCPs to the output.
+// Tiles of finished (all-equal) segments copy ids and LCPs to the output;
+// tiles of jump segments measure the common prefix.
 __global__ void __launch_bounds__(TILE_THREADS) k_classify(Work w, uint32_t nbig)
 {
     __shared__ uint64_t tree[1024];
     __shared__ uint32_t hist[MAX_BKT];
+    __shared__ uint32_t best;
+    __shared__ uint32_t anydiff;
     const uint32_t t = blockIdx.x;
     const int s = find_tile_seg(w.tile_start, nbig, t);
-    const Seg sg = w.big[w.cur][s];
+    const Seg sg = w.list[L_BIG][w.cur][s];
     const uint32_t lo = sg.begin + (t - w.tile_start[s]) * TILE;
     const uint32_t hi = min(lo + TILE, sg.begin + sg.size);
     const int buf = sg.meta & META_BUF;
+    const uint32_t* ids = w.ids[buf];
     if (sg.meta & META_FINAL) {
         for (uint32_t p = lo + threadIdx.x; p < hi; p += TILE_THREADS) {
-            w.perm[p] = w.ids[buf][p];
+            w.perm[p] = ids[p];
             if (w.lcp && p > sg.begin) w.lcp[p] = sg.depth;
         }
         return;
     }
     const uint32_t L = w.tree_bits[s];
+    if (L == TREE_TIE) {
+        if (threadIdx.x == 0) {
+            best = *((volatile uint32_t*)(w.jump_min + s));
+            anydiff = 0;
+        }
+        __syncthreads();
+        const uint64_t boff = __ldg(w.offs + ids[sg.begin]) + sg.depth;
+        bool differs = false;
+        for (uint32_t p = lo + threadIdx.x; p < hi; p += TILE_THREADS) {
+            const uint32_t stop = *((volatile uint32_t*)&best);
+            const uint32_t l = shared_chars(w, boff, ids[p], sg.depth, stop, &differs);
+            if (l < stop) atomicMin(&best, l);
+        }
+        if (differs) anydiff = 1;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            atomicMin(w.jump_min + s, best);
+            if (anydiff) atomicOr(w.jump_diff + s, 1u);
+        }
+        return;
+    }
     const uint32_t k = (1u << L) - 1;
     const uint32_t B = 2 * k + 1;
     const uint64_t* gtree = w.tree + (size_t)s * 1024;
@@ -138,7 +200,6 @@ __global__ void __launch_bounds__(TILE_THREADS) k_classify(Work w, uint32_t nbig
     for (uint32_t b = threadIdx.x; b < B; b += TILE_THREADS) hist[b] = 0;
     __syncthreads();
     const bool valid = sg.meta & META_VALID;
-    const uint32_t* ids = w.ids[buf];
     uint64_t* keys = w.keys[buf];
     for (uint32_t p = lo + threadIdx.x; p < hi; p += TILE_THREADS) {
         uint64_t key;
@@ -167,6 +228,11 @@ __global__ void __launch_bounds__(TILE_THREADS) k_classify(Work w, uint32_t nbig
         if (hist[b]) atomicAdd(bc + b, hist[b]);
 }
 
+__device__ __forceinline__ bool classified(uint8_t L)
+{
+    return L != 0 && L != TREE_TIE;
+}
+
 // Bucket starts (exclusive prefix over buckets) and the one-bucket test.
 __global__ void __launch_bounds__(1024) k_bstart(Work w)
 {
@@ -174,9 +240,9 @@ __global__ void __launch_bounds__(1024) k_bstart(Work w)
     __shared__ uint32_t tmp[32];
     __shared__ int one;
     const int s = blockIdx.x;
-    const Seg sg = w.big[w.cur][s];
-    if (sg.meta & META_FINAL) return;
-    const uint32_t L = w.tree_bits[s];
+    const Seg sg = w.list[L_BIG][w.cur][s];
+    const uint8_t L = w.tree_bits[s];
+    if (!classified(L)) return;
     const uint32_t B = (2u << L) - 1;
     const uint32_t* bc = w.bcount + (size_t)s * MAX_BKT;
     if (threadIdx.x == 0) one = 0;
@@ -227,19 +293,17 @@ __global__ void __launch_bounds__(TILE_THREADS) k_scatter(Work w, uint32_t nbig)
     uint32_t* lcount = sm.lcount;
     uint32_t* lstart = sm.lstart;
     uint32_t* gbase = sm.gbase;
-    uint32_t* tmp = sm.tmp;
-    uint32_t& vt_s = sm.vt;
-    if (threadIdx.x == 0) vt_s = atomicAdd(w.counters + C_TICKET, 1u);
+    if (threadIdx.x == 0) sm.vt = atomicAdd(w.counters + C_TICKET, 1u);
     __syncthreads();
-    const uint32_t vt = vt_s;
+    const uint32_t vt = sm.vt;
     const int s = find_tile_seg(w.tile_start, nbig, vt);
-    const Seg sg = w.big[w.cur][s];
-    if ((sg.meta & META_FINAL) || w.bflags[s]) return;
+    const Seg sg = w.list[L_BIG][w.cur][s];
+    const uint8_t L = w.tree_bits[s];
+    if (!classified(L) || w.bflags[s]) return;
     const uint32_t tin = vt - w.tile_start[s];
     const uint32_t lo = sg.begin + tin * TILE;
     const uint32_t hi = min(lo + TILE, sg.begin + sg.size);
     const uint32_t cnt = hi - lo;
-    const uint32_t L = w.tree_bits[s];
     const uint32_t B = (2u << L) - 1;
     const int buf = sg.meta & META_BUF;
     for (uint32_t b = threadIdx.x; b < B; b += TILE_THREADS) lcount[b] = 0;
@@ -292,7 +356,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_scatter(Work w, uint32_t nbig)
         lstart[b] = lcount[b];
     }
     __syncthreads();
-    block_scan_array<TILE_THREADS>(lstart, (int)B, tmp);
+    block_scan_array<TILE_THREADS>(lstart, (int)B, sm.tmp);
     // stage the tile in bucket order, then write bucket runs contiguously
 #pragma unroll
     for (int j = 0; j < PER; ++j) {
@@ -321,32 +385,47 @@ __global__ void __launch_bounds__(TILE_THREADS) k_scatter(Work w, uint32_t nbig)
 
 __device__ __forceinline__ void push_seg(Work& w, int nxt, Seg c)
 {
-    if (c.size > SMALL_MAX) {
-        const uint32_t at = atomicAdd(w.counters + 3 * nxt + C_NBIG, 1u);
-        if (at >= w.big_cap) { set_error(w.counters + C_ERR, ERR_OVERFLOW); return; }
-        w.big[nxt][at] = c;
-        atomicAdd(w.counters + 3 * nxt + C_NTILES, (c.size + TILE - 1) / TILE);
-    } else {
-        const uint32_t at = atomicAdd(w.counters + 3 * nxt + C_NSMALL, 1u);
-        if (at >= w.small_cap) { set_error(w.counters + C_ERR, ERR_OVERFLOW); return; }
-        w.small[nxt][at] = c;
+    int cls;
+    if (c.size > SMALL_MAX) cls = L_BIG;
+    else if (c.size > 256) cls = L_SMALLB;
+    else if (c.size > WARP_GROUP_MAX) cls = L_SMALLA;
+    else cls = L_TINY;
+    const uint32_t at = atomicAdd(w.counters + C_PAR * nxt + cls, 1u);
+    if (at >= w.cap[cls]) {
+        set_error(w.counters + C_ERR, ERR_OVERFLOW);
+        return;
     }
+    w.list[cls][nxt][at] = c;
+    if (cls == L_BIG) atomicAdd(w.counters + C_PAR * nxt + C_NTILES, (c.size + TILE - 1) / TILE);
 }
 
-// Children of each bucket, after the scatter has placed them.
+// Children of each bucket, after the scatter has placed them; the next
+// segment of a jump segment.
 __global__ void __launch_bounds__(1024) k_children(Work w)
 {
     const int s = blockIdx.x;
-    const Seg sg = w.big[w.cur][s];
-    if (sg.meta & META_FINAL) return;
-    const uint32_t L = w.tree_bits[s];
-    const uint32_t B = (2u << L) - 1;
+    const Seg sg = w.list[L_BIG][w.cur][s];
+    const uint8_t L = w.tree_bits[s];
     const int buf = sg.meta & META_BUF;
+    const int nxt = w.cur ^ 1;
+    if (L == TREE_TIE) {
+        if (threadIdx.x == 0) {
+            const uint32_t mn = w.jump_min[s];
+            if (!w.jump_diff[s])  // every string equals the base
+                push_seg(w, nxt, Seg{sg.begin, sg.size, sg.depth + mn, (uint32_t)buf | META_FINAL});
+            else if (mn == 0)     // no shared char: classify at this depth
+                push_seg(w, nxt, Seg{sg.begin, sg.size, sg.depth, (uint32_t)buf | META_NOTIE});
+            else
+                push_seg(w, nxt, Seg{sg.begin, sg.size, sg.depth + mn, (uint32_t)buf});
+        }
+        return;
+    }
+    if (!classified(L)) return;
+    const uint32_t B = (2u << L) - 1;
     const int nbuf = w.bflags[s] ? buf : buf ^ 1;
     const uint32_t* bc = w.bcount + (size_t)s * MAX_BKT;
     const uint32_t* bs = w.bstart + (size_t)s * MAX_BKT;
     const uint64_t* spl = w.spl + (size_t)s * 1024;
-    const int nxt = w.cur ^ 1;
     const uint32_t* ids = w.ids[nbuf];
     for (uint32_t b = threadIdx.x; b < B; b += blockDim.x) {
         const uint32_t c = bc[b];

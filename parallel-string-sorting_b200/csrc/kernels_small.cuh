@@ -1,17 +1,21 @@
-// kernels_small.cuh -- finishes segments of at most SMALL_MAX strings in one
-// block, including every deeper character round and the LCP array. This is
-// the device counterpart of pS5's base cases: sort_mkqs_cache /
+// kernels_small.cuh -- finishes segments of at most SMALL_MAX strings,
+// including every deeper character round and the LCP array. This is the
+// device counterpart of pS5's base cases: sort_mkqs_cache /
 // insertion_sort_cache on 8-byte caches (src/parallel/
 // bingmann-parallel_sample_sort.hpp:805-861, 1056-1178), inssort_generic
 // (src/sequential/inssort.hpp:63-95) and lcp_insertion_sort
 // (src/sequential/bingmann-lcp_inssort.hpp:38-189).
 //
-// Phase A (block): sort (group, key, id) with a shared-memory bitonic sort;
-// runs of equal keys become groups one 8-byte round deeper. Groups larger
-// than a warp stay in phase A; smaller ones are parked.
-// Phase B (warp per parked group): the same rounds on <= 32 strings with
-// shuffles only. A group that stops splitting jumps to its common prefix with
-// a warp-wide 256-byte compare, so deep repeats cost O(LCP / 256) rounds.
+// Size classes (push_seg in kernels_big.cuh picks the list):
+//   k_tiny           <= 32 strings, one warp per segment, shuffles only
+//   k_small<256,128> <= 256 strings, one block
+//   k_small<2048,256> <= 2048 strings, one block
+// Block phase: sort (group, key, id) with a shared-memory bitonic sort;
+// runs of equal keys become groups one 8-byte round deeper; a group that
+// stops splitting jumps to its common prefix. Groups of <= 32 strings are
+// parked and finished by the warp phase (the k_tiny rounds), where a group
+// that stops splitting jumps ahead with a warp-wide 256-byte compare, so deep
+// repeats cost O(LCP / 256) rounds.
 #pragma once
 
 #include "block_util.cuh"
@@ -19,18 +23,19 @@
 
 namespace pssgpu {
 
+template <int MAXN>
 struct SmallSmem {
-    uint64_t key[SMALL_MAX];
-    uint32_t id[SMALL_MAX];
-    uint32_t gdep[SMALL_MAX];   // depth of the active group starting here
-    uint32_t ndep[SMALL_MAX];   // next depth, staged
-    uint16_t grp[SMALL_MAX];    // start index of the element's group
-    uint16_t rs[SMALL_MAX];     // start index of the element's run
-    uint16_t runlen[SMALL_MAX]; // run length, at the run start
-    uint8_t state[SMALL_MAX];   // 0 active (phase A), 1 done, 2 parked
-    uint16_t park_start[SMALL_MAX / 2];
-    uint16_t park_len[SMALL_MAX / 2];
-    uint32_t park_dep[SMALL_MAX / 2];
+    uint64_t key[MAXN];
+    uint32_t id[MAXN];
+    uint32_t gdep[MAXN];   // depth of the active group starting here
+    uint32_t ndep[MAXN];   // next depth, staged
+    uint16_t grp[MAXN];    // start index of the element's group
+    uint16_t rs[MAXN];     // start index of the element's run
+    uint16_t runlen[MAXN]; // run length, at the run start
+    uint8_t state[MAXN];   // 0 active (block phase), 1 done, 2 parked
+    uint16_t park_start[MAXN / 2];
+    uint16_t park_len[MAXN / 2];
+    uint32_t park_dep[MAXN / 2];
     uint32_t tmp[32];
     uint32_t npark;
     uint32_t nactive;
@@ -47,32 +52,9 @@ __device__ __forceinline__ bool tuple_less(uint32_t ga, uint64_t ka, uint32_t ia
     return ia < ib;
 }
 
-// Bitonic sort of sm.{grp,key,id}[0, npad) by (grp, key, id).
-__device__ void small_bitonic(SmallSmem& sm, uint32_t npad)
-{
-    for (uint32_t kk = 2; kk <= npad; kk <<= 1) {
-        for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
-            for (uint32_t i = threadIdx.x; i < npad / 2; i += SMALL_THREADS) {
-                const uint32_t a = 2 * i - (i & (j - 1));
-                const uint32_t b = a + j;
-                const bool asc = (a & kk) == 0;
-                const uint32_t ga = sm.grp[a], gb = sm.grp[b];
-                const uint64_t ka = sm.key[a], kb = sm.key[b];
-                const uint32_t ia = sm.id[a], ib = sm.id[b];
-                if (tuple_less(gb, kb, ib, ga, ka, ia) == asc) {
-                    sm.grp[a] = (uint16_t)gb; sm.grp[b] = (uint16_t)ga;
-                    sm.key[a] = kb; sm.key[b] = ka;
-                    sm.id[a] = ib; sm.id[b] = ia;
-                }
-            }
-            __syncthreads();
-        }
-    }
-}
-
-// Common-prefix extension (in 8-byte chunks from depth d) of a set of
-// strings against `base`: the first chunk where some string differs from
-// base or base ends. Used when a group stopped splitting.
+// Common-prefix extension (in 8-byte chunks from depth d) of `other`
+// against `base`: the first chunk where they differ or base ends, at most
+// `limit`.
 __device__ __forceinline__ uint32_t chunks_equal(const Work& w, uint32_t base, uint32_t other,
                                                  uint32_t d, uint32_t limit)
 {
@@ -87,25 +69,29 @@ __device__ __forceinline__ uint32_t chunks_equal(const Work& w, uint32_t base, u
     return c;
 }
 
-// Warp-level rounds for one parked group of c <= 32 strings at depth d,
-// occupying sm.id[start, start + c) and positions begin + start + ...
-__device__ void warp_group_sort(const Work& w, SmallSmem& sm, uint32_t begin,
-                                uint32_t start, uint32_t c, uint32_t d)
+// Warp rounds for one group of c <= 32 strings sharing d chars; lane i holds
+// id i on entry and the i-th smallest id on return. LCPs go to
+// lcp[pos0 + lane] for lanes >= 1. first_keys (may be null) holds the keys at
+// depth d, saving the first gather.
+__device__ uint32_t warp_rounds(const Work& w, uint32_t myid, uint32_t c, uint32_t d,
+                                uint32_t pos0, const uint64_t* first_keys)
 {
     const uint32_t lane = threadIdx.x & 31;
     const bool real = lane < c;
-    uint32_t myid = real ? sm.id[start + lane] : 0xFFFFFFFFu;
+    if (!real) myid = 0xFFFFFFFFu;
     uint32_t mygrp = real ? 0u : 0xFFFFFFFFu;
     uint32_t mydep = d;
     uint32_t mystate = real ? 0u : 1u;  // 0 active, 1 done
     uint64_t mykey = 0;
     uint32_t prev_active = c;
     bool stalled = false;
+    bool first = first_keys != nullptr;
     while (true) {
         const uint32_t A = __ballot_sync(0xffffffffu, mystate == 0);
         if (A == 0) break;
         if (stalled) {
-            // exactly one active group: jump to its common prefix
+            // exactly one active group that did not split: jump to its
+            // common prefix, 32 chunks of 8 bytes per step
             const int f = __ffs(A) - 1;
             const uint32_t base = __shfl_sync(0xffffffffu, myid, f);
             const uint32_t dd = __shfl_sync(0xffffffffu, mydep, f);
@@ -130,7 +116,9 @@ __device__ void warp_group_sort(const Work& w, SmallSmem& sm, uint32_t begin,
             }
             if (mystate == 0) mydep = dd + 8u * best;
         }
-        if (mystate == 0) mykey = gather_key(w.chars, w.nchars, w.offs, myid, mydep);
+        if (mystate == 0)
+            mykey = first ? first_keys[lane] : gather_key(w.chars, w.nchars, w.offs, myid, mydep);
+        first = false;
         // bitonic sort of the 32 lanes by (grp, key, id), carrying dep/state
 #pragma unroll
         for (uint32_t kk = 2; kk <= 32; kk <<= 1) {
@@ -144,7 +132,7 @@ __device__ void warp_group_sort(const Work& w, SmallSmem& sm, uint32_t begin,
                 const bool lower = (lane & j) == 0;
                 const bool asc = (lane & kk) == 0;
                 const bool other_less = tuple_less(og, ok, oi, mygrp, mykey, myid);
-                // lower lane keeps the smaller in an ascending pair
+                // the lower lane of an ascending pair keeps the smaller
                 const bool take = (lower == asc) ? other_less : !other_less;
                 if (take) { mygrp = og; mykey = ok; myid = oi; mydep = od; mystate = os; }
             }
@@ -160,7 +148,7 @@ __device__ void warp_group_sort(const Work& w, SmallSmem& sm, uint32_t begin,
         const uint32_t len = nx - rs;
         if (mystate == 0) {
             if (lane >= 1 && pg == mygrp && w.lcp) {
-                const uint32_t pos = begin + start + lane;
+                const uint32_t pos = pos0 + lane;
                 if (pk != mykey) w.lcp[pos] = mydep + lcp_key_type(pk, mykey);
                 else if (key_terminated(mykey)) w.lcp[pos] = mydep + lcp_key_depth(mykey);
             }
@@ -174,20 +162,62 @@ __device__ void warp_group_sort(const Work& w, SmallSmem& sm, uint32_t begin,
         stalled = (na == prev_active) && (__popc(G2) == 1);
         prev_active = na;
     }
-    if (real) sm.id[start + lane] = myid;
+    return myid;
 }
 
-__global__ void __launch_bounds__(SMALL_THREADS) k_small(Work w, uint32_t nsmall)
+// One warp per segment of at most 32 strings; 8 segments per block.
+constexpr int TINY_WARPS = 8;
+__global__ void __launch_bounds__(32 * TINY_WARPS) k_tiny(Work w, const Seg* list, uint32_t count)
+{
+    const uint32_t g = blockIdx.x * TINY_WARPS + (threadIdx.x >> 5);
+    if (g >= count) return;  // whole warp
+    const uint32_t lane = threadIdx.x & 31;
+    const Seg sg = list[g];
+    const int buf = sg.meta & META_BUF;
+    if (lane == 0) atomicAdd(w.counters + C_P_SMALL, sg.size);
+    uint32_t myid = lane < sg.size ? w.ids[buf][sg.begin + lane] : 0xFFFFFFFFu;
+    const uint64_t* fk = (sg.meta & META_VALID) ? w.keys[buf] + sg.begin : nullptr;
+    myid = warp_rounds(w, myid, sg.size, sg.depth, sg.begin, fk);
+    if (lane < sg.size) w.perm[sg.begin + lane] = myid;
+}
+
+// Bitonic sort of sm.{grp,key,id}[0, npad) by (grp, key, id).
+template <int MAXN, int THREADS>
+__device__ void small_bitonic(SmallSmem<MAXN>& sm, uint32_t npad)
+{
+    for (uint32_t kk = 2; kk <= npad; kk <<= 1) {
+        for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = threadIdx.x; i < npad / 2; i += THREADS) {
+                const uint32_t a = 2 * i - (i & (j - 1));
+                const uint32_t b = a + j;
+                const bool asc = (a & kk) == 0;
+                const uint32_t ga = sm.grp[a], gb = sm.grp[b];
+                const uint64_t ka = sm.key[a], kb = sm.key[b];
+                const uint32_t ia = sm.id[a], ib = sm.id[b];
+                if (tuple_less(gb, kb, ib, ga, ka, ia) == asc) {
+                    sm.grp[a] = (uint16_t)gb; sm.grp[b] = (uint16_t)ga;
+                    sm.key[a] = kb; sm.key[b] = ka;
+                    sm.id[a] = ib; sm.id[b] = ia;
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// One block per segment of 33..MAXN strings (or an all-equal segment to copy).
+template <int MAXN, int THREADS>
+__global__ void __launch_bounds__(THREADS) k_small(Work w, const Seg* list)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    SmallSmem& sm = *reinterpret_cast<SmallSmem*>(smem_raw);
-    const Seg sg = w.small[w.cur][blockIdx.x];
+    SmallSmem<MAXN>& sm = *reinterpret_cast<SmallSmem<MAXN>*>(smem_raw);
+    const Seg sg = list[blockIdx.x];
     const uint32_t m = sg.size, begin = sg.begin;
     const int buf = sg.meta & META_BUF;
     const uint32_t* gids = w.ids[buf];
     if (threadIdx.x == 0) atomicAdd(w.counters + C_P_SMALL, m);
     if (sg.meta & META_FINAL) {
-        for (uint32_t i = threadIdx.x; i < m; i += SMALL_THREADS) {
+        for (uint32_t i = threadIdx.x; i < m; i += THREADS) {
             w.perm[begin + i] = gids[begin + i];
             if (w.lcp && i) w.lcp[begin + i] = sg.depth;
         }
@@ -197,7 +227,7 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_small(Work w, uint32_t nsmall
         sm.npark = 0;
         atomicAdd(w.counters + C_SMALLSEGS, 1u);
     }
-    for (uint32_t i = threadIdx.x; i < m; i += SMALL_THREADS) sm.id[i] = gids[begin + i];
+    for (uint32_t i = threadIdx.x; i < m; i += THREADS) sm.id[i] = gids[begin + i];
     __syncthreads();
     if (m <= (uint32_t)WARP_GROUP_MAX) {
         if (threadIdx.x == 0) {
@@ -206,11 +236,11 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_small(Work w, uint32_t nsmall
         }
         __syncthreads();
     } else {
-        // ---------------- phase A ----------------
+        // ---------------- block phase ----------------
         uint32_t npad = 1;
         while (npad < m) npad <<= 1;
         const bool valid = sg.meta & META_VALID;
-        for (uint32_t i = threadIdx.x; i < npad; i += SMALL_THREADS) {
+        for (uint32_t i = threadIdx.x; i < npad; i += THREADS) {
             if (i < m) {
                 sm.key[i] = valid ? w.keys[buf][begin + i]
                                   : gather_key(w.chars, w.nchars, w.offs, sm.id[i], sg.depth);
@@ -226,7 +256,7 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_small(Work w, uint32_t nsmall
         if (threadIdx.x == 0) sm.gdep[0] = sg.depth;
         uint32_t prev_active = m;
         bool stalled = false;
-        const uint32_t per = (m + SMALL_THREADS - 1) / SMALL_THREADS;
+        const uint32_t per = (m + THREADS - 1) / THREADS;
         const uint32_t clo = min(threadIdx.x * per, m), chi = min(clo + per, m);
         while (true) {
             __syncthreads();
@@ -237,7 +267,7 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_small(Work w, uint32_t nsmall
                 const uint32_t base = sm.id[g0];
                 if (threadIdx.x == 0) sm.jump = 0xFFFFFFFFu;
                 __syncthreads();
-                for (uint32_t i = threadIdx.x; i < m; i += SMALL_THREADS) {
+                for (uint32_t i = threadIdx.x; i < m; i += THREADS) {
                     if (sm.state[i] != 0 || i == g0) continue;
                     const uint32_t lim = *((volatile uint32_t*)&sm.jump);
                     const uint32_t c = chunks_equal(w, base, sm.id[i], d0, lim);
@@ -246,12 +276,12 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_small(Work w, uint32_t nsmall
                 __syncthreads();
                 if (threadIdx.x == 0) sm.gdep[g0] = d0 + 8u * sm.jump;
                 __syncthreads();
-                for (uint32_t i = threadIdx.x; i < m; i += SMALL_THREADS)
+                for (uint32_t i = threadIdx.x; i < m; i += THREADS)
                     if (sm.state[i] == 0)
                         sm.key[i] = gather_key(w.chars, w.nchars, w.offs, sm.id[i], sm.gdep[sm.grp[i]]);
                 __syncthreads();
             }
-            small_bitonic(sm, npad);
+            small_bitonic<MAXN, THREADS>(sm, npad);
             // run starts: a run is a maximal stretch of equal (grp, key)
             uint32_t last = 0;
             for (uint32_t i = clo; i < chi; ++i) {
@@ -259,7 +289,7 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_small(Work w, uint32_t nsmall
                 if (ns) last = i;
             }
             const bool any = clo < chi;
-            uint32_t carry = block_excl_max<SMALL_THREADS>(any ? last : 0u, sm.tmp);
+            uint32_t carry = block_excl_max<THREADS>(any ? last : 0u, sm.tmp);
             for (uint32_t i = clo; i < chi; ++i) {
                 const bool ns = i == 0 || sm.grp[i] != sm.grp[i - 1] || sm.key[i] != sm.key[i - 1];
                 if (ns) carry = i;
@@ -270,7 +300,7 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_small(Work w, uint32_t nsmall
             if (threadIdx.x == 0) { sm.nactive = 0; sm.ngroups = 0; }
             __syncthreads();
             // resolve: LCPs, new states, parked groups (reads gdep only)
-            for (uint32_t i = threadIdx.x; i < m; i += SMALL_THREADS) {
+            for (uint32_t i = threadIdx.x; i < m; i += THREADS) {
                 if (sm.state[i] != 0) continue;
                 const uint64_t k = sm.key[i];
                 const uint32_t d = sm.gdep[sm.grp[i]];
@@ -293,7 +323,7 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_small(Work w, uint32_t nsmall
                 }
             }
             __syncthreads();
-            for (uint32_t i = threadIdx.x; i < m; i += SMALL_THREADS) {
+            for (uint32_t i = threadIdx.x; i < m; i += THREADS) {
                 if (sm.state[i] != 0) continue;
                 const uint32_t r = sm.rs[i];
                 const uint32_t len = sm.runlen[r];
@@ -319,20 +349,30 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_small(Work w, uint32_t nsmall
             stalled = (na == prev_active) && (sm.ngroups == 1);
             prev_active = na;
             if (!stalled) {
-                for (uint32_t i = threadIdx.x; i < m; i += SMALL_THREADS)
+                for (uint32_t i = threadIdx.x; i < m; i += THREADS)
                     if (sm.state[i] == 0)
                         sm.key[i] = gather_key(w.chars, w.nchars, w.offs, sm.id[i], sm.gdep[sm.grp[i]]);
             }
         }
         __syncthreads();
     }
-    // ---------------- phase B ----------------
-    const uint32_t warp = threadIdx.x >> 5;
+    // ---------------- warp phase ----------------
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t np = sm.npark;
-    for (uint32_t g = warp; g < np; g += SMALL_THREADS / 32)
-        warp_group_sort(w, sm, begin, sm.park_start[g], sm.park_len[g], sm.park_dep[g]);
+    for (uint32_t g = warp; g < np; g += THREADS / 32) {
+        const uint32_t start = sm.park_start[g], c = sm.park_len[g];
+        uint32_t myid = lane < c ? sm.id[start + lane] : 0xFFFFFFFFu;
+        myid = warp_rounds(w, myid, c, sm.park_dep[g], begin + start, nullptr);
+        if (lane < c) sm.id[start + lane] = myid;
+    }
     __syncthreads();
-    for (uint32_t i = threadIdx.x; i < m; i += SMALL_THREADS) w.perm[begin + i] = sm.id[i];
+    for (uint32_t i = threadIdx.x; i < m; i += THREADS) w.perm[begin + i] = sm.id[i];
 }
+
+// the two block-sized classes
+constexpr int SMALL_A = 256;
+constexpr int SMALL_A_THREADS = 128;
+#define K_SMALL_A k_small<SMALL_A, SMALL_A_THREADS>
+#define K_SMALL_B k_small<SMALL_MAX, SMALL_THREADS>
 
 }  // namespace pssgpu

@@ -52,16 +52,19 @@ __global__ void k_root(Work w)
 }
 
 struct Sizes {
-    uint64_t n, big_cap, small_cap, tile_cap;
+    uint64_t n, cap[L_NCLASS], tile_cap;
 };
 
 static Sizes sizes_for(uint64_t n)
 {
     Sizes s;
     s.n = std::max<uint64_t>(n, 1);
-    s.big_cap = s.n / (SMALL_MAX + 1) + 2;
-    s.small_cap = s.n / 2 + 2;
-    s.tile_cap = s.n / TILE + s.big_cap + 1;
+    // a segment of class c has more strings than the class below it holds
+    s.cap[L_BIG] = s.n / (SMALL_MAX + 1) + 2;
+    s.cap[L_SMALLB] = s.n / 257 + 2;
+    s.cap[L_SMALLA] = s.n / (WARP_GROUP_MAX + 1) + 2;
+    s.cap[L_TINY] = s.n / 2 + 2;
+    s.tile_cap = s.n / TILE + s.cap[L_BIG] + 1;
     return s;
 }
 
@@ -69,17 +72,19 @@ static uint64_t align256(uint64_t b) { return (b + 255) & ~255ull; }
 
 static uint64_t workspace_bytes(const Sizes& s)
 {
+    const uint64_t big = s.cap[L_BIG];
     uint64_t b = 0;
     b += 2 * align256(4 * s.n);                    // ids
     b += 2 * align256(8 * s.n);                    // keys
     b += align256(2 * s.n);                        // bucket ids
     b += align256(8 * s.n);                        // boundary list
-    b += 2 * align256(16 * s.big_cap);             // big lists
-    b += 2 * align256(16 * s.small_cap);           // small lists
-    b += align256(4 * (s.big_cap + 1));            // tile starts
-    b += 2 * align256(s.big_cap);                  // tree bits, one-bucket flags
-    b += 2 * align256(8ull * 1024 * s.big_cap);    // trees, splitters
-    b += 2 * align256(4ull * MAX_BKT * s.big_cap); // bucket counts, starts
+    for (int c = 0; c < L_NCLASS; ++c)
+        b += 2 * align256(16 * s.cap[c]);          // segment lists
+    b += align256(4 * (big + 1));                  // tile starts
+    b += 2 * align256(big);                        // tree bits, one-bucket flags
+    b += 2 * align256(4 * big);                    // jump minimum, jump differs
+    b += 2 * align256(8ull * 1024 * big);          // trees, splitters
+    b += 2 * align256(4ull * MAX_BKT * big);       // bucket counts, starts
     b += align256(8ull * MAX_BKT * s.tile_cap);    // look-back status
     b += align256(4 * C_COUNT);                    // counters
     return b;
@@ -106,7 +111,7 @@ struct Ctx {
     // workspace
     unsigned char* ws = nullptr;
     uint64_t ws_bytes = 0;
-    Sizes cap{0, 0, 0, 0};
+    Sizes cap{};
     Work base{};
     uint32_t epoch = 0;
     uint32_t* host_counters = nullptr;  // pinned
@@ -168,17 +173,20 @@ static int ensure_workspace(Ctx* c, uint64_t n)
     w.bkt = (uint16_t*)take(2 * s.n);
     w.bnd = (uint2*)take(8 * s.n);
     w.bnd_cap = (uint32_t)s.n;
-    for (int i = 0; i < 2; ++i) w.big[i] = (Seg*)take(16 * s.big_cap);
-    for (int i = 0; i < 2; ++i) w.small[i] = (Seg*)take(16 * s.small_cap);
-    w.big_cap = (uint32_t)s.big_cap;
-    w.small_cap = (uint32_t)s.small_cap;
-    w.tile_start = (uint32_t*)take(4 * (s.big_cap + 1));
-    w.tree_bits = (uint8_t*)take(s.big_cap);
-    w.bflags = (uint8_t*)take(s.big_cap);
-    w.tree = (uint64_t*)take(8ull * 1024 * s.big_cap);
-    w.spl = (uint64_t*)take(8ull * 1024 * s.big_cap);
-    w.bcount = (uint32_t*)take(4ull * MAX_BKT * s.big_cap);
-    w.bstart = (uint32_t*)take(4ull * MAX_BKT * s.big_cap);
+    for (int c = 0; c < L_NCLASS; ++c) {
+        for (int i = 0; i < 2; ++i) w.list[c][i] = (Seg*)take(16 * s.cap[c]);
+        w.cap[c] = (uint32_t)s.cap[c];
+    }
+    const uint64_t big = s.cap[L_BIG];
+    w.tile_start = (uint32_t*)take(4 * (big + 1));
+    w.tree_bits = (uint8_t*)take(big);
+    w.bflags = (uint8_t*)take(big);
+    w.jump_min = (uint32_t*)take(4 * big);
+    w.jump_diff = (uint32_t*)take(4 * big);
+    w.tree = (uint64_t*)take(8ull * 1024 * big);
+    w.spl = (uint64_t*)take(8ull * 1024 * big);
+    w.bcount = (uint32_t*)take(4ull * MAX_BKT * big);
+    w.bstart = (uint32_t*)take(4ull * MAX_BKT * big);
     w.status = (uint64_t*)take(8ull * MAX_BKT * s.tile_cap);
     w.tile_cap = (uint32_t)s.tile_cap;
     w.counters = (uint32_t*)take(4 * C_COUNT);
@@ -187,17 +195,25 @@ static int ensure_workspace(Ctx* c, uint64_t n)
     return PSSGPU_OK;
 }
 
+// Shared-memory limits of the kernels that need more than 48 KB, set once
+// per device (the attribute belongs to the device's context).
 static int setup_kernels()
 {
-    static int done = 0;
+    constexpr int MAXDEV = 64;
+    static bool done[MAXDEV] = {};
     static std::mutex mu;
+    int dev = 0;
+    PSS_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= MAXDEV) return fail(PSSGPU_ENODEV, "device index out of range");
     std::lock_guard<std::mutex> lk(mu);
-    if (done) return PSSGPU_OK;
-    PSS_CUDA(cudaFuncSetAttribute(k_small, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)sizeof(SmallSmem)));
+    if (done[dev]) return PSSGPU_OK;
+    PSS_CUDA(cudaFuncSetAttribute(K_SMALL_A, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sizeof(SmallSmem<SMALL_A>)));
+    PSS_CUDA(cudaFuncSetAttribute(K_SMALL_B, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sizeof(SmallSmem<SMALL_MAX>)));
     PSS_CUDA(cudaFuncSetAttribute(k_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)sizeof(ScatterSmem)));
-    done = 1;
+    done[dev] = true;
     return PSSGPU_OK;
 }
 
@@ -241,11 +257,15 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
     PSS_CUDA(cudaMemcpyAsync(hc, w.counters, 4 * C_COUNT, cudaMemcpyDeviceToHost, st));
     PSS_CUDA(cudaStreamSynchronize(st));
     kt.collect();
-    uint32_t nbig = hc[C_NBIG], nsmall = hc[C_NSMALL], ntiles = hc[C_NTILES];
+    uint32_t cnt[L_NCLASS];
+    for (int k = 0; k < L_NCLASS; ++k) cnt[k] = hc[k];
+    uint32_t ntiles = hc[C_NTILES];
     uint32_t err = hc[C_ERR];
     int cur = 0;
-    while (!err && (nbig || nsmall)) {
+    auto pending = [&]() { return cnt[L_BIG] || cnt[L_TINY] || cnt[L_SMALLA] || cnt[L_SMALLB]; };
+    while (!err && pending()) {
         const int nxt = cur ^ 1;
+        const uint32_t nbig = cnt[L_BIG];
         w.cur = cur;
         if (nbig) {
             if (++c->epoch >= 0xFFFFu) {
@@ -254,15 +274,30 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
             }
             w.epoch = c->epoch;
         }
-        PSS_CUDA(cudaMemsetAsync(w.counters + 3 * nxt, 0, 12, st));
+        PSS_CUDA(cudaMemsetAsync(w.counters + C_PAR * nxt, 0, 4 * C_PAR, st));
         PSS_CUDA(cudaMemsetAsync(w.counters + C_TICKET, 0, 4, st));
-        PSS_CUDA(cudaMemsetAsync(w.counters + C_P_BIG, 0, 4 * (C_P_SMALL - C_P_BIG + 1), st));
-        if (nsmall) {
+        PSS_CUDA(cudaMemsetAsync(w.counters + C_P_FIRST, 0, 4 * (C_P_LAST - C_P_FIRST + 1), st));
+        if (cnt[L_TINY] || cnt[L_SMALLA] || cnt[L_SMALLB]) {
             kt.begin(K_SMALL);
-            k_small<<<nsmall, SMALL_THREADS, sizeof(SmallSmem), st>>>(w, nsmall);
+            if (cnt[L_TINY]) {
+                k_tiny<<<(cnt[L_TINY] + TINY_WARPS - 1) / TINY_WARPS, 32 * TINY_WARPS, 0, st>>>(
+                    w, w.list[L_TINY][cur], cnt[L_TINY]);
+                c->kstat[K_SMALL].launches += 1;
+                stats.kernel_launches += 1;
+            }
+            if (cnt[L_SMALLA]) {
+                K_SMALL_A<<<cnt[L_SMALLA], SMALL_A_THREADS, sizeof(SmallSmem<SMALL_A>), st>>>(
+                    w, w.list[L_SMALLA][cur]);
+                c->kstat[K_SMALL].launches += 1;
+                stats.kernel_launches += 1;
+            }
+            if (cnt[L_SMALLB]) {
+                K_SMALL_B<<<cnt[L_SMALLB], SMALL_THREADS, sizeof(SmallSmem<SMALL_MAX>), st>>>(
+                    w, w.list[L_SMALLB][cur]);
+                c->kstat[K_SMALL].launches += 1;
+                stats.kernel_launches += 1;
+            }
             kt.end(K_SMALL);
-            c->kstat[K_SMALL].launches += 1;
-            stats.kernel_launches += 1;
         }
         if (nbig) {
             if (ntiles > c->cap.tile_cap) return fail(PSSGPU_ECUDA, "tile capacity exceeded");
@@ -298,21 +333,22 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
             // per-string algorithmic bytes of each kernel class: key gather
             // 4 id + 8 chars + 8 key write; classify 8 key read; scatter
             // 12 read + 12 write; base case 12 read + output
+            // (a jump string is charged like a gather: 4 id + 8 offset + 8 chars)
             const uint64_t big = hc[C_P_BIG], stale = hc[C_P_STALE], fin = hc[C_P_FINAL];
-            const uint64_t sc = hc[C_P_SCATTER], sm = hc[C_P_SMALL];
-            stats.big_elements += big;
-            c->kstat[K_SAMPLE].strings += big;
-            c->kstat[K_CLASSIFY].strings += big + fin;
-            c->kstat[K_CLASSIFY].alg_bytes += 20 * stale + 8 * (big - stale) + (4 + out_bytes) * fin;
+            const uint64_t sc = hc[C_P_SCATTER], sm = hc[C_P_SMALL], tie = hc[C_P_TIE];
+            stats.big_elements += big + tie;
+            c->kstat[K_SAMPLE].strings += big + tie;
+            c->kstat[K_CLASSIFY].strings += big + fin + tie;
+            c->kstat[K_CLASSIFY].alg_bytes +=
+                20 * stale + 8 * (big - stale) + (4 + out_bytes) * fin + 20 * tie;
             c->kstat[K_SCATTER].strings += sc;
             c->kstat[K_SCATTER].alg_bytes += 24 * sc;
             c->kstat[K_SMALL].strings += sm;
             c->kstat[K_SMALL].alg_bytes += (12 + out_bytes) * sm;
             c->kstat[K_CHILDREN].strings += big;
         }
-        nbig = hc[3 * nxt + C_NBIG];
-        nsmall = hc[3 * nxt + C_NSMALL];
-        ntiles = hc[3 * nxt + C_NTILES];
+        for (int k = 0; k < L_NCLASS; ++k) cnt[k] = hc[C_PAR * nxt + k];
+        ntiles = hc[C_PAR * nxt + C_NTILES];
         err = hc[C_ERR];
         cur = nxt;
     }
@@ -633,7 +669,7 @@ void pssgpu_sort_strings_lcp_cache(uint8_t** strings, uintptr_t* lcp, uint8_t* c
 // pssgpu_sort_device_noalloc sorts at most PSSGPU_NOALLOC_MAX_STRINGS strings
 // with the small-segment kernel and allocates nothing. Its scratch -- the id
 // buffer, the one segment descriptor and the counters that kernel uses -- is
-// the file-scope array below (8,272 bytes), which every device that loads this
+// the file-scope array below (8,336 bytes), which every device that loads this
 // library holds until the process exits. In host code the array's name is
 // only a host-side stand-in: kernels get the device address that
 // cudaGetSymbolAddress returns, looked up once per device with that device
@@ -691,8 +727,8 @@ extern "C" int pssgpu_sort_device_noalloc(const uint8_t* d_chars, uint64_t nchar
             void* p = nullptr;
             if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p)
                 return fail(PSSGPU_ECUDA, "symbol lookup");
-            if (cudaFuncSetAttribute(k_small, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)sizeof(SmallSmem)) != cudaSuccess)
+            if (cudaFuncSetAttribute(K_SMALL_B, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sizeof(SmallSmem<SMALL_MAX>)) != cudaSuccess)
                 return fail(PSSGPU_ECUDA, "smem limit");
             g_noalloc_addr[dev] = static_cast<NoAllocScratch*>(p);
         }
@@ -714,10 +750,9 @@ extern "C" int pssgpu_sort_device_noalloc(const uint8_t* d_chars, uint64_t nchar
     w.perm = d_perm;
     w.lcp = d_lcp;
     w.counters = scratch->counters;
-    w.small[0] = w.small[1] = &scratch->seg;
     w.cur = 0;
     k_noalloc_prep<<<1, SMALL_THREADS, 0, st>>>(d_offs, nchars, (uint32_t)n);
-    k_small<<<1, SMALL_THREADS, sizeof(SmallSmem), st>>>(w, 1u);
+    K_SMALL_B<<<1, SMALL_THREADS, sizeof(SmallSmem<SMALL_MAX>), st>>>(w, &scratch->seg);
     uint32_t err = 0;
     if (cudaGetLastError() != cudaSuccess ||
         cudaMemcpyAsync(&err, scratch->counters + C_ERR, 4, cudaMemcpyDeviceToHost, st) !=

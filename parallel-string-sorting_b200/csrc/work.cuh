@@ -9,28 +9,34 @@ constexpr int TILE = 4096;          // strings per classify / scatter tile
 constexpr int TILE_THREADS = 256;   // 16 strings per thread
 constexpr int MAX_TREE_BITS = 10;   // 1023 splitters, 2047 buckets (pS5's DefaultTreebits)
 constexpr int MAX_BKT = 2048;       // bucket slots per big segment
-constexpr int SMALL_MAX = 2048;     // largest segment the small-sort kernel takes
+constexpr int SMALL_MAX = 2048;     // largest segment the block sorter takes
 constexpr int SMALL_THREADS = 256;
 constexpr int WARP_GROUP_MAX = 32;  // groups this small are finished by one warp
 constexpr int FINAL_INLINE = 64;    // equal-string buckets this small are copied inline
 constexpr uint32_t SPIN_CAP = 1u << 20;  // look-back wait limit (polls, ~0.1 s)
+constexpr uint8_t TREE_TIE = 0xFF;  // tree_bits marker: all samples equal, jump instead
+
+// segment list classes
+enum : int { L_BIG = 0, L_TINY = 1, L_SMALLA = 2, L_SMALLB = 3, L_NCLASS = 4 };
 
 // counters[] layout
 enum : int {
-    C_NBIG = 0,       // + 3 * parity
-    C_NSMALL = 1,     // + 3 * parity
-    C_NTILES = 2,     // + 3 * parity
-    C_NBND = 6,       // boundary list length
-    C_TICKET = 7,     // scatter tile ticket
-    C_ERR = 8,        // error bits
-    C_SMALLSEGS = 9,  // statistics: segments finished by the small sorter
+    C_PAR = 8,        // counters per parity block: [class] lengths, then tiles
+    C_NTILES = 4,     // + C_PAR * parity: tiles of the big list
+    C_NBND = 16,      // boundary list length
+    C_TICKET = 17,    // scatter tile ticket
+    C_ERR = 18,       // error bits
+    C_SMALLSEGS = 19, // statistics: segments finished by the block sorter
     // per-pass statistics, reset every pass
-    C_P_BIG = 10,      // strings in big sample-sort segments
-    C_P_STALE = 11,    // of those, strings whose key was gathered this pass
-    C_P_FINAL = 12,    // strings copied out of big all-equal segments
-    C_P_SCATTER = 13,  // strings moved by the scatter
-    C_P_SMALL = 14,    // strings finished by the small sorter
-    C_COUNT = 16
+    C_P_BIG = 20,     // strings in big sample-sort segments
+    C_P_STALE = 21,   // of those, strings whose key was gathered this pass
+    C_P_FINAL = 22,   // strings copied out of big all-equal segments
+    C_P_SCATTER = 23, // strings moved by the scatter
+    C_P_SMALL = 24,   // strings finished by the small sorters
+    C_P_TIE = 25,     // strings of segments that took the common-prefix jump
+    C_P_FIRST = C_P_BIG,
+    C_P_LAST = C_P_TIE,
+    C_COUNT = 32
 };
 
 struct Work {
@@ -50,18 +56,19 @@ struct Work {
     uint32_t* counters;
     uint2* bnd;  // (position, depth) of split boundaries
     uint32_t bnd_cap;
-    // segment lists, double-buffered by pass parity
-    Seg* big[2];
-    Seg* small[2];
-    uint32_t big_cap, small_cap;
+    // segment lists per class, double-buffered by pass parity
+    Seg* list[L_NCLASS][2];
+    uint32_t cap[L_NCLASS];
     // per big segment of the current pass
-    uint32_t* tile_start;  // [big_cap + 1]
-    uint8_t* tree_bits;    // [big_cap]
-    uint64_t* tree;        // [big_cap][1024], level order, index 1..k
-    uint64_t* spl;         // [big_cap][1024], sorted splitters
-    uint32_t* bcount;      // [big_cap][MAX_BKT]
-    uint32_t* bstart;      // [big_cap][MAX_BKT]
-    uint8_t* bflags;       // [big_cap]: 1 = whole segment in one bucket
+    uint32_t* tile_start;  // [cap[L_BIG] + 1]
+    uint8_t* tree_bits;    // [cap[L_BIG]]; 0 = all-equal copy, TREE_TIE = jump
+    uint64_t* tree;        // [cap[L_BIG]][1024], level order, index 1..k
+    uint64_t* spl;         // [cap[L_BIG]][1024], sorted splitters
+    uint32_t* bcount;      // [cap[L_BIG]][MAX_BKT]
+    uint32_t* bstart;      // [cap[L_BIG]][MAX_BKT]
+    uint8_t* bflags;       // [cap[L_BIG]]: 1 = whole segment in one bucket
+    uint32_t* jump_min;    // [cap[L_BIG]]: min common prefix beyond depth (jump)
+    uint32_t* jump_diff;   // [cap[L_BIG]]: some string differs from the base
     uint64_t* status;      // [tile_cap][MAX_BKT] decoupled look-back words
     uint32_t tile_cap;
     uint32_t epoch;        // look-back epoch of this pass (1..65535)

@@ -70,6 +70,32 @@ def test_edge_cases(pkg, orc, ctx, strings):
     check_against_oracle(orc, chars, offs, perm, lcp)
 
 
+def _rand_tails(n, k, seed):
+    rng = np.random.default_rng(seed)
+    return [bytes(rng.integers(97, 100, k, dtype=np.uint8)) for _ in range(n)]
+
+
+@pytest.mark.parametrize("case", ["all_equal_big", "long_prefix_big", "few_differ_early",
+                                  "one_differs_first_char"])
+def test_common_prefix_jump(pkg, orc, ctx, case):
+    """Big segments whose samples are all equal take the common-prefix jump:
+    all strings equal (finished by the jump), a long shared prefix, a few
+    strings leaving the prefix early, one string differing at char 0 (the
+    jump makes no progress and the segment is classified instead)."""
+    if case == "all_equal_big":
+        strings = [b"q" * 500] * 100000
+    elif case == "long_prefix_big":
+        strings = [b"p" * 1000 + t for t in _rand_tails(50000, 3, 1)]
+    elif case == "few_differ_early":
+        strings = [b"r" * 300 + t for t in _rand_tails(30000, 2, 2)]
+        strings += [b"r" * 5 + b"a" + t for t in _rand_tails(10, 4, 3)]
+    else:
+        strings = [b"s" * 40] * 20000 + [b"a"]
+    chars, offs = pkg.pack_strings(strings)
+    perm, lcp = ctx.sort_host(chars, offs, lcp=True)
+    check_against_oracle(orc, chars, offs, perm, lcp)
+
+
 def test_deep_repeats_suffixes(pkg, orc, ctx):
     # a periodic text: suffix LCPs up to the text length
     text = (b"abcab" * 4000)[:19999] + b"\0"

@@ -87,6 +87,15 @@ typedef struct pssgpu_kernel_stats {
 int pssgpu_ctx_set_profile(pssgpu_ctx* ctx, int on);
 int pssgpu_ctx_kernel_stats(pssgpu_ctx* ctx, pssgpu_kernel_stats* out, int max);
 
+/* Context options. PSSGPU_OPT_PROFILE: as pssgpu_ctx_set_profile.
+ * PSSGPU_OPT_INDIRECT_HANDLES: carry bare string ids through the sort and
+ * read offsets from the offset array at every gather -- the path a sort takes
+ * on its own when an id and an arena offset do not fit one 64-bit handle;
+ * for testing that path on small inputs. */
+#define PSSGPU_OPT_PROFILE 1
+#define PSSGPU_OPT_INDIRECT_HANDLES 2
+int pssgpu_ctx_set_option(pssgpu_ctx* ctx, int option, int64_t value);
+
 /* ---- arena sorts ---------------------------------------------------------
  * chars[0, nchars) holds the strings; string i starts at chars + offs[i] and
  * ends at its first NUL, which must lie inside the arena (chars[nchars-1]
@@ -136,7 +145,7 @@ int pssgpu_sort_strings_status(unsigned char** strings, uintptr_t* lcp,
  * already fully reserved. Inputs and outputs are caller-owned device buffers
  * exactly as for pssgpu_sort_device; `stream` is a cudaStream_t (NULL: the
  * default stream); the call returns after the sort has completed.
- * Scratch is one file-scope device array of 8,336 bytes inside the library,
+ * Scratch is one file-scope device array of 16,528 bytes inside the library,
  * held by every device that loads the library until the process exits. All
  * calls share it: calls whose GPU work overlaps (other streams, other host
  * threads) race on it, so the caller must serialise them. The first call on

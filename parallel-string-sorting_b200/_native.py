@@ -26,6 +26,7 @@ GPU_SIGNATURES = {
     "pssgpu_ctx_stats": (C.c_int, [C.c_void_p, C.c_void_p]),
     "pssgpu_ctx_set_profile": (C.c_int, [C.c_void_p, C.c_int]),
     "pssgpu_ctx_kernel_stats": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "pssgpu_ctx_set_option": (C.c_int, [C.c_void_p, C.c_int, C.c_int64]),
     "pssgpu_sort_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64,
                                    C.c_void_p, C.c_void_p]),
     "pssgpu_sort_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64,

@@ -77,6 +77,12 @@ class Context:
         kernel_stats())."""
         _check(_native.gpu().pssgpu_ctx_set_profile(self._h, 1 if on else 0))
 
+    OPT_PROFILE = 1
+    OPT_INDIRECT_HANDLES = 2
+
+    def set_option(self, option: int, value: int) -> None:
+        _check(_native.gpu().pssgpu_ctx_set_option(self._h, option, value))
+
     def kernel_stats(self) -> list:
         arr = (PssKernelStats * 16)()
         k = _native.gpu().pssgpu_ctx_kernel_stats(self._h, arr, 16)

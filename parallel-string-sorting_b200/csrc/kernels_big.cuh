@@ -84,7 +84,7 @@ __global__ void __launch_bounds__(1024) k_sample(Work w)
         const uint64_t h = mix64(((uint64_t)sg.begin << 32) ^ ((uint64_t)sg.depth << 12) ^ i);
         const uint32_t r = sg.begin + (uint32_t)(h % sg.size);
         samp[i] = valid ? w.keys[buf][r]
-                        : gather_key(w.chars, w.nchars, w.offs, w.ids[buf][r], sg.depth);
+                        : h_key(w, w.hnd[buf][r], sg.depth);
     }
     __syncthreads();
     // bitonic sort of the S samples
@@ -127,23 +127,31 @@ __global__ void __launch_bounds__(1024) k_sample(Work w)
     if (threadIdx.x == 0) w.tree_bits[s] = (uint8_t)L;
 }
 
-// Chars string `id` shares with the base string (at arena offset boff, both
-// from depth d on); *differs is set when the two strings are not equal.
-// Gives up (returning a value > stop) once the shared length exceeds `stop`,
-// which then cannot lower the segment minimum.
-__device__ __forceinline__ uint32_t shared_chars(const Work& w, uint64_t boff, uint32_t id,
+// Chars the string behind handle h shares with the base string (at arena
+// offset boff, both from depth d on); *differs is set when the two strings
+// are not equal. Gives up (returning a value > stop) once the shared length
+// exceeds `stop`, which then cannot lower the segment minimum. Two 8-byte
+// chunks per step keep two loads of each string in flight.
+__device__ __forceinline__ uint32_t shared_chars(const Work& w, uint64_t boff, uint64_t h,
                                                  uint32_t d, uint32_t stop, bool* differs)
 {
-    const uint64_t o = __ldg(w.offs + id) + d;
-    for (uint32_t c = 0;; ++c) {
+    const uint64_t o = h_off(w, h) + d;
+    for (uint32_t c = 0;; c += 2) {
         if (8u * c > stop) return 8u * c;
-        const uint64_t ka = load_key(w.chars, w.nchars, boff + 8ull * c);
-        const uint64_t kb = load_key(w.chars, w.nchars, o + 8ull * c);
-        if (ka != kb) {
+        const uint64_t ka0 = load_key(w.chars, w.nchars, boff + 8ull * c);
+        const uint64_t kb0 = load_key(w.chars, w.nchars, o + 8ull * c);
+        const uint64_t ka1 = load_key(w.chars, w.nchars, boff + 8ull * c + 8);
+        const uint64_t kb1 = load_key(w.chars, w.nchars, o + 8ull * c + 8);
+        if (ka0 != kb0) {
             *differs = true;
-            return 8u * c + lcp_key_type(ka, kb);
+            return 8u * c + lcp_key_type(ka0, kb0);
         }
-        if (key_terminated(ka)) return 8u * c + lcp_key_depth(ka);
+        if (key_terminated(ka0)) return 8u * c + lcp_key_depth(ka0);
+        if (ka1 != kb1) {
+            *differs = true;
+            return 8u * c + 8 + lcp_key_type(ka1, kb1);
+        }
+        if (key_terminated(ka1)) return 8u * c + 8 + lcp_key_depth(ka1);
     }
 }
 
@@ -163,10 +171,10 @@ __global__ void __launch_bounds__(TILE_THREADS) k_classify(Work w, uint32_t nbig
     const uint32_t lo = sg.begin + (t - w.tile_start[s]) * TILE;
     const uint32_t hi = min(lo + TILE, sg.begin + sg.size);
     const int buf = sg.meta & META_BUF;
-    const uint32_t* ids = w.ids[buf];
+    const uint64_t* hs = w.hnd[buf];
     if (sg.meta & META_FINAL) {
         for (uint32_t p = lo + threadIdx.x; p < hi; p += TILE_THREADS) {
-            w.perm[p] = ids[p];
+            w.perm[p] = h_id(w, hs[p]);
             if (w.lcp && p > sg.begin) w.lcp[p] = sg.depth;
         }
         return;
@@ -178,11 +186,11 @@ __global__ void __launch_bounds__(TILE_THREADS) k_classify(Work w, uint32_t nbig
             anydiff = 0;
         }
         __syncthreads();
-        const uint64_t boff = __ldg(w.offs + ids[sg.begin]) + sg.depth;
+        const uint64_t boff = h_off(w, hs[sg.begin]) + sg.depth;
         bool differs = false;
         for (uint32_t p = lo + threadIdx.x; p < hi; p += TILE_THREADS) {
             const uint32_t stop = *((volatile uint32_t*)&best);
-            const uint32_t l = shared_chars(w, boff, ids[p], sg.depth, stop, &differs);
+            const uint32_t l = shared_chars(w, boff, hs[p], sg.depth, stop, &differs);
             if (l < stop) atomicMin(&best, l);
         }
         if (differs) anydiff = 1;
@@ -206,7 +214,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_classify(Work w, uint32_t nbig
         if (valid) {
             key = keys[p];
         } else {
-            key = gather_key(w.chars, w.nchars, w.offs, ids[p], sg.depth);
+            key = h_key(w, hs[p], sg.depth);
             keys[p] = key;
         }
         uint32_t i = 1;
@@ -270,12 +278,10 @@ __device__ __forceinline__ uint64_t lb_word(uint32_t epoch, uint64_t flag, uint6
 }
 
 struct ScatterSmem {
-    uint64_t key[TILE];
-    uint32_t id[TILE];
-    uint16_t bkt[TILE];
-    uint32_t lcount[MAX_BKT];
-    uint32_t lstart[MAX_BKT];
-    uint32_t gbase[MAX_BKT];
+    uint64_t stage[TILE];      // the tile's keys in bucket order, then its handles
+    uint16_t sbkt[TILE];       // bucket of each staged slot
+    uint32_t lcount[MAX_BKT];  // per-bucket count in the tile, then its start
+    uint32_t gdelta[MAX_BKT];  // per bucket: global position - tile slot
     uint32_t tmp[32];
     uint32_t vt;
 };
@@ -285,14 +291,9 @@ struct ScatterSmem {
 __global__ void __launch_bounds__(TILE_THREADS) k_scatter(Work w, uint32_t nbig)
 {
     constexpr int PER = TILE / TILE_THREADS;
+    constexpr int NB = MAX_BKT / TILE_THREADS;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ScatterSmem& sm = *reinterpret_cast<ScatterSmem*>(smem_raw);
-    uint64_t* skey = sm.key;
-    uint32_t* sid = sm.id;
-    uint16_t* sbkt = sm.bkt;
-    uint32_t* lcount = sm.lcount;
-    uint32_t* lstart = sm.lstart;
-    uint32_t* gbase = sm.gbase;
     if (threadIdx.x == 0) sm.vt = atomicAdd(w.counters + C_TICKET, 1u);
     __syncthreads();
     const uint32_t vt = sm.vt;
@@ -306,18 +307,17 @@ __global__ void __launch_bounds__(TILE_THREADS) k_scatter(Work w, uint32_t nbig)
     const uint32_t cnt = hi - lo;
     const uint32_t B = (2u << L) - 1;
     const int buf = sg.meta & META_BUF;
-    for (uint32_t b = threadIdx.x; b < B; b += TILE_THREADS) lcount[b] = 0;
+    for (uint32_t b = threadIdx.x; b < B; b += TILE_THREADS) sm.lcount[b] = 0;
     __syncthreads();
-    uint64_t key[PER];
-    uint32_t id[PER], bk[PER], rank[PER];
+    // rank of every string inside its bucket in this tile: (bucket << 16) | rank
+    uint32_t pk[PER];
 #pragma unroll
     for (int j = 0; j < PER; ++j) {
         const uint32_t p = lo + threadIdx.x + j * TILE_THREADS;
+        pk[j] = 0xFFFFFFFFu;
         if (p < hi) {
-            key[j] = w.keys[buf][p];
-            id[j] = w.ids[buf][p];
-            bk[j] = w.bkt[p];
-            rank[j] = atomicAdd(&lcount[bk[j]], 1u);
+            const uint32_t b = w.bkt[p];
+            pk[j] = (b << 16) | atomicAdd(&sm.lcount[b], 1u);
         }
     }
     __syncthreads();
@@ -325,61 +325,99 @@ __global__ void __launch_bounds__(TILE_THREADS) k_scatter(Work w, uint32_t nbig)
     volatile uint64_t* st = w.status + (size_t)vt * MAX_BKT;
     const uint32_t ep = w.epoch;
     for (uint32_t b = threadIdx.x; b < B; b += TILE_THREADS)
-        st[b] = lb_word(ep, tin == 0 ? LB_PRE : LB_AGG, lcount[b]);
-    const uint32_t* bs = w.bstart + (size_t)s * MAX_BKT;
-    for (uint32_t b = threadIdx.x; b < B; b += TILE_THREADS) {
-        uint64_t excl = 0;
-        if (tin > 0) {
-            uint32_t j = vt - 1;
-            uint32_t spins = 0;
-            while (true) {
-                const uint64_t wd = *((volatile uint64_t*)(w.status + (size_t)j * MAX_BKT + b));
-                const uint64_t flag = (wd >> 46) & 3u;
-                if ((uint32_t)(wd >> 48) != ep || flag == 0) {
-                    // bounded wait: give up (and make every later wait give up
-                    // at once) after SPIN_CAP polls
-                    if (++spins > SPIN_CAP ||
-                        (*((volatile uint32_t*)(w.counters + C_ERR)) & ERR_TIMEOUT)) {
-                        set_error(w.counters + C_ERR, ERR_TIMEOUT);
-                        break;
-                    }
-                    if (spins > 64) __nanosleep(64);
-                    continue;
-                }
-                excl += wd & ((1ull << 46) - 1);
-                if (flag == LB_PRE) break;
-                --j;
+        st[b] = lb_word(ep, tin == 0 ? LB_PRE : LB_AGG, sm.lcount[b]);
+    // Look back for every bucket this thread owns at once: each round issues
+    // one status load per unfinished bucket, so the chains overlap in memory.
+    uint64_t excl[NB];
+    uint32_t jb[NB];
+    uint32_t open = 0;  // bit i: bucket threadIdx.x + i * TILE_THREADS still walking
+#pragma unroll
+    for (int i = 0; i < NB; ++i) {
+        excl[i] = 0;
+        jb[i] = vt - 1;
+        const uint32_t b = threadIdx.x + i * TILE_THREADS;
+        if (tin > 0 && b < B) open |= 1u << i;
+    }
+    uint32_t spins = 0;
+    while (open) {
+        uint64_t wd[NB];
+#pragma unroll
+        for (int i = 0; i < NB; ++i)
+            if (open & (1u << i))
+                wd[i] = *((volatile uint64_t*)(w.status + (size_t)jb[i] * MAX_BKT + threadIdx.x +
+                                               i * TILE_THREADS));
+        bool waiting = false;
+#pragma unroll
+        for (int i = 0; i < NB; ++i) {
+            if (!(open & (1u << i))) continue;
+            const uint64_t flag = (wd[i] >> 46) & 3u;
+            if ((uint32_t)(wd[i] >> 48) != ep || flag == 0) {
+                waiting = true;
+                continue;
             }
-            st[b] = lb_word(ep, LB_PRE, excl + lcount[b]);
+            excl[i] += wd[i] & ((1ull << 46) - 1);
+            if (flag == LB_PRE) open &= ~(1u << i);
+            else --jb[i];
         }
-        gbase[b] = sg.begin + bs[b] + (uint32_t)excl;
-        lstart[b] = lcount[b];
+        if (waiting) {
+            // bounded wait: give up (and make every later wait give up at
+            // once) after SPIN_CAP polls
+            if (++spins > SPIN_CAP || (*((volatile uint32_t*)(w.counters + C_ERR)) & ERR_TIMEOUT)) {
+                set_error(w.counters + C_ERR, ERR_TIMEOUT);
+                break;
+            }
+            if (spins > 64) __nanosleep(64);
+        }
+    }
+    if (tin > 0) {
+#pragma unroll
+        for (int i = 0; i < NB; ++i) {
+            const uint32_t b = threadIdx.x + i * TILE_THREADS;
+            if (b < B) st[b] = lb_word(ep, LB_PRE, excl[i] + sm.lcount[b]);
+        }
     }
     __syncthreads();
-    block_scan_array<TILE_THREADS>(lstart, (int)B, sm.tmp);
-    // stage the tile in bucket order, then write bucket runs contiguously
+    block_scan_array<TILE_THREADS>(sm.lcount, (int)B, sm.tmp);  // counts -> tile starts
+    const uint32_t* bs = w.bstart + (size_t)s * MAX_BKT;
+#pragma unroll
+    for (int i = 0; i < NB; ++i) {
+        const uint32_t b = threadIdx.x + i * TILE_THREADS;
+        if (b < B) sm.gdelta[b] = sg.begin + bs[b] + (uint32_t)excl[i] - sm.lcount[b];
+    }
+    // stage keys in bucket order and write bucket runs contiguously; then ids
+    const uint64_t* ikeys = w.keys[buf];
 #pragma unroll
     for (int j = 0; j < PER; ++j) {
-        const uint32_t p = lo + threadIdx.x + j * TILE_THREADS;
-        if (p < hi) {
-            const uint32_t slot = lstart[bk[j]] + rank[j];
-            skey[slot] = key[j];
-            sid[slot] = id[j];
-            sbkt[slot] = (uint16_t)bk[j];
-        }
+        if (pk[j] == 0xFFFFFFFFu) continue;
+        const uint32_t b = pk[j] >> 16;
+        const uint32_t slot = sm.lcount[b] + (pk[j] & 0xFFFFu);
+        sm.stage[slot] = ikeys[lo + threadIdx.x + j * TILE_THREADS];
+        sm.sbkt[slot] = (uint16_t)b;
     }
     __syncthreads();
     uint64_t* okeys = w.keys[buf ^ 1];
-    uint32_t* oids = w.ids[buf ^ 1];
     for (uint32_t slot = threadIdx.x; slot < cnt; slot += TILE_THREADS) {
-        const uint32_t b = sbkt[slot];
-        const uint32_t dest = gbase[b] + (slot - lstart[b]);
+        const uint32_t dest = slot + sm.gdelta[sm.sbkt[slot]];
         if (dest - sg.begin >= sg.size) {  // only after a failed look-back
             set_error(w.counters + C_ERR, ERR_INTERNAL);
             continue;
         }
-        okeys[dest] = skey[slot];
-        oids[dest] = sid[slot];
+        okeys[dest] = sm.stage[slot];
+    }
+    __syncthreads();
+    const uint64_t* ihs = w.hnd[buf];
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+        if (pk[j] == 0xFFFFFFFFu) continue;
+        const uint32_t slot = sm.lcount[pk[j] >> 16] + (pk[j] & 0xFFFFu);
+        sm.stage[slot] = ihs[lo + threadIdx.x + j * TILE_THREADS];
+    }
+    __syncthreads();
+    uint64_t* ohs = w.hnd[buf ^ 1];
+    for (uint32_t slot = threadIdx.x; slot < cnt; slot += TILE_THREADS) {
+        const uint32_t dest = slot + sm.gdelta[sm.sbkt[slot]];
+        if (dest - sg.begin >= sg.size) continue;
+        ohs[dest] = sm.stage[slot];
     }
 }
 
@@ -421,23 +459,35 @@ __global__ void __launch_bounds__(1024) k_children(Work w)
         return;
     }
     if (!classified(L)) return;
+    // block-aggregated appends: slots in shared memory first, then one
+    // global reservation per list
+    __shared__ uint32_t lcnt[L_NCLASS], gbase[L_NCLASS];
+    __shared__ uint32_t ltiles, lbnd, bbase;
+    if (threadIdx.x < L_NCLASS) lcnt[threadIdx.x] = 0;
+    if (threadIdx.x == 0) { ltiles = 0; lbnd = 0; }
+    __syncthreads();
     const uint32_t B = (2u << L) - 1;
     const int nbuf = w.bflags[s] ? buf : buf ^ 1;
     const uint32_t* bc = w.bcount + (size_t)s * MAX_BKT;
     const uint32_t* bs = w.bstart + (size_t)s * MAX_BKT;
     const uint64_t* spl = w.spl + (size_t)s * 1024;
-    const uint32_t* ids = w.ids[nbuf];
-    for (uint32_t b = threadIdx.x; b < B; b += blockDim.x) {
+    const uint64_t* hs = w.hnd[nbuf];
+    constexpr int PER = (MAX_BKT + 1023) / 1024;
+    Seg child[PER];
+    int cls[PER];
+    uint32_t slot[PER], bslot[PER];
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+        cls[j] = -1;
+        bslot[j] = 0xFFFFFFFFu;
+        const uint32_t b = threadIdx.x + 1024u * j;
+        if (b >= B) continue;
         const uint32_t c = bc[b];
         if (c == 0) continue;
         const uint32_t P = sg.begin + bs[b];
-        if (P > sg.begin && w.lcp) {
-            const uint32_t at = atomicAdd(w.counters + C_NBND, 1u);
-            if (at < w.bnd_cap) w.bnd[at] = make_uint2(P, sg.depth);
-            else set_error(w.counters + C_ERR, ERR_OVERFLOW);
-        }
+        if (P > sg.begin && w.lcp) bslot[j] = atomicAdd(&lbnd, 1u);
         if (c == 1) {
-            w.perm[P] = ids[P];
+            w.perm[P] = h_id(w, hs[P]);
             continue;
         }
         if (b & 1) {
@@ -446,17 +496,44 @@ __global__ void __launch_bounds__(1024) k_children(Work w)
                 const uint32_t v = sg.depth + lcp_key_depth(key);
                 if (c <= FINAL_INLINE) {
                     for (uint32_t q = 0; q < c; ++q) {
-                        w.perm[P + q] = ids[P + q];
+                        w.perm[P + q] = h_id(w, hs[P + q]);
                         if (w.lcp && q) w.lcp[P + q] = v;
                     }
-                } else {
-                    push_seg(w, nxt, Seg{P, c, v, (uint32_t)nbuf | META_FINAL});
+                    continue;
                 }
+                child[j] = Seg{P, c, v, (uint32_t)nbuf | META_FINAL};
             } else {
-                push_seg(w, nxt, Seg{P, c, sg.depth + 8, (uint32_t)nbuf});
+                child[j] = Seg{P, c, sg.depth + 8, (uint32_t)nbuf};
             }
         } else {
-            push_seg(w, nxt, Seg{P, c, sg.depth, (uint32_t)nbuf | META_VALID});
+            child[j] = Seg{P, c, sg.depth, (uint32_t)nbuf | META_VALID};
+        }
+        if (c > SMALL_MAX) cls[j] = L_BIG;
+        else if (c > 256) cls[j] = L_SMALLB;
+        else if (c > WARP_GROUP_MAX) cls[j] = L_SMALLA;
+        else cls[j] = L_TINY;
+        slot[j] = atomicAdd(&lcnt[cls[j]], 1u);
+        if (cls[j] == L_BIG) atomicAdd(&ltiles, (c + TILE - 1) / TILE);
+    }
+    __syncthreads();
+    if (threadIdx.x < L_NCLASS && lcnt[threadIdx.x])
+        gbase[threadIdx.x] = atomicAdd(w.counters + C_PAR * nxt + threadIdx.x, lcnt[threadIdx.x]);
+    if (threadIdx.x == 32 && ltiles) atomicAdd(w.counters + C_PAR * nxt + C_NTILES, ltiles);
+    if (threadIdx.x == 64 && lbnd) bbase = atomicAdd(w.counters + C_NBND, lbnd);
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+        const uint32_t b = threadIdx.x + 1024u * j;
+        if (b >= B) continue;
+        if (bslot[j] != 0xFFFFFFFFu) {
+            const uint32_t at = bbase + bslot[j];
+            if (at < w.bnd_cap) w.bnd[at] = make_uint2(sg.begin + bs[b], sg.depth);
+            else set_error(w.counters + C_ERR, ERR_OVERFLOW);
+        }
+        if (cls[j] >= 0) {
+            const uint32_t at = gbase[cls[j]] + slot[j];
+            if (at < w.cap[cls[j]]) w.list[cls[j]][nxt][at] = child[j];
+            else set_error(w.counters + C_ERR, ERR_OVERFLOW);
         }
     }
 }

@@ -7,10 +7,10 @@
 // (src/sequential/bingmann-lcp_inssort.hpp:38-189).
 //
 // Size classes (push_seg in kernels_big.cuh picks the list):
-//   k_tiny           <= 32 strings, one warp per segment, shuffles only
-//   k_small<256,128> <= 256 strings, one block
+//   k_tiny            <= 32 strings, one warp per segment, shuffles only
+//   k_small<256,128>  <= 256 strings, one block
 //   k_small<2048,256> <= 2048 strings, one block
-// Block phase: sort (group, key, id) with a shared-memory bitonic sort;
+// Block phase: sort (group, key, handle) with a shared-memory bitonic sort;
 // runs of equal keys become groups one 8-byte round deeper; a group that
 // stops splitting jumps to its common prefix. Groups of <= 32 strings are
 // parked and finished by the warp phase (the k_tiny rounds), where a group
@@ -26,7 +26,7 @@ namespace pssgpu {
 template <int MAXN>
 struct SmallSmem {
     uint64_t key[MAXN];
-    uint32_t id[MAXN];
+    uint64_t hnd[MAXN];
     uint32_t gdep[MAXN];   // depth of the active group starting here
     uint32_t ndep[MAXN];   // next depth, staged
     uint16_t grp[MAXN];    // start index of the element's group
@@ -44,22 +44,22 @@ struct SmallSmem {
     uint32_t jump;
 };
 
-__device__ __forceinline__ bool tuple_less(uint32_t ga, uint64_t ka, uint32_t ia,
-                                           uint32_t gb, uint64_t kb, uint32_t ib)
+__device__ __forceinline__ bool tuple_less(uint32_t ga, uint64_t ka, uint64_t ha,
+                                           uint32_t gb, uint64_t kb, uint64_t hb)
 {
     if (ga != gb) return ga < gb;
     if (ka != kb) return ka < kb;
-    return ia < ib;
+    return ha < hb;
 }
 
-// Common-prefix extension (in 8-byte chunks from depth d) of `other`
-// against `base`: the first chunk where they differ or base ends, at most
-// `limit`.
-__device__ __forceinline__ uint32_t chunks_equal(const Work& w, uint32_t base, uint32_t other,
+// Common-prefix extension (in 8-byte chunks from depth d) of the string
+// behind handle `other` against the one behind `base`: the first chunk where
+// they differ or base ends, at most `limit`.
+__device__ __forceinline__ uint32_t chunks_equal(const Work& w, uint64_t base, uint64_t other,
                                                  uint32_t d, uint32_t limit)
 {
     uint32_t c = 0;
-    const uint64_t ob = __ldg(w.offs + base) + d, oo = __ldg(w.offs + other) + d;
+    const uint64_t ob = h_off(w, base) + d, oo = h_off(w, other) + d;
     while (c < limit) {
         const uint64_t ka = load_key(w.chars, w.nchars, ob + 8ull * c);
         const uint64_t kb = load_key(w.chars, w.nchars, oo + 8ull * c);
@@ -70,16 +70,18 @@ __device__ __forceinline__ uint32_t chunks_equal(const Work& w, uint32_t base, u
 }
 
 // Warp rounds for one group of c <= 32 strings sharing d chars; lane i holds
-// id i on entry and the i-th smallest id on return. LCPs go to
-// lcp[pos0 + lane] for lanes >= 1. first_keys (may be null) holds the keys at
-// depth d, saving the first gather.
-__device__ uint32_t warp_rounds(const Work& w, uint32_t myid, uint32_t c, uint32_t d,
-                                uint32_t pos0, const uint64_t* first_keys)
+// handle i on entry and the i-th smallest handle's string on return. LCPs go
+// to lcp[pos0 + lane] for lanes >= 1. first_keys (may be null) holds the keys
+// at depth d, saving the first gather. Each round sorts (group, key, source
+// lane) with a 32-lane bitonic network on three shuffled words and then
+// fetches the rest of the element from its source lane.
+__device__ __forceinline__ uint64_t warp_rounds(const Work& w, uint64_t myh, uint32_t c,
+                                                uint32_t d, uint32_t pos0,
+                                                const uint64_t* first_keys)
 {
     const uint32_t lane = threadIdx.x & 31;
     const bool real = lane < c;
-    if (!real) myid = 0xFFFFFFFFu;
-    uint32_t mygrp = real ? 0u : 0xFFFFFFFFu;
+    uint32_t mygrp = real ? 0u : 32u;   // lanes past c sort last
     uint32_t mydep = d;
     uint32_t mystate = real ? 0u : 1u;  // 0 active, 1 done
     uint64_t mykey = 0;
@@ -93,16 +95,16 @@ __device__ uint32_t warp_rounds(const Work& w, uint32_t myid, uint32_t c, uint32
             // exactly one active group that did not split: jump to its
             // common prefix, 32 chunks of 8 bytes per step
             const int f = __ffs(A) - 1;
-            const uint32_t base = __shfl_sync(0xffffffffu, myid, f);
+            const uint64_t base = __shfl_sync(0xffffffffu, myh, f);
             const uint32_t dd = __shfl_sync(0xffffffffu, mydep, f);
             uint32_t best = 0xFFFFFFFFu;
             uint32_t rest = A & ~(1u << f);
-            const uint64_t ob = __ldg(w.offs + base) + dd;
+            const uint64_t ob = h_off(w, base) + dd;
             while (rest) {
                 const int j = __ffs(rest) - 1;
                 rest &= rest - 1;
-                const uint32_t other = __shfl_sync(0xffffffffu, myid, j);
-                const uint64_t oo = __ldg(w.offs + other) + dd;
+                const uint64_t other = __shfl_sync(0xffffffffu, myh, j);
+                const uint64_t oo = h_off(w, other) + dd;
                 for (uint32_t t = 0; t * 32 < best; ++t) {
                     const uint32_t ch = t * 32 + lane;
                     const uint64_t ka = load_key(w.chars, w.nchars, ob + 8ull * ch);
@@ -116,27 +118,32 @@ __device__ uint32_t warp_rounds(const Work& w, uint32_t myid, uint32_t c, uint32
             }
             if (mystate == 0) mydep = dd + 8u * best;
         }
-        if (mystate == 0)
-            mykey = first ? first_keys[lane] : gather_key(w.chars, w.nchars, w.offs, myid, mydep);
+        if (mystate == 0) mykey = first ? first_keys[lane] : h_key(w, myh, mydep);
         first = false;
-        // bitonic sort of the 32 lanes by (grp, key, id), carrying dep/state
+        uint32_t tag = (mygrp << 5) | lane;
+        uint64_t k = mykey;
 #pragma unroll
         for (uint32_t kk = 2; kk <= 32; kk <<= 1) {
 #pragma unroll
             for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
-                const uint32_t og = __shfl_xor_sync(0xffffffffu, mygrp, j);
-                const uint64_t ok = __shfl_xor_sync(0xffffffffu, mykey, j);
-                const uint32_t oi = __shfl_xor_sync(0xffffffffu, myid, j);
-                const uint32_t od = __shfl_xor_sync(0xffffffffu, mydep, j);
-                const uint32_t os = __shfl_xor_sync(0xffffffffu, mystate, j);
+                const uint32_t ot = __shfl_xor_sync(0xffffffffu, tag, j);
+                const uint64_t ok = __shfl_xor_sync(0xffffffffu, k, j);
                 const bool lower = (lane & j) == 0;
                 const bool asc = (lane & kk) == 0;
-                const bool other_less = tuple_less(og, ok, oi, mygrp, mykey, myid);
+                bool other_less;
+                if ((ot >> 5) != (tag >> 5)) other_less = (ot >> 5) < (tag >> 5);
+                else if (ok != k) other_less = ok < k;
+                else other_less = (ot & 31u) < (tag & 31u);
                 // the lower lane of an ascending pair keeps the smaller
-                const bool take = (lower == asc) ? other_less : !other_less;
-                if (take) { mygrp = og; mykey = ok; myid = oi; mydep = od; mystate = os; }
+                if ((lower == asc) ? other_less : !other_less) { tag = ot; k = ok; }
             }
         }
+        const uint32_t src = tag & 31u;
+        myh = __shfl_sync(0xffffffffu, myh, src);
+        mydep = __shfl_sync(0xffffffffu, mydep, src);
+        mystate = __shfl_sync(0xffffffffu, mystate, src);
+        mygrp = tag >> 5;
+        mykey = k;
         const uint32_t pg = __shfl_up_sync(0xffffffffu, mygrp, 1);
         const uint64_t pk = __shfl_up_sync(0xffffffffu, mykey, 1);
         const bool ns = lane == 0 || mygrp != pg || mykey != pk;
@@ -162,7 +169,7 @@ __device__ uint32_t warp_rounds(const Work& w, uint32_t myid, uint32_t c, uint32
         stalled = (na == prev_active) && (__popc(G2) == 1);
         prev_active = na;
     }
-    return myid;
+    return myh;
 }
 
 // One warp per segment of at most 32 strings; 8 segments per block.
@@ -175,13 +182,13 @@ __global__ void __launch_bounds__(32 * TINY_WARPS) k_tiny(Work w, const Seg* lis
     const Seg sg = list[g];
     const int buf = sg.meta & META_BUF;
     if (lane == 0) atomicAdd(w.counters + C_P_SMALL, sg.size);
-    uint32_t myid = lane < sg.size ? w.ids[buf][sg.begin + lane] : 0xFFFFFFFFu;
+    uint64_t myh = lane < sg.size ? w.hnd[buf][sg.begin + lane] : ~0ull;
     const uint64_t* fk = (sg.meta & META_VALID) ? w.keys[buf] + sg.begin : nullptr;
-    myid = warp_rounds(w, myid, sg.size, sg.depth, sg.begin, fk);
-    if (lane < sg.size) w.perm[sg.begin + lane] = myid;
+    myh = warp_rounds(w, myh, sg.size, sg.depth, sg.begin, fk);
+    if (lane < sg.size) w.perm[sg.begin + lane] = h_id(w, myh);
 }
 
-// Bitonic sort of sm.{grp,key,id}[0, npad) by (grp, key, id).
+// Bitonic sort of sm.{grp,key,hnd}[0, npad) by (grp, key, hnd).
 template <int MAXN, int THREADS>
 __device__ void small_bitonic(SmallSmem<MAXN>& sm, uint32_t npad)
 {
@@ -193,11 +200,11 @@ __device__ void small_bitonic(SmallSmem<MAXN>& sm, uint32_t npad)
                 const bool asc = (a & kk) == 0;
                 const uint32_t ga = sm.grp[a], gb = sm.grp[b];
                 const uint64_t ka = sm.key[a], kb = sm.key[b];
-                const uint32_t ia = sm.id[a], ib = sm.id[b];
-                if (tuple_less(gb, kb, ib, ga, ka, ia) == asc) {
+                const uint64_t ha = sm.hnd[a], hb = sm.hnd[b];
+                if (tuple_less(gb, kb, hb, ga, ka, ha) == asc) {
                     sm.grp[a] = (uint16_t)gb; sm.grp[b] = (uint16_t)ga;
                     sm.key[a] = kb; sm.key[b] = ka;
-                    sm.id[a] = ib; sm.id[b] = ia;
+                    sm.hnd[a] = hb; sm.hnd[b] = ha;
                 }
             }
             __syncthreads();
@@ -214,11 +221,11 @@ __global__ void __launch_bounds__(THREADS) k_small(Work w, const Seg* list)
     const Seg sg = list[blockIdx.x];
     const uint32_t m = sg.size, begin = sg.begin;
     const int buf = sg.meta & META_BUF;
-    const uint32_t* gids = w.ids[buf];
+    const uint64_t* ghs = w.hnd[buf];
     if (threadIdx.x == 0) atomicAdd(w.counters + C_P_SMALL, m);
     if (sg.meta & META_FINAL) {
         for (uint32_t i = threadIdx.x; i < m; i += THREADS) {
-            w.perm[begin + i] = gids[begin + i];
+            w.perm[begin + i] = h_id(w, ghs[begin + i]);
             if (w.lcp && i) w.lcp[begin + i] = sg.depth;
         }
         return;
@@ -227,7 +234,7 @@ __global__ void __launch_bounds__(THREADS) k_small(Work w, const Seg* list)
         sm.npark = 0;
         atomicAdd(w.counters + C_SMALLSEGS, 1u);
     }
-    for (uint32_t i = threadIdx.x; i < m; i += THREADS) sm.id[i] = gids[begin + i];
+    for (uint32_t i = threadIdx.x; i < m; i += THREADS) sm.hnd[i] = ghs[begin + i];
     __syncthreads();
     if (m <= (uint32_t)WARP_GROUP_MAX) {
         if (threadIdx.x == 0) {
@@ -242,13 +249,12 @@ __global__ void __launch_bounds__(THREADS) k_small(Work w, const Seg* list)
         const bool valid = sg.meta & META_VALID;
         for (uint32_t i = threadIdx.x; i < npad; i += THREADS) {
             if (i < m) {
-                sm.key[i] = valid ? w.keys[buf][begin + i]
-                                  : gather_key(w.chars, w.nchars, w.offs, sm.id[i], sg.depth);
+                sm.key[i] = valid ? w.keys[buf][begin + i] : h_key(w, sm.hnd[i], sg.depth);
                 sm.grp[i] = 0;
                 sm.state[i] = 0;
             } else {
                 sm.key[i] = ~0ull;
-                sm.id[i] = 0xFFFFFFFFu;
+                sm.hnd[i] = ~0ull;
                 sm.grp[i] = 0xFFFF;
                 sm.state[i] = 1;
             }
@@ -264,21 +270,20 @@ __global__ void __launch_bounds__(THREADS) k_small(Work w, const Seg* list)
                 // one active group that did not split: jump to its common prefix
                 const uint32_t g0 = sm.g0;
                 const uint32_t d0 = sm.gdep[g0];
-                const uint32_t base = sm.id[g0];
+                const uint64_t base = sm.hnd[g0];
                 if (threadIdx.x == 0) sm.jump = 0xFFFFFFFFu;
                 __syncthreads();
                 for (uint32_t i = threadIdx.x; i < m; i += THREADS) {
                     if (sm.state[i] != 0 || i == g0) continue;
                     const uint32_t lim = *((volatile uint32_t*)&sm.jump);
-                    const uint32_t c = chunks_equal(w, base, sm.id[i], d0, lim);
-                    atomicMin(&sm.jump, c);
+                    const uint32_t cc = chunks_equal(w, base, sm.hnd[i], d0, lim);
+                    atomicMin(&sm.jump, cc);
                 }
                 __syncthreads();
                 if (threadIdx.x == 0) sm.gdep[g0] = d0 + 8u * sm.jump;
                 __syncthreads();
                 for (uint32_t i = threadIdx.x; i < m; i += THREADS)
-                    if (sm.state[i] == 0)
-                        sm.key[i] = gather_key(w.chars, w.nchars, w.offs, sm.id[i], sm.gdep[sm.grp[i]]);
+                    if (sm.state[i] == 0) sm.key[i] = h_key(w, sm.hnd[i], sm.gdep[sm.grp[i]]);
                 __syncthreads();
             }
             small_bitonic<MAXN, THREADS>(sm, npad);
@@ -350,8 +355,7 @@ __global__ void __launch_bounds__(THREADS) k_small(Work w, const Seg* list)
             prev_active = na;
             if (!stalled) {
                 for (uint32_t i = threadIdx.x; i < m; i += THREADS)
-                    if (sm.state[i] == 0)
-                        sm.key[i] = gather_key(w.chars, w.nchars, w.offs, sm.id[i], sm.gdep[sm.grp[i]]);
+                    if (sm.state[i] == 0) sm.key[i] = h_key(w, sm.hnd[i], sm.gdep[sm.grp[i]]);
             }
         }
         __syncthreads();
@@ -361,12 +365,12 @@ __global__ void __launch_bounds__(THREADS) k_small(Work w, const Seg* list)
     const uint32_t np = sm.npark;
     for (uint32_t g = warp; g < np; g += THREADS / 32) {
         const uint32_t start = sm.park_start[g], c = sm.park_len[g];
-        uint32_t myid = lane < c ? sm.id[start + lane] : 0xFFFFFFFFu;
-        myid = warp_rounds(w, myid, c, sm.park_dep[g], begin + start, nullptr);
-        if (lane < c) sm.id[start + lane] = myid;
+        uint64_t myh = lane < c ? sm.hnd[start + lane] : ~0ull;
+        myh = warp_rounds(w, myh, c, sm.park_dep[g], begin + start, nullptr);
+        if (lane < c) sm.hnd[start + lane] = myh;
     }
     __syncthreads();
-    for (uint32_t i = threadIdx.x; i < m; i += THREADS) w.perm[begin + i] = sm.id[i];
+    for (uint32_t i = threadIdx.x; i < m; i += THREADS) w.perm[begin + i] = h_id(w, sm.hnd[i]);
 }
 
 // the two block-sized classes

@@ -41,7 +41,7 @@ static int fail(int code, const std::string& msg)
 __global__ void k_init(Work w)
 {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < w.n; i += gridDim.x * blockDim.x) {
-        w.ids[0][i] = i;
+        w.hnd[0][i] = h_make(w, i, w.offs[i]);
         if (w.offs[i] >= w.nchars) set_error(w.counters + C_ERR, ERR_OFFSET);
     }
 }
@@ -49,6 +49,17 @@ __global__ void k_init(Work w)
 __global__ void k_root(Work w)
 {
     push_seg(w, 0, Seg{0u, w.n, 0u, 0u});
+}
+
+static uint32_t bit_length(uint64_t x) { return x ? 64u - (uint32_t)__builtin_clzll(x) : 0u; }
+
+// Packed handles (id << hbits | offset) when id and offset fit 64 bits.
+static void set_handle_format(Work& w, bool force_indirect)
+{
+    w.hbits = std::max<uint32_t>(1, bit_length(w.nchars ? w.nchars - 1 : 0));
+    w.hmask = w.hbits >= 64 ? ~0ull : ((1ull << w.hbits) - 1);
+    const uint32_t idbits = bit_length(w.n ? w.n - 1 : 0);
+    w.packed = (!force_indirect && w.hbits <= 63 && idbits + w.hbits <= 64) ? 1 : 0;
 }
 
 struct Sizes {
@@ -74,7 +85,7 @@ static uint64_t workspace_bytes(const Sizes& s)
 {
     const uint64_t big = s.cap[L_BIG];
     uint64_t b = 0;
-    b += 2 * align256(4 * s.n);                    // ids
+    b += 2 * align256(8 * s.n);                    // string handles
     b += 2 * align256(8 * s.n);                    // keys
     b += align256(2 * s.n);                        // bucket ids
     b += align256(8 * s.n);                        // boundary list
@@ -121,6 +132,9 @@ struct Ctx {
     pssgpu_stats stats{};
     // profile mode: events around every kernel class, per-class totals
     bool profile = false;
+    // carry bare ids and read offsets through offs[] (the path taken when
+    // id and offset do not fit one 64-bit handle); settable for testing
+    bool indirect_handles = false;
     cudaEvent_t kev[2 * K_NCLASS] = {};
     KStat kstat[K_NCLASS];
 };
@@ -168,7 +182,7 @@ static int ensure_workspace(Ctx* c, uint64_t n)
     auto take = [&](uint64_t b) { unsigned char* r = p; p += align256(b); return r; };
     Work& w = c->base;
     w = Work{};
-    for (int i = 0; i < 2; ++i) w.ids[i] = (uint32_t*)take(4 * s.n);
+    for (int i = 0; i < 2; ++i) w.hnd[i] = (uint64_t*)take(8 * s.n);
     for (int i = 0; i < 2; ++i) w.keys[i] = (uint64_t*)take(8 * s.n);
     w.bkt = (uint16_t*)take(2 * s.n);
     w.bnd = (uint2*)take(8 * s.n);
@@ -239,6 +253,7 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
     w.n = n;
     w.perm = perm;
     w.lcp = lcp;
+    set_handle_format(w, c->indirect_handles);
     pssgpu_stats stats{};
     for (int k = 0; k < K_NCLASS; ++k) c->kstat[k] = KStat{};
     KTimer kt{c, st};
@@ -584,6 +599,18 @@ int pssgpu_ctx_set_profile(pssgpu_ctx* ctx, int on)
     return PSSGPU_OK;
 }
 
+int pssgpu_ctx_set_option(pssgpu_ctx* ctx, int option, int64_t value)
+{
+    if (!ctx) return fail(PSSGPU_EINVAL, "null context");
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    std::lock_guard<std::mutex> lk(c->mu);
+    switch (option) {
+    case PSSGPU_OPT_PROFILE: c->profile = value != 0; return PSSGPU_OK;
+    case PSSGPU_OPT_INDIRECT_HANDLES: c->indirect_handles = value != 0; return PSSGPU_OK;
+    default: return fail(PSSGPU_EINVAL, "unknown option");
+    }
+}
+
 int pssgpu_ctx_kernel_stats(pssgpu_ctx* ctx, pssgpu_kernel_stats* out, int max)
 {
     if (!ctx || (!out && max > 0)) return -fail(PSSGPU_EINVAL, "null argument");
@@ -667,17 +694,18 @@ void pssgpu_sort_strings_lcp_cache(uint8_t** strings, uintptr_t* lcp, uint8_t* c
 // Allocation-free entry point.
 //
 // pssgpu_sort_device_noalloc sorts at most PSSGPU_NOALLOC_MAX_STRINGS strings
-// with the small-segment kernel and allocates nothing. Its scratch -- the id
-// buffer, the one segment descriptor and the counters that kernel uses -- is
-// the file-scope array below (8,336 bytes), which every device that loads this
-// library holds until the process exits. In host code the array's name is
-// only a host-side stand-in: kernels get the device address that
-// cudaGetSymbolAddress returns, looked up once per device with that device
-// current. Device code may name the array directly (k_noalloc_prep does).
+// with the small-segment kernel and allocates nothing. Its scratch -- the
+// string-handle buffer, the one segment descriptor and the counters that
+// kernel uses -- is the file-scope array below (16,528 bytes), which every
+// device that loads this library holds until the process exits. In host code
+// the array's name is only a host-side stand-in: kernels get the device
+// address that cudaGetSymbolAddress returns, looked up once per device with
+// that device current. Device code may name the array directly
+// (k_noalloc_prep does).
 namespace pssgpu {
 
 struct NoAllocScratch {
-    uint32_t ids[PSSGPU_NOALLOC_MAX_STRINGS];
+    uint64_t hnd[PSSGPU_NOALLOC_MAX_STRINGS];
     Seg seg;
     uint32_t counters[C_COUNT];
 };
@@ -685,17 +713,17 @@ struct NoAllocScratch {
 static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocScratch)];
 
 // One block: clear the counters (the array keeps the previous call's
-// contents), write the identity ids and the single segment, check offsets.
-__global__ void k_noalloc_prep(const uint64_t* __restrict__ offs, uint64_t nchars, uint32_t n)
+// contents), write the initial handles and the single segment, check offsets.
+__global__ void k_noalloc_prep(Work w)
 {
     NoAllocScratch* s = reinterpret_cast<NoAllocScratch*>(g_noalloc_scratch);
     for (int i = threadIdx.x; i < C_COUNT; i += blockDim.x) s->counters[i] = 0;
     __syncthreads();
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-        s->ids[i] = i;
-        if (offs[i] >= nchars) atomicOr(&s->counters[C_ERR], ERR_OFFSET);
+    for (uint32_t i = threadIdx.x; i < w.n; i += blockDim.x) {
+        s->hnd[i] = h_make(w, i, w.offs[i]);
+        if (w.offs[i] >= w.nchars) atomicOr(&s->counters[C_ERR], ERR_OFFSET);
     }
-    if (threadIdx.x == 0) s->seg = Seg{0u, n, 0u, 0u};
+    if (threadIdx.x == 0) s->seg = Seg{0u, w.n, 0u, 0u};
 }
 
 constexpr int NOALLOC_MAX_DEVICES = 64;
@@ -746,12 +774,13 @@ extern "C" int pssgpu_sort_device_noalloc(const uint8_t* d_chars, uint64_t nchar
     w.nchars = nchars;
     w.offs = d_offs;
     w.n = (uint32_t)n;
-    w.ids[0] = w.ids[1] = scratch->ids;
+    w.hnd[0] = w.hnd[1] = scratch->hnd;
     w.perm = d_perm;
     w.lcp = d_lcp;
     w.counters = scratch->counters;
     w.cur = 0;
-    k_noalloc_prep<<<1, SMALL_THREADS, 0, st>>>(d_offs, nchars, (uint32_t)n);
+    set_handle_format(w, false);
+    k_noalloc_prep<<<1, SMALL_THREADS, 0, st>>>(w);
     K_SMALL_B<<<1, SMALL_THREADS, sizeof(SmallSmem<SMALL_MAX>), st>>>(w, &scratch->seg);
     uint32_t err = 0;
     if (cudaGetLastError() != cudaSuccess ||

@@ -45,8 +45,14 @@ struct Work {
     uint64_t nchars;
     const uint64_t* offs;
     uint32_t n;
-    // permutation / key ping-pong
-    uint32_t* ids[2];
+    // String handles: (id << hbits) | arena offset when both fit in 64 bits
+    // (packed), else the id alone and the offset is read from offs[id].
+    // Carrying the offset saves the dependent offs[id] load of every gather.
+    uint32_t hbits;
+    uint64_t hmask;
+    int packed;
+    // handle / key ping-pong
+    uint64_t* hnd[2];
     uint64_t* keys[2];
     uint16_t* bkt;
     // outputs
@@ -74,5 +80,26 @@ struct Work {
     uint32_t epoch;        // look-back epoch of this pass (1..65535)
     int cur;               // parity of the lists read in this pass
 };
+
+__device__ __forceinline__ uint64_t h_make(const Work& w, uint32_t id, uint64_t off)
+{
+    return w.packed ? (((uint64_t)id << w.hbits) | off) : (uint64_t)id;
+}
+
+__device__ __forceinline__ uint32_t h_id(const Work& w, uint64_t h)
+{
+    return w.packed ? (uint32_t)(h >> w.hbits) : (uint32_t)h;
+}
+
+__device__ __forceinline__ uint64_t h_off(const Work& w, uint64_t h)
+{
+    return w.packed ? (h & w.hmask) : __ldg(w.offs + h);
+}
+
+// key of the string behind handle h at depth d
+__device__ __forceinline__ uint64_t h_key(const Work& w, uint64_t h, uint32_t d)
+{
+    return load_key(w.chars, w.nchars, h_off(w, h) + d);
+}
 
 }  // namespace pssgpu

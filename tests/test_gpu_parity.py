@@ -105,6 +105,20 @@ def test_deep_repeats_suffixes(pkg, orc, ctx):
     check_against_oracle(orc, chars, offs, perm, lcp)
 
 
+@pytest.mark.parametrize("n,alpha,lmax,seed", [(3000, b"ab", 40, 31), (200000, b"abc", 30, 32)])
+def test_indirect_handles(pkg, orc, n, alpha, lmax, seed):
+    """The path for inputs whose string id and arena offset do not fit one
+    64-bit handle (offsets read through the offset array), forced on."""
+    c = pkg.Context(0)
+    try:
+        c.set_option(c.OPT_INDIRECT_HANDLES, 1)
+        chars, offs, _ = pkg.workloads.random_strings(n, 0, lmax, alpha, seed)
+        perm, lcp = c.sort_host(chars, offs, lcp=True)
+        check_against_oracle(orc, chars, offs, perm, lcp)
+    finally:
+        c.close()
+
+
 def test_lcp_optional(pkg, ctx):
     chars, offs, _ = pkg.workloads.random_strings(20000, 0, 10, b"abc", 11)
     p1, _ = ctx.sort_host(chars, offs, lcp=False)

@@ -435,6 +435,7 @@ __device__ __forceinline__ void push_seg(Work& w, int nxt, Seg c)
     }
     w.list[cls][nxt][at] = c;
     if (cls == L_BIG) atomicAdd(w.counters + C_PAR * nxt + C_NTILES, (c.size + TILE - 1) / TILE);
+    else atomicAdd(w.counters + C_PAR * nxt + C_NSTR + cls, c.size);
 }
 
 // Children of each bucket, after the scatter has placed them; the next
@@ -461,9 +462,9 @@ __global__ void __launch_bounds__(1024) k_children(Work w)
     if (!classified(L)) return;
     // block-aggregated appends: slots in shared memory first, then one
     // global reservation per list
-    __shared__ uint32_t lcnt[L_NCLASS], gbase[L_NCLASS];
+    __shared__ uint32_t lcnt[L_NCLASS], gbase[L_NCLASS], lstr[L_NCLASS];
     __shared__ uint32_t ltiles, lbnd, bbase;
-    if (threadIdx.x < L_NCLASS) lcnt[threadIdx.x] = 0;
+    if (threadIdx.x < L_NCLASS) { lcnt[threadIdx.x] = 0; lstr[threadIdx.x] = 0; }
     if (threadIdx.x == 0) { ltiles = 0; lbnd = 0; }
     __syncthreads();
     const uint32_t B = (2u << L) - 1;
@@ -514,11 +515,14 @@ __global__ void __launch_bounds__(1024) k_children(Work w)
         else cls[j] = L_TINY;
         slot[j] = atomicAdd(&lcnt[cls[j]], 1u);
         if (cls[j] == L_BIG) atomicAdd(&ltiles, (c + TILE - 1) / TILE);
+        else atomicAdd(&lstr[cls[j]], c);
     }
     __syncthreads();
     if (threadIdx.x < L_NCLASS && lcnt[threadIdx.x])
         gbase[threadIdx.x] = atomicAdd(w.counters + C_PAR * nxt + threadIdx.x, lcnt[threadIdx.x]);
     if (threadIdx.x == 32 && ltiles) atomicAdd(w.counters + C_PAR * nxt + C_NTILES, ltiles);
+    if (threadIdx.x >= 33 && threadIdx.x < 32 + L_NCLASS && lstr[threadIdx.x - 32])
+        atomicAdd(w.counters + C_PAR * nxt + C_NSTR + (threadIdx.x - 32), lstr[threadIdx.x - 32]);
     if (threadIdx.x == 64 && lbnd) bbase = atomicAdd(w.counters + C_NBND, lbnd);
     __syncthreads();
 #pragma unroll

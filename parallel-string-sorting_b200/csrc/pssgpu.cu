@@ -4,8 +4,8 @@
 // Enqueue (src/parallel/bingmann-parallel_sample_sort.hpp:1613-1634) with
 // level-synchronous passes: every pass runs one sample-sort step over all
 // segments larger than SMALL_MAX strings (kernels_big.cuh) and finishes all
-// smaller segments in shared memory (kernels_small.cuh). One 24-byte
-// device-to-host read per pass sizes the next pass's grids.
+// smaller segments in shared memory (kernels_block.cuh, kernels_small.cuh).
+// One device-to-host read of the counters per pass sizes the next grids.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -18,7 +18,7 @@
 
 #include "../../include/pssgpu.h"
 #include "kernels_big.cuh"
-#include "kernels_small.cuh"
+#include "kernels_block.cuh"
 
 namespace pssgpu {
 
@@ -102,10 +102,11 @@ static uint64_t workspace_bytes(const Sizes& s)
 }
 
 // Kernel classes reported by pssgpu_ctx_kernel_stats.
-enum KClass { K_INIT = 0, K_SAMPLE, K_CLASSIFY, K_BSTART, K_SCATTER, K_CHILDREN, K_SMALL,
-              K_BOUNDARY, K_NCLASS };
+enum KClass { K_INIT = 0, K_SAMPLE, K_CLASSIFY, K_BSTART, K_SCATTER, K_CHILDREN, K_TINY,
+              K_SMALLA, K_SMALLB, K_BOUNDARY, K_NCLASS };
 static const char* const kclass_name[K_NCLASS] = {
-    "init", "sample", "classify", "bstart", "scatter", "children", "small", "boundary"};
+    "init", "sample", "classify", "bstart", "scatter", "children", "tiny",
+    "small256", "small2048", "boundary"};
 
 struct KStat {
     uint32_t launches = 0;
@@ -221,10 +222,10 @@ static int setup_kernels()
     if (dev < 0 || dev >= MAXDEV) return fail(PSSGPU_ENODEV, "device index out of range");
     std::lock_guard<std::mutex> lk(mu);
     if (done[dev]) return PSSGPU_OK;
-    PSS_CUDA(cudaFuncSetAttribute(K_SMALL_A, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)sizeof(SmallSmem<SMALL_A>)));
-    PSS_CUDA(cudaFuncSetAttribute(K_SMALL_B, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)sizeof(SmallSmem<SMALL_MAX>)));
+    PSS_CUDA(cudaFuncSetAttribute(K_BLOCK_A, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sizeof(BlockSmem<SMALL_A>)));
+    PSS_CUDA(cudaFuncSetAttribute(K_BLOCK_B, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sizeof(BlockSmem<SMALL_MAX>)));
     PSS_CUDA(cudaFuncSetAttribute(k_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)sizeof(ScatterSmem)));
     done[dev] = true;
@@ -272,9 +273,13 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
     PSS_CUDA(cudaMemcpyAsync(hc, w.counters, 4 * C_COUNT, cudaMemcpyDeviceToHost, st));
     PSS_CUDA(cudaStreamSynchronize(st));
     kt.collect();
-    uint32_t cnt[L_NCLASS];
-    for (int k = 0; k < L_NCLASS; ++k) cnt[k] = hc[k];
+    uint32_t cnt[L_NCLASS], nstr[L_NCLASS];
+    for (int k = 0; k < L_NCLASS; ++k) {
+        cnt[k] = hc[k];
+        nstr[k] = k == L_BIG ? 0u : hc[C_NSTR + k];
+    }
     uint32_t ntiles = hc[C_NTILES];
+    uint64_t small_segments = 0;
     uint32_t err = hc[C_ERR];
     int cur = 0;
     auto pending = [&]() { return cnt[L_BIG] || cnt[L_TINY] || cnt[L_SMALLA] || cnt[L_SMALLB]; };
@@ -292,27 +297,30 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
         PSS_CUDA(cudaMemsetAsync(w.counters + C_PAR * nxt, 0, 4 * C_PAR, st));
         PSS_CUDA(cudaMemsetAsync(w.counters + C_TICKET, 0, 4, st));
         PSS_CUDA(cudaMemsetAsync(w.counters + C_P_FIRST, 0, 4 * (C_P_LAST - C_P_FIRST + 1), st));
-        if (cnt[L_TINY] || cnt[L_SMALLA] || cnt[L_SMALLB]) {
-            kt.begin(K_SMALL);
-            if (cnt[L_TINY]) {
-                k_tiny<<<(cnt[L_TINY] + TINY_WARPS - 1) / TINY_WARPS, 32 * TINY_WARPS, 0, st>>>(
-                    w, w.list[L_TINY][cur], cnt[L_TINY]);
-                c->kstat[K_SMALL].launches += 1;
-                stats.kernel_launches += 1;
-            }
-            if (cnt[L_SMALLA]) {
-                K_SMALL_A<<<cnt[L_SMALLA], SMALL_A_THREADS, sizeof(SmallSmem<SMALL_A>), st>>>(
-                    w, w.list[L_SMALLA][cur]);
-                c->kstat[K_SMALL].launches += 1;
-                stats.kernel_launches += 1;
-            }
-            if (cnt[L_SMALLB]) {
-                K_SMALL_B<<<cnt[L_SMALLB], SMALL_THREADS, sizeof(SmallSmem<SMALL_MAX>), st>>>(
-                    w, w.list[L_SMALLB][cur]);
-                c->kstat[K_SMALL].launches += 1;
-                stats.kernel_launches += 1;
-            }
-            kt.end(K_SMALL);
+        if (cnt[L_TINY]) {
+            kt.begin(K_TINY);
+            constexpr uint32_t per_block = TINY_WARPS * TINY_PER_WARP;
+            k_tiny<<<(cnt[L_TINY] + per_block - 1) / per_block, 32 * TINY_WARPS, 0, st>>>(
+                w, w.list[L_TINY][cur], cnt[L_TINY]);
+            kt.end(K_TINY);
+            c->kstat[K_TINY].launches += 1;
+            stats.kernel_launches += 1;
+        }
+        if (cnt[L_SMALLA]) {
+            kt.begin(K_SMALLA);
+            K_BLOCK_A<<<cnt[L_SMALLA], SMALL_A_THREADS, sizeof(BlockSmem<SMALL_A>), st>>>(
+                w, w.list[L_SMALLA][cur]);
+            kt.end(K_SMALLA);
+            c->kstat[K_SMALLA].launches += 1;
+            stats.kernel_launches += 1;
+        }
+        if (cnt[L_SMALLB]) {
+            kt.begin(K_SMALLB);
+            K_BLOCK_B<<<cnt[L_SMALLB], SMALL_THREADS, sizeof(BlockSmem<SMALL_MAX>), st>>>(
+                w, w.list[L_SMALLB][cur]);
+            kt.end(K_SMALLB);
+            c->kstat[K_SMALLB].launches += 1;
+            stats.kernel_launches += 1;
         }
         if (nbig) {
             if (ntiles > c->cap.tile_cap) return fail(PSSGPU_ECUDA, "tile capacity exceeded");
@@ -350,7 +358,7 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
             // 12 read + 12 write; base case 12 read + output
             // (a jump string is charged like a gather: 4 id + 8 offset + 8 chars)
             const uint64_t big = hc[C_P_BIG], stale = hc[C_P_STALE], fin = hc[C_P_FINAL];
-            const uint64_t sc = hc[C_P_SCATTER], sm = hc[C_P_SMALL], tie = hc[C_P_TIE];
+            const uint64_t sc = hc[C_P_SCATTER], tie = hc[C_P_TIE];
             stats.big_elements += big + tie;
             c->kstat[K_SAMPLE].strings += big + tie;
             c->kstat[K_CLASSIFY].strings += big + fin + tie;
@@ -358,11 +366,19 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
                 20 * stale + 8 * (big - stale) + (4 + out_bytes) * fin + 20 * tie;
             c->kstat[K_SCATTER].strings += sc;
             c->kstat[K_SCATTER].alg_bytes += 24 * sc;
-            c->kstat[K_SMALL].strings += sm;
-            c->kstat[K_SMALL].alg_bytes += (12 + out_bytes) * sm;
+            const int sk[3] = {K_TINY, K_SMALLA, K_SMALLB};
+            const int lk[3] = {L_TINY, L_SMALLA, L_SMALLB};
+            for (int q = 0; q < 3; ++q) {
+                c->kstat[sk[q]].strings += nstr[lk[q]];
+                c->kstat[sk[q]].alg_bytes += (12 + out_bytes) * nstr[lk[q]];
+                small_segments += cnt[lk[q]];
+            }
             c->kstat[K_CHILDREN].strings += big;
         }
-        for (int k = 0; k < L_NCLASS; ++k) cnt[k] = hc[C_PAR * nxt + k];
+        for (int k = 0; k < L_NCLASS; ++k) {
+            cnt[k] = hc[C_PAR * nxt + k];
+            nstr[k] = k == L_BIG ? 0u : hc[C_PAR * nxt + C_NSTR + k];
+        }
         ntiles = hc[C_PAR * nxt + C_NTILES];
         err = hc[C_ERR];
         cur = nxt;
@@ -385,7 +401,7 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
     }
     PSS_CUDA(cudaGetLastError());
     err = hc[C_ERR];
-    stats.small_segments = hc[C_SMALLSEGS];
+    stats.small_segments = small_segments;
     stats.boundaries = hc[C_NBND];
     cudaEventElapsedTime(&stats.device_ms, c->ev0, c->ev1);
     c->stats = stats;
@@ -755,8 +771,8 @@ extern "C" int pssgpu_sort_device_noalloc(const uint8_t* d_chars, uint64_t nchar
             void* p = nullptr;
             if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p)
                 return fail(PSSGPU_ECUDA, "symbol lookup");
-            if (cudaFuncSetAttribute(K_SMALL_B, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)sizeof(SmallSmem<SMALL_MAX>)) != cudaSuccess)
+            if (cudaFuncSetAttribute(K_BLOCK_B, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sizeof(BlockSmem<SMALL_MAX>)) != cudaSuccess)
                 return fail(PSSGPU_ECUDA, "smem limit");
             g_noalloc_addr[dev] = static_cast<NoAllocScratch*>(p);
         }
@@ -781,7 +797,7 @@ extern "C" int pssgpu_sort_device_noalloc(const uint8_t* d_chars, uint64_t nchar
     w.cur = 0;
     set_handle_format(w, false);
     k_noalloc_prep<<<1, SMALL_THREADS, 0, st>>>(w);
-    K_SMALL_B<<<1, SMALL_THREADS, sizeof(SmallSmem<SMALL_MAX>), st>>>(w, &scratch->seg);
+    K_BLOCK_B<<<1, SMALL_THREADS, sizeof(BlockSmem<SMALL_MAX>), st>>>(w, &scratch->seg);
     uint32_t err = 0;
     if (cudaGetLastError() != cudaSuccess ||
         cudaMemcpyAsync(&err, scratch->counters + C_ERR, 4, cudaMemcpyDeviceToHost, st) !=

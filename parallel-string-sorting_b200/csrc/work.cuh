@@ -23,6 +23,7 @@ enum : int { L_BIG = 0, L_TINY = 1, L_SMALLA = 2, L_SMALLB = 3, L_NCLASS = 4 };
 enum : int {
     C_PAR = 8,        // counters per parity block: [class] lengths, then tiles
     C_NTILES = 4,     // + C_PAR * parity: tiles of the big list
+    C_NSTR = 4,       // + C_PAR * parity + class (1..3): strings in the small lists
     C_NBND = 16,      // boundary list length
     C_TICKET = 17,    // scatter tile ticket
     C_ERR = 18,       // error bits
@@ -32,8 +33,7 @@ enum : int {
     C_P_STALE = 21,   // of those, strings whose key was gathered this pass
     C_P_FINAL = 22,   // strings copied out of big all-equal segments
     C_P_SCATTER = 23, // strings moved by the scatter
-    C_P_SMALL = 24,   // strings finished by the small sorters
-    C_P_TIE = 25,     // strings of segments that took the common-prefix jump
+    C_P_TIE = 24,     // strings of segments that took the common-prefix jump
     C_P_FIRST = C_P_BIG,
     C_P_LAST = C_P_TIE,
     C_COUNT = 32

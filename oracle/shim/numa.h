@@ -9,3 +9,9 @@ static inline int numa_num_configured_nodes(void) { return 1; }
 static inline void numa_tonode_memory(void* p, size_t s, int node) { (void)p; (void)s; (void)node; }
 static inline void* numa_alloc_onnode(size_t s, int node) { (void)node; return malloc(s); }
 static inline void numa_free(void* p, size_t s) { (void)s; free(p); }
+struct bitmask { unsigned long size; unsigned long* maskp; };
+static struct bitmask* const numa_all_nodes_ptr = 0;
+static struct bitmask* const numa_all_cpus_ptr = 0;
+static inline void numa_set_interleave_mask(struct bitmask* m) { (void)m; }
+static inline void numa_interleave_memory(void* p, size_t s, struct bitmask* m) { (void)p; (void)s; (void)m; }
+static inline void numa_set_strict(int flag) { (void)flag; }

@@ -55,6 +55,11 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--cpu-sample", type=int, default=CPU_SAMPLE)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--mode", choices=["sort", "batched", "autotune"], default="sort",
+                   help="sort: the headline line; batched: the 100k-instance batch "
+                        "against one call per instance; autotune: write the tuning table")
+    p.add_argument("--sample-instances", type=int, default=1000,
+                   help="batched mode: instances timed one call each")
     return p.parse_args()
 
 
@@ -194,10 +199,115 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def run_autotune():
+    import __graft_entry__
+    pkg = __graft_entry__.load_package()
+    from importlib import import_module
+    at = import_module("pss_b200.autotune")
+    res = at.tune()
+    at.save_table(res)
+    print(json.dumps({"mode": "autotune", "table": res["table"]}))
+
+
+def run_batched(args):
+    """The batched workload (100k instances, <= 1 GiB of chars) sorted by one
+    batched call, against one pssgpu_sort_device call per instance timed on a
+    random sample of instances and scaled to all instances."""
+    import torch
+    import __graft_entry__
+    from importlib import import_module
+    pkg = __graft_entry__.load_package()
+    at = import_module("pss_b200.autotune")
+    canonical_ids = pkg.workloads.canonical_ids
+    alloc = pinned_alloc(torch)
+    t0 = time.perf_counter()
+    h_chars, h_offs, nchars, inst = pkg.workloads.batched(alloc=alloc)
+    gen_s = time.perf_counter() - t0
+    n = len(h_offs)
+    ninst = len(inst) - 1
+    ctx = pkg.Context(0)
+    table = at.load_table()
+    stream = torch.cuda.current_stream()
+    dc = torch.from_numpy(h_chars).cuda()
+    do = torch.from_numpy(h_offs.view(np.int64)).cuda()
+    dp = torch.empty(n, dtype=torch.int32, device="cuda")
+    dl = torch.empty(n, dtype=torch.int32, device="cuda")
+
+    def timed(fn, reps):
+        ms = []
+        for _ in range(reps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return ms
+
+    def batch():
+        ctx.sort_batch_device(dc, nchars, do, inst, dp, dl, stream=stream)
+
+    res = {}
+    for name, tb in (("default", None), ("tuned", table)):
+        if name == "tuned" and tb is None:
+            continue
+        ctx.set_tree_bits(tb if tb is not None else [0] * 33)
+        for _ in range(max(args.warmup, 3)):
+            batch()
+        ms = timed(batch, args.steps)
+        res[name] = {"ms": statistics.median(ms), "ms_all": ms,
+                     "launches": ctx.stats()["kernel_launches"]}
+    best = min(res.values(), key=lambda r: r["ms"])
+    batch()  # output of the best configuration for the comparison
+    perm_b = dp.cpu().numpy().view(np.uint32)
+    lcp_b = dl.cpu().numpy().view(np.uint32)
+
+    # one call per instance on a random sample of instances
+    lens_all = pkg.workloads.string_lengths(h_chars[: nchars + 1], h_offs)
+    rng = np.random.default_rng(0)
+    sample = rng.choice(ninst, min(args.sample_instances, ninst), replace=False)
+    p1 = torch.empty(int((inst[1:] - inst[:-1]).max()), dtype=torch.int32, device="cuda")
+    l1 = torch.empty_like(p1)
+    single_ms = 0.0
+    identical = True
+    for k in sample:
+        b, e = int(inst[k]), int(inst[k + 1])
+        ms = timed(lambda: ctx.sort_device(dc, nchars, do[b:e], p1, l1, stream=stream), 1)[0]
+        single_ms += ms
+        pp = p1[: e - b].cpu().numpy().view(np.uint32)
+        ll = l1[: e - b].cpu().numpy().view(np.uint32)
+        offs_k = h_offs[b:e]
+        lens_k = lens_all[b:e]
+        if not (np.array_equal(ll[1:], lcp_b[b + 1:e]) and np.array_equal(
+                canonical_ids(h_chars, offs_k, pp, ll, lens_k),
+                canonical_ids(h_chars, offs_k, perm_b[b:e], lcp_b[b:e], lens_k))):
+            identical = False
+    per_instance_ms = single_ms * ninst / len(sample)
+    line = {"mode": "batched", "metric": "batched sort time", "unit": "ms",
+            "config": {"workload": "batched-100k", "instances": ninst, "strings": n,
+                       "chars": nchars, "sizes": "log-uniform 16..1Mi, scaled to <= 1 GiB",
+                       "lengths": "lognormal(3, 0.5) clipped 1..256", "alphabet": "32..126"},
+            "batched_ms": best["ms"], "batched": res,
+            "char_gb_s": nchars / (best["ms"] / 1e3) / 1e9,
+            "per_instance_ms_est": per_instance_ms,
+            "per_instance_sample": len(sample),
+            "speedup_vs_per_instance": per_instance_ms / best["ms"],
+            "identical_output_on_sample": identical, "generate_s": gen_s}
+    print(json.dumps(line))
+    ctx.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.mode == "autotune":
+        run_autotune()
+        return
+    if args.mode == "batched":
+        run_batched(args)
         return
     import torch
     import torch.distributed as dist

@@ -117,6 +117,28 @@ int pssgpu_sort_device(pssgpu_ctx* ctx, const uint8_t* d_chars,
                        uint64_t nchars, const uint64_t* d_offs, uint64_t n,
                        uint32_t* d_perm, uint32_t* d_lcp, void* stream);
 
+/* ---- batched sorts ---------------------------------------------------------
+ * Many independent sort instances in one call: every instance becomes a
+ * root segment of the same device passes, so instances of any size share
+ * the kernel launches. Instance k owns strings [inst[k], inst[k+1]) of the
+ * offset array (inst is a host array of ninst + 1 entries, inst[0] = 0,
+ * non-decreasing, inst[ninst] = n). On return perm[p] for p in
+ * [inst[k], inst[k+1]) is a string id of instance k counted from 0, i.e. the
+ * instance's own permutation; lcp (may be NULL) holds each instance's LCP
+ * array with its first entry written as 0. No counterpart in the reference,
+ * which sorts one string set per call. */
+int pssgpu_sort_batch_host(pssgpu_ctx* ctx, const uint8_t* chars, uint64_t nchars,
+                           const uint64_t* offs, const uint64_t* inst, uint32_t ninst,
+                           uint32_t* perm, uint32_t* lcp);
+int pssgpu_sort_batch_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nchars,
+                             const uint64_t* d_offs, const uint64_t* inst, uint32_t ninst,
+                             uint32_t* d_perm, uint32_t* d_lcp, void* stream);
+
+/* Tuning table: splitter-tree levels (1..10) for big segments of
+ * 2^k .. 2^(k+1)-1 strings, k < count <= 33; 0 keeps the default rule
+ * (about 16 strings per bucket). Written by the autotuner. */
+int pssgpu_ctx_set_tree_bits(pssgpu_ctx* ctx, const uint8_t* tree_bits, int count);
+
 /* ---- psstest Contest drop-ins --------------------------------------------
  * The three contestant signatures of Contestant_UCArray
  * (src/tools/contest.hpp:88-91). Each permutes `strings` in place into

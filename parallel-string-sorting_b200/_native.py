@@ -31,6 +31,12 @@ GPU_SIGNATURES = {
                                    C.c_void_p, C.c_void_p]),
     "pssgpu_sort_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64,
                                      C.c_void_p, C.c_void_p, C.c_void_p]),
+    "pssgpu_sort_batch_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p,
+                                         C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
+    "pssgpu_sort_batch_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p,
+                                           C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
+                                           C.c_void_p]),
+    "pssgpu_ctx_set_tree_bits": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     "pssgpu_sort_strings": (None, [C.c_void_p, C.c_size_t]),
     "pssgpu_sort_strings_lcp": (None, [C.c_void_p, C.c_void_p, C.c_size_t]),
     "pssgpu_sort_strings_lcp_cache": (None, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t]),
@@ -49,6 +55,8 @@ WORK_SIGNATURES = {
     "pssw_prefix_fill": (None, [C.c_uint64, C.c_uint64, C.c_void_p, C.c_double, C.c_void_p,
                                 C.c_void_p]),
     "pssw_dna_text": (C.c_uint64, [C.c_uint64, C.c_uint64, C.c_double, C.c_void_p]),
+    "pssw_lognormal_offsets": (C.c_uint64, [C.c_uint64, C.c_uint64, C.c_double, C.c_double,
+                                            C.c_uint32, C.c_uint32, C.c_void_p]),
     "pssw_alg_bytes": (None, [C.c_void_p, C.c_uint64, C.c_uint32, C.POINTER(C.c_uint64),
                               C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                               C.POINTER(C.c_uint32)]),

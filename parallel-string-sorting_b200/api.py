@@ -109,6 +109,35 @@ class Context:
                                               _ptr(perm), _ptr(lcp_a)))
         return perm, lcp_a
 
+    def set_tree_bits(self, table) -> None:
+        """Splitter-tree levels per size class (index k: segments of 2^k..2^(k+1)-1
+        strings; 0 = default rule)."""
+        t = np.ascontiguousarray(np.asarray(table, dtype=np.uint8))
+        _check(_native.gpu().pssgpu_ctx_set_tree_bits(self._h, t.ctypes.data, t.shape[0]))
+
+    def sort_batch_host(self, chars: np.ndarray, offs: np.ndarray, inst: np.ndarray,
+                        lcp: bool = True, out_perm=None, out_lcp=None):
+        """Sort independent instances (inst: ninst+1 boundaries into offs);
+        returns per-instance permutations and LCP arrays, concatenated."""
+        chars = np.ascontiguousarray(chars, dtype=np.uint8)
+        offs = np.ascontiguousarray(offs, dtype=np.uint64)
+        inst = np.ascontiguousarray(inst, dtype=np.uint64)
+        n = offs.shape[0]
+        perm = np.empty(n, dtype=np.uint32) if out_perm is None else out_perm
+        lcp_a = (np.zeros(n, dtype=np.uint32) if out_lcp is None else out_lcp) if lcp else None
+        _check(_native.gpu().pssgpu_sort_batch_host(self._h, _ptr(chars), chars.shape[0],
+                                                    _ptr(offs), inst.ctypes.data,
+                                                    inst.shape[0] - 1, _ptr(perm), _ptr(lcp_a)))
+        return perm, lcp_a
+
+    def sort_batch_device(self, chars, nchars: int, offs, inst: np.ndarray, perm, lcp=None,
+                          stream=None) -> None:
+        inst = np.ascontiguousarray(inst, dtype=np.uint64)
+        s = None if stream is None else (stream if isinstance(stream, int) else stream.cuda_stream)
+        _check(_native.gpu().pssgpu_sort_batch_device(
+            self._h, chars.data_ptr(), nchars, offs.data_ptr(), inst.ctypes.data,
+            inst.shape[0] - 1, perm.data_ptr(), None if lcp is None else lcp.data_ptr(), s))
+
     def sort_device(self, chars, nchars: int, offs, perm, lcp=None, stream=None) -> None:
         """Sort an arena resident on this context's device (torch tensors or
         raw device pointers). ``chars`` must hold nchars + 16 bytes."""

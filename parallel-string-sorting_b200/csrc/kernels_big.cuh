@@ -36,10 +36,13 @@ __device__ __forceinline__ int find_tile_seg(const uint32_t* tile_start, int nbi
     return lo;
 }
 
-__device__ __forceinline__ uint32_t tree_bits_for(uint32_t m)
+__device__ __forceinline__ uint32_t tree_bits_for(const Work& w, uint32_t m)
 {
-    // about 16 strings per '<' bucket, at most pS5's 10 tree levels
+    // a tuned value for this size class, else about 16 strings per '<'
+    // bucket; at most pS5's 10 tree levels
     const int lg = 31 - __clz((int)m);
+    const uint32_t tuned = w.tree_bits_by_size[lg];
+    if (tuned) return min((uint32_t)MAX_TREE_BITS, tuned);
     return (uint32_t)min(MAX_TREE_BITS, max(1, lg - 4));
 }
 
@@ -75,7 +78,7 @@ __global__ void __launch_bounds__(1024) k_sample(Work w)
         }
         return;
     }
-    const uint32_t L = tree_bits_for(sg.size);
+    const uint32_t L = tree_bits_for(w, sg.size);
     const uint32_t k = (1u << L) - 1;
     const uint32_t S = 2u << L;  // oversampling factor 2 (hpp:1388)
     const int buf = sg.meta & META_BUF;

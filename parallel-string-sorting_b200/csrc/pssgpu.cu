@@ -46,9 +46,33 @@ __global__ void k_init(Work w)
     }
 }
 
-__global__ void k_root(Work w)
+// Root segments: the whole input, or one per instance of a batch (instance k
+// owns positions [inst[k], inst[k+1])). A one-string instance is final at
+// once; the batch's ids are global until k_localize.
+__global__ void k_roots(Work w, const uint64_t* __restrict__ inst, uint32_t ninst)
 {
-    push_seg(w, 0, Seg{0u, w.n, 0u, 0u});
+    if (!inst) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) push_seg(w, 0, Seg{0u, w.n, 0u, 0u});
+        return;
+    }
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < ninst; k += gridDim.x * blockDim.x) {
+        const uint32_t b = (uint32_t)inst[k], e = (uint32_t)inst[k + 1];
+        if (e - b >= 2) push_seg(w, 0, Seg{b, e - b, 0u, 0u});
+        else if (e - b == 1) w.perm[b] = b;
+    }
+}
+
+// Batch output: ids relative to their instance.
+// Batch output: ids relative to their instance; the first LCP of every
+// instance is 0.
+__global__ void k_localize(uint32_t* __restrict__ perm, uint32_t* __restrict__ lcp,
+                           const uint64_t* __restrict__ inst, uint32_t ninst)
+{
+    for (uint32_t k = blockIdx.x; k < ninst; k += gridDim.x) {
+        const uint32_t b = (uint32_t)inst[k], e = (uint32_t)inst[k + 1];
+        for (uint32_t p = b + threadIdx.x; p < e; p += blockDim.x) perm[p] -= b;
+        if (lcp && threadIdx.x == 0 && e > b) lcp[b] = 0;
+    }
 }
 
 static uint32_t bit_length(uint64_t x) { return x ? 64u - (uint32_t)__builtin_clzll(x) : 0u; }
@@ -136,6 +160,11 @@ struct Ctx {
     // carry bare ids and read offsets through offs[] (the path taken when
     // id and offset do not fit one 64-bit handle); settable for testing
     bool indirect_handles = false;
+    // splitter-tree levels per size class of big segments (0 = default)
+    uint8_t tree_bits_by_size[33] = {};
+    // device copy of a batch's instance boundaries
+    uint64_t* inst_buf = nullptr;
+    uint64_t inst_cap = 0;
     cudaEvent_t kev[2 * K_NCLASS] = {};
     KStat kstat[K_NCLASS];
 };
@@ -242,7 +271,8 @@ static int map_device_error(uint32_t err)
 
 // Sort n strings already resident on the device. Caller holds c->mu.
 static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_t* offs,
-                    uint32_t n, uint32_t* perm, uint32_t* lcp, cudaStream_t st)
+                    uint32_t n, uint32_t* perm, uint32_t* lcp, cudaStream_t st,
+                    const uint64_t* d_inst = nullptr, uint32_t ninst = 0)
 {
     int rc = ensure_workspace(c, n);
     if (rc) return rc;
@@ -255,6 +285,7 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
     w.perm = perm;
     w.lcp = lcp;
     set_handle_format(w, c->indirect_handles);
+    memcpy(w.tree_bits_by_size, c->tree_bits_by_size, sizeof(w.tree_bits_by_size));
     pssgpu_stats stats{};
     for (int k = 0; k < K_NCLASS; ++k) c->kstat[k] = KStat{};
     KTimer kt{c, st};
@@ -263,7 +294,7 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
     PSS_CUDA(cudaMemsetAsync(w.counters, 0, 4 * C_COUNT, st));
     kt.begin(K_INIT);
     k_init<<<1184, 256, 0, st>>>(w);
-    k_root<<<1, 1, 0, st>>>(w);
+    k_roots<<<d_inst ? 148 : 1, 256, 0, st>>>(w, d_inst, ninst);
     kt.end(K_INIT);
     c->kstat[K_INIT].launches += 2;
     c->kstat[K_INIT].strings += n;
@@ -390,6 +421,10 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
         c->kstat[K_BOUNDARY].launches += 1;
         stats.kernel_launches += 1;
     }
+    if (!err && d_inst) {
+        k_localize<<<1184, 256, 0, st>>>(perm, lcp, d_inst, ninst);
+        stats.kernel_launches += 1;
+    }
     PSS_CUDA(cudaEventRecord(c->ev1, st));
     PSS_CUDA(cudaMemcpyAsync(hc, w.counters, 4 * C_COUNT, cudaMemcpyDeviceToHost, st));
     PSS_CUDA(cudaStreamSynchronize(st));
@@ -439,6 +474,7 @@ static void ctx_destroy(Ctx* c)
     cudaSetDevice(c->device);
     if (c->ws) cudaFree(c->ws);
     if (c->io) cudaFree(c->io);
+    if (c->inst_buf) cudaFree(c->inst_buf);
     if (c->host_counters) cudaFreeHost(c->host_counters);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
@@ -493,6 +529,59 @@ static int sort_host_locked(Ctx* c, const uint8_t* chars, uint64_t nchars, const
     PSS_CUDA(cudaMemcpyAsync(perm, d_perm, 4 * n, cudaMemcpyDeviceToHost, st));
     if (lcp && n > 1)
         PSS_CUDA(cudaMemcpyAsync(lcp + 1, d_lcp + 1, 4 * (n - 1), cudaMemcpyDeviceToHost, st));
+    PSS_CUDA(cudaStreamSynchronize(st));
+    return PSSGPU_OK;
+}
+
+// Batch: check the instance boundaries and copy them to the device.
+static int stage_instances(Ctx* c, const uint64_t* inst, uint32_t ninst, uint64_t n,
+                           cudaStream_t st)
+{
+    if (!inst || ninst == 0) return fail(PSSGPU_EINVAL, "batch without instances");
+    if (inst[0] != 0 || inst[ninst] != n)
+        return fail(PSSGPU_EINVAL, "instance boundaries must start at 0 and end at n");
+    for (uint32_t k = 0; k < ninst; ++k)
+        if (inst[k + 1] < inst[k]) return fail(PSSGPU_EINVAL, "instance boundaries decrease");
+    const uint64_t need = (uint64_t)ninst + 1;
+    if (!c->inst_buf || c->inst_cap < need) {
+        if (c->inst_buf) cudaFree(c->inst_buf);
+        c->inst_buf = nullptr;
+        PSS_CUDA(cudaMalloc(&c->inst_buf, 8 * need));
+        c->inst_cap = need;
+    }
+    PSS_CUDA(cudaMemcpyAsync(c->inst_buf, inst, 8 * need, cudaMemcpyHostToDevice, st));
+    return PSSGPU_OK;
+}
+
+static int sort_batch_host_locked(Ctx* c, const uint8_t* chars, uint64_t nchars,
+                                  const uint64_t* offs, const uint64_t* inst, uint32_t ninst,
+                                  uint32_t* perm, uint32_t* lcp)
+{
+    const uint64_t n = inst ? inst[ninst] : 0;
+    int rc = check_args(nchars, n);
+    if (rc) return rc;
+    if (n == 0) return PSSGPU_OK;
+    if (chars[nchars - 1] != 0) return fail(PSSGPU_EINVAL, "arena does not end with NUL");
+    PSS_CUDA(cudaSetDevice(c->device));
+    cudaStream_t st = c->stream;
+    if ((rc = stage_instances(c, inst, ninst, n, st))) return rc;
+    const uint64_t b_chars = align256(nchars + PSSGPU_ARENA_PAD);
+    const uint64_t b_offs = align256(8 * n);
+    const uint64_t b_perm = align256(4 * n);
+    const uint64_t b_lcp = lcp ? align256(4 * n) : 0;
+    if ((rc = ensure_io(c, b_chars + b_offs + b_perm + b_lcp))) return rc;
+    uint8_t* d_chars = c->io;
+    uint64_t* d_offs = (uint64_t*)(c->io + b_chars);
+    uint32_t* d_perm = (uint32_t*)(c->io + b_chars + b_offs);
+    uint32_t* d_lcp = lcp ? (uint32_t*)(c->io + b_chars + b_offs + b_perm) : nullptr;
+    PSS_CUDA(cudaMemcpyAsync(d_chars, chars, nchars, cudaMemcpyHostToDevice, st));
+    PSS_CUDA(cudaMemsetAsync(d_chars + nchars, 0, b_chars - nchars, st));
+    PSS_CUDA(cudaMemcpyAsync(d_offs, offs, 8 * n, cudaMemcpyHostToDevice, st));
+    if ((rc = run_sort(c, d_chars, nchars, d_offs, (uint32_t)n, d_perm, d_lcp, st, c->inst_buf,
+                       ninst)))
+        return rc;
+    PSS_CUDA(cudaMemcpyAsync(perm, d_perm, 4 * n, cudaMemcpyDeviceToHost, st));
+    if (lcp) PSS_CUDA(cudaMemcpyAsync(lcp, d_lcp, 4 * n, cudaMemcpyDeviceToHost, st));
     PSS_CUDA(cudaStreamSynchronize(st));
     return PSSGPU_OK;
 }
@@ -673,6 +762,56 @@ int pssgpu_sort_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nchars,
     PSS_CUDA(cudaStreamSynchronize(st));
     if (last != 0) return fail(PSSGPU_EINVAL, "arena does not end with NUL");
     return run_sort(c, d_chars, nchars, d_offs, (uint32_t)n, d_perm, d_lcp, st);
+}
+
+int pssgpu_ctx_set_tree_bits(pssgpu_ctx* ctx, const uint8_t* tree_bits, int count)
+{
+    if (!ctx || (count > 0 && !tree_bits)) return fail(PSSGPU_EINVAL, "null argument");
+    if (count < 0 || count > 33) return fail(PSSGPU_EINVAL, "at most 33 size classes");
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    std::lock_guard<std::mutex> lk(c->mu);
+    memset(c->tree_bits_by_size, 0, sizeof(c->tree_bits_by_size));
+    for (int k = 0; k < count; ++k) {
+        if (tree_bits[k] > MAX_TREE_BITS) return fail(PSSGPU_EINVAL, "at most 10 tree levels");
+        c->tree_bits_by_size[k] = tree_bits[k];
+    }
+    return PSSGPU_OK;
+}
+
+int pssgpu_sort_batch_host(pssgpu_ctx* ctx, const uint8_t* chars, uint64_t nchars,
+                           const uint64_t* offs, const uint64_t* inst, uint32_t ninst,
+                           uint32_t* perm, uint32_t* lcp)
+{
+    if (!ctx) return fail(PSSGPU_EINVAL, "null context");
+    if (!inst) return fail(PSSGPU_EINVAL, "null instance boundaries");
+    if (inst[ninst] && (!chars || !offs || !perm)) return fail(PSSGPU_EINVAL, "null buffer");
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    std::lock_guard<std::mutex> lk(c->mu);
+    return sort_batch_host_locked(c, chars, nchars, offs, inst, ninst, perm, lcp);
+}
+
+int pssgpu_sort_batch_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nchars,
+                             const uint64_t* d_offs, const uint64_t* inst, uint32_t ninst,
+                             uint32_t* d_perm, uint32_t* d_lcp, void* stream)
+{
+    if (!ctx) return fail(PSSGPU_EINVAL, "null context");
+    if (!inst) return fail(PSSGPU_EINVAL, "null instance boundaries");
+    const uint64_t n = inst[ninst];
+    int rc = check_args(nchars, n);
+    if (rc) return rc;
+    if (n == 0) return PSSGPU_OK;
+    if (!d_chars || !d_offs || !d_perm) return fail(PSSGPU_EINVAL, "null buffer");
+    if (((uintptr_t)d_chars & 7) != 0) return fail(PSSGPU_EINVAL, "arena not 8-byte aligned");
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    std::lock_guard<std::mutex> lk(c->mu);
+    PSS_CUDA(cudaSetDevice(c->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    if ((rc = stage_instances(c, inst, ninst, n, st))) return rc;
+    uint8_t last = 1;
+    PSS_CUDA(cudaMemcpyAsync(&last, d_chars + nchars - 1, 1, cudaMemcpyDeviceToHost, st));
+    PSS_CUDA(cudaStreamSynchronize(st));
+    if (last != 0) return fail(PSSGPU_EINVAL, "arena does not end with NUL");
+    return run_sort(c, d_chars, nchars, d_offs, (uint32_t)n, d_perm, d_lcp, st, c->inst_buf, ninst);
 }
 
 int pssgpu_sort_strings_status(unsigned char** strings, uintptr_t* lcp, uint8_t* cache, size_t n)

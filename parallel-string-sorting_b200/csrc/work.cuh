@@ -79,6 +79,9 @@ struct Work {
     uint32_t tile_cap;
     uint32_t epoch;        // look-back epoch of this pass (1..65535)
     int cur;               // parity of the lists read in this pass
+    // splitter-tree levels for a big segment of 2^k..2^(k+1)-1 strings
+    // (0: the default rule), set from a tuning table
+    uint8_t tree_bits_by_size[33];
 };
 
 __device__ __forceinline__ uint64_t h_make(const Work& w, uint32_t id, uint64_t off)

@@ -154,6 +154,26 @@ uint64_t pssw_dna_text(uint64_t seed, uint64_t len, double copy_frac, uint8_t* t
     return copies;
 }
 
+// ---- strings of lognormal length: len = round(exp(mu + sigma * z)) clipped
+// to [lmin, lmax], z standard normal (Box-Muller on two counter-based
+// uniforms). Returns nchars (terminators included). ------------------------
+uint64_t pssw_lognormal_offsets(uint64_t seed, uint64_t n, double mu, double sigma,
+                                uint32_t lmin, uint32_t lmax, uint64_t* offs)
+{
+    uint64_t total = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+        const double u1 = unit(rnd(seed, 40, i)) + 1e-300;
+        const double u2 = unit(rnd(seed, 41, i));
+        const double z = std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2);
+        double len = std::floor(std::exp(mu + sigma * z) + 0.5);
+        if (len < lmin) len = lmin;
+        if (len > lmax) len = lmax;
+        offs[i] = total;
+        total += (uint64_t)len + 1;
+    }
+    return total;
+}
+
 // ---- algorithmic bytes of the sample-sort method for a sorted LCP array --
 // Groups at depth 8r are maximal runs of sorted strings whose interior LCPs
 // are >= 8r. Every string in a group larger than T at round r costs 52 bytes

@@ -89,6 +89,56 @@ def dna_suffixes(length: int = 32 * 1024 * 1024, seed: int = 3, copy_frac: float
     return chars, offs, length + 1
 
 
+PRINTABLE = bytes(range(32, 127))
+
+
+def batch_sizes(ninst: int = 100_000, smin: int = 16, smax: int = 1 << 20,
+                budget_chars: int = 1 << 30, mean_chars: float = 23.8, seed: int = 4):
+    """Instance sizes of the batched workload: log-uniform in [smin, smax],
+    then all scaled by one common factor f (with a floor of smin) so that the
+    expected total chars (sizes x mean_chars per string incl. terminator)
+    stay within budget_chars. Returns (sizes, f)."""
+    rng = np.random.default_rng(seed)
+    raw = np.exp(rng.uniform(np.log(smin), np.log(smax), ninst))
+
+    def total(f):
+        return np.maximum(smin, np.floor(raw * f)).sum() * mean_chars
+
+    f = 1.0
+    if total(1.0) > budget_chars:
+        lo, hi = 0.0, 1.0
+        for _ in range(60):
+            mid = (lo + hi) / 2
+            if total(mid) <= budget_chars:
+                lo = mid
+            else:
+                hi = mid
+        f = lo
+    sizes = np.maximum(smin, np.floor(raw * f)).astype(np.uint64)
+    return sizes, f
+
+
+def batched(ninst: int = 100_000, seed: int = 4, budget_chars: int = 1 << 30,
+            smin: int = 16, smax: int = 1 << 20, alloc: Callable = _alloc_np):
+    """The batched workload: ninst independent instances (batch_sizes), string
+    lengths lognormal(mu=3, sigma=0.5) clipped to [1, 256], chars uniform over
+    printable ASCII 32..126, all packed into one arena. Returns (chars, offs,
+    nchars, inst) with inst the ninst + 1 instance boundaries."""
+    sizes, _ = batch_sizes(ninst, smin, smax, budget_chars, seed=seed)
+    inst = np.zeros(ninst + 1, dtype=np.uint64)
+    np.cumsum(sizes, out=inst[1:])
+    n = int(inst[-1])
+    w = _native.work()
+    offs = alloc(8 * n, np.uint64)
+    nchars = w.pssw_lognormal_offsets(seed, n, 3.0, 0.5, 1, 256, offs.ctypes.data)
+    chars = alloc(nchars + PAD, np.uint8)
+    chars[nchars:] = 0
+    alpha = np.frombuffer(PRINTABLE, dtype=np.uint8).copy()
+    w.pssw_random_fill(seed, n, offs.ctypes.data, nchars, alpha.ctypes.data, len(alpha),
+                       chars.ctypes.data)
+    return chars, offs, int(nchars), inst
+
+
 def alg_bytes(lcp: np.ndarray, T: int = 32) -> dict:
     """Algorithmic bytes of the sample-sort method for a sorted LCP array."""
     lcp = np.ascontiguousarray(lcp, dtype=np.uint32)
@@ -97,6 +147,30 @@ def alg_bytes(lcp: np.ndarray, T: int = 32) -> dict:
     _native.work().pssw_alg_bytes(lcp.ctypes.data, lcp.shape[0], T, C.byref(tot), C.byref(rb),
                                   C.byref(bb), C.byref(mr))
     return {"total": tot.value, "rounds": rb.value, "base": bb.value, "max_round": mr.value}
+
+
+def string_lengths(chars: np.ndarray, offs: np.ndarray) -> np.ndarray:
+    """strlen of every string of the arena."""
+    zeros = np.flatnonzero(np.asarray(chars) == 0).astype(np.uint64)
+    pos = np.searchsorted(zeros, np.asarray(offs, dtype=np.uint64))
+    return (zeros[pos] - np.asarray(offs, dtype=np.uint64)).astype(np.uint64)
+
+
+def canonical_ids(chars, offs, ids, lcp, lengths=None) -> np.ndarray:
+    """Sorted ids with every run of equal strings in increasing id order: two
+    correct sorts of the same input (which may order equal strings
+    differently) have the same canonical ids. `lengths` (the strlen of every
+    string of offs) may be passed to skip scanning the arena."""
+    ids = np.asarray(ids, dtype=np.uint32)
+    n = ids.shape[0]
+    if n == 0:
+        return ids.copy()
+    lens = (string_lengths(chars, offs) if lengths is None else np.asarray(lengths))[ids]
+    lcp = np.asarray(lcp, dtype=np.uint64)
+    eq = np.zeros(n, dtype=bool)
+    eq[1:] = (lcp[1:] == lens[1:]) & (lens[1:] == lens[:-1])
+    run = np.cumsum(~eq)
+    return ids[np.lexsort((ids, run))]
 
 
 def strings_of(chars: np.ndarray, offs: np.ndarray, ids: Optional[np.ndarray] = None) -> list:

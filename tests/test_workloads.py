@@ -43,6 +43,24 @@ def test_random_strings_deterministic(pkg):
     assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
 
 
+def test_batch_sizes_cap(pkg):
+    sizes, f = pkg.workloads.batch_sizes()
+    assert len(sizes) == 100_000
+    assert sizes.min() == 16
+    assert 0 < f < 1  # the 1 GiB cap binds: about 200 GB uncapped
+    assert sizes.sum() * 23.8 <= (1 << 30)
+    assert sizes.sum() * 23.8 > 0.95 * (1 << 30)
+
+
+def test_batched_small(pkg):
+    chars, offs, nchars, inst = pkg.workloads.batched(ninst=100, budget_chars=1 << 20, seed=1)
+    assert len(inst) == 101 and inst[0] == 0 and inst[-1] == len(offs)
+    lens = string_lengths(chars, offs)
+    assert lens.min() >= 1 and lens.max() <= 256
+    body = chars[:nchars]
+    assert set(np.unique(body).tolist()) <= set(range(32, 127)) | {0}
+
+
 def test_alg_bytes_hand_count(pkg):
     # 40 strings tied at depth 0 (one group > 32) splitting into singletons
     lcp = np.zeros(40, np.uint32)

@@ -55,9 +55,13 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--cpu-sample", type=int, default=CPU_SAMPLE)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--mode", choices=["sort", "batched", "autotune"], default="sort",
+    p.add_argument("--mode", choices=["sort", "batched", "serving", "autotune"], default="sort",
                    help="sort: the headline line; batched: the 100k-instance batch "
-                        "against one call per instance; autotune: write the tuning table")
+                        "against one call per instance; serving: the request stream "
+                        "through the server; autotune: write the tuning table")
+    p.add_argument("--duration", type=float, default=60.0, help="serving: seconds of arrivals")
+    p.add_argument("--rate", type=float, default=2000.0, help="serving: requests per second")
+    p.add_argument("--budget-gb", type=float, default=40.0, help="serving: HBM budget")
     p.add_argument("--sample-instances", type=int, default=1000,
                    help="batched mode: instances timed one call each")
     return p.parse_args()
@@ -298,10 +302,52 @@ def run_batched(args):
     ctx.close()
 
 
+def run_serving(args):
+    """The serving stream: Poisson arrivals at --rate for --duration seconds,
+    sizes log-uniform 1 KB..64 MB, alphabets {4, 10, 26, 95}, lengths
+    U[1, 64], through the continuous-batching server under --budget-gb."""
+    import torch
+    import __graft_entry__
+    from importlib import import_module
+    __graft_entry__.load_package()
+    serving = import_module("pss_b200.serving")
+    alloc = pinned_alloc(torch)
+    t0 = time.perf_counter()
+    pools = serving.make_pools(bytes_per_pool=512 << 20, alloc=alloc)
+    t1 = time.perf_counter()
+    reqs = serving.make_stream(pools, rate=args.rate, duration=args.duration)
+    t2 = time.perf_counter()
+    srv = serving.Server(budget=int(args.budget_gb * (1 << 30)), workers=3,
+                         max_batch_strings=8 << 20)
+    # warm the workers' kernels with a short burst
+    serving.run_stream(srv, pools, serving.make_stream(pools, rate=2000, duration=0.05, seed=1))
+    t3 = time.perf_counter()
+    print(json.dumps({"pools_s": t1 - t0, "stream_s": t2 - t1, "server_warm_s": t3 - t2,
+                      "requests": len(reqs)}), file=sys.stderr, flush=True)
+    clocks = Clocks(0)
+    clocks.start()
+    res = serving.run_stream(srv, pools, reqs)
+    clk = clocks.stop()
+    st = srv.stats()
+    srv.close()
+    line = {"mode": "serving", "metric": "request latency and sustained char GB/s",
+            "config": {"workload": "serving-poisson", "rate_per_s": args.rate,
+                       "duration_s": args.duration, "request_bytes": "log-uniform 1 KB..64 MB",
+                       "alphabets": [4, 10, 26, 95], "lengths": "U[1,64]",
+                       "hbm_budget_gb": args.budget_gb, "workers": 3,
+                       "max_batch_strings": 8 << 20},
+            **res, "batches": st["batches"], "slab_gb": st["slab_bytes"] / 2**30,
+            "slab_peak_gb": st["slab_peak_bytes"] / 2**30, "clocks": clk}
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.mode == "serving":
+        run_serving(args)
         return
     if args.mode == "autotune":
         run_autotune()

@@ -139,6 +139,46 @@ int pssgpu_sort_batch_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t n
  * (about 16 strings per bucket). Written by the autotuner. */
 int pssgpu_ctx_set_tree_bits(pssgpu_ctx* ctx, const uint8_t* tree_bits, int count);
 
+/* ---- serving ---------------------------------------------------------------
+ * A request server with continuous batching; no counterpart in the
+ * reference. hbm_budget bounds all device memory the server holds: every
+ * worker reserves a workspace for max_batch_strings strings, the rest is a
+ * slab that keeps admitted requests' arenas and offsets resident. submit()
+ * only queues the request and returns a ticket; an admission thread admits
+ * requests in arrival order as slab space frees up, and each worker sorts
+ * all admitted requests it can take (up to max_batch_strings strings and
+ * max_batch_requests requests, 0 = 4096) as one batch on its own stream, so
+ * requests arriving while others run join the next batch and the workers'
+ * batches overlap on the device. Results are written to the caller's perm
+ * and lcp (may be NULL; lcp[0] untouched) before wait() returns; the caller
+ * keeps chars, offs and the outputs alive until then. String i of a request
+ * starts at chars + (offs[i] - offs_base). */
+typedef struct pssgpu_server pssgpu_server;
+typedef struct pssgpu_server_config {
+    uint64_t hbm_budget;
+    uint64_t max_batch_strings;
+    uint32_t workers;
+    uint32_t max_batch_requests;
+} pssgpu_server_config;
+typedef struct pssgpu_request_info {
+    int status;
+    uint32_t batch_requests;  /* requests sorted in the same batch */
+    uint64_t batch_strings;   /* strings in that batch */
+    uint64_t t_submit_ns, t_admit_ns, t_start_ns, t_done_ns;  /* steady clock */
+} pssgpu_request_info;
+typedef struct pssgpu_server_stats {
+    uint64_t slab_bytes, slab_peak_bytes;
+    uint64_t batches, batched_requests;
+    uint64_t pending, ready;
+} pssgpu_server_stats;
+int pssgpu_server_create(int device, const pssgpu_server_config* cfg, pssgpu_server** out);
+void pssgpu_server_destroy(pssgpu_server* srv);
+int pssgpu_server_submit(pssgpu_server* srv, const uint8_t* chars, uint64_t nchars,
+                         const uint64_t* offs, uint64_t offs_base, uint64_t n,
+                         uint32_t* perm, uint32_t* lcp, uint64_t* ticket);
+int pssgpu_server_wait(pssgpu_server* srv, uint64_t ticket, pssgpu_request_info* info);
+int pssgpu_server_get_stats(pssgpu_server* srv, pssgpu_server_stats* out);
+
 /* ---- psstest Contest drop-ins --------------------------------------------
  * The three contestant signatures of Contestant_UCArray
  * (src/tools/contest.hpp:88-91). Each permutes `strings` in place into

@@ -37,6 +37,13 @@ GPU_SIGNATURES = {
                                            C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
                                            C.c_void_p]),
     "pssgpu_ctx_set_tree_bits": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "pssgpu_server_create": (C.c_int, [C.c_int, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "pssgpu_server_destroy": (None, [C.c_void_p]),
+    "pssgpu_server_submit": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64,
+                                       C.c_uint64, C.c_void_p, C.c_void_p,
+                                       C.POINTER(C.c_uint64)]),
+    "pssgpu_server_wait": (C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p]),
+    "pssgpu_server_get_stats": (C.c_int, [C.c_void_p, C.c_void_p]),
     "pssgpu_sort_strings": (None, [C.c_void_p, C.c_size_t]),
     "pssgpu_sort_strings_lcp": (None, [C.c_void_p, C.c_void_p, C.c_size_t]),
     "pssgpu_sort_strings_lcp_cache": (None, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t]),
@@ -81,6 +88,38 @@ class PssKernelStats(C.Structure):
         ("strings", C.c_uint64),
         ("alg_bytes", C.c_uint64),
         ("ms", C.c_double),
+    ]
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [
+        ("hbm_budget", C.c_uint64),
+        ("max_batch_strings", C.c_uint64),
+        ("workers", C.c_uint32),
+        ("max_batch_requests", C.c_uint32),
+    ]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [
+        ("status", C.c_int),
+        ("batch_requests", C.c_uint32),
+        ("batch_strings", C.c_uint64),
+        ("t_submit_ns", C.c_uint64),
+        ("t_admit_ns", C.c_uint64),
+        ("t_start_ns", C.c_uint64),
+        ("t_done_ns", C.c_uint64),
+    ]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [
+        ("slab_bytes", C.c_uint64),
+        ("slab_peak_bytes", C.c_uint64),
+        ("batches", C.c_uint64),
+        ("batched_requests", C.c_uint64),
+        ("pending", C.c_uint64),
+        ("ready", C.c_uint64),
     ]
 
 

@@ -659,11 +659,177 @@ static int sort_pointer_array(unsigned char** strings, uintptr_t* lcp_out, uint8
 
 }  // namespace pssgpu
 
+#include "server.cuh"
+
 using namespace pssgpu;
 
-
-
 extern "C" {
+
+int pssgpu_server_create(int device, const pssgpu_server_config* cfg, pssgpu_server** out)
+{
+    if (!cfg || !out) return fail(PSSGPU_EINVAL, "null argument");
+    if (cfg->workers < 1 || cfg->workers > 16) return fail(PSSGPU_EINVAL, "1..16 workers");
+    if (cfg->max_batch_strings < 1024 || cfg->max_batch_strings > PSSGPU_MAX_STRINGS)
+        return fail(PSSGPU_EINVAL, "max_batch_strings out of range");
+    Server* s = new Server;
+    s->device = device;
+    s->budget = cfg->hbm_budget;
+    s->max_batch_strings = cfg->max_batch_strings;
+    s->max_batch_requests = cfg->max_batch_requests ? cfg->max_batch_requests : 4096;
+    auto bail = [&](int rc) {
+        pssgpu_server_destroy(reinterpret_cast<pssgpu_server*>(s));
+        return rc;
+    };
+    // each worker reserves a workspace and batch buffers for its largest batch
+    const uint64_t per_worker =
+        workspace_bytes(sizes_for(cfg->max_batch_strings)) + 16 * cfg->max_batch_strings;
+    const uint64_t reserve = per_worker * cfg->workers;
+    if (cfg->hbm_budget <= reserve + (64ull << 20))
+        return bail(fail(PSSGPU_EBUDGET, "budget below the workers' reserve"));
+    s->slab_size = align256(cfg->hbm_budget - reserve) - 256;
+    int rc;
+    if (cudaSetDevice(device) != cudaSuccess) return bail(fail(PSSGPU_ENODEV, "no such device"));
+    if (cudaMalloc(&s->slab, s->slab_size + 256) != cudaSuccess)
+        return bail(fail(PSSGPU_ENOMEM, "slab allocation failed"));
+    // the slab's tail stays zero: it ends the arena and pads the last reads
+    cudaMemset(s->slab + s->slab_size - 256, 0, 512);
+    s->alloc.init(s->slab_size - 256);
+    if (cudaStreamCreateWithFlags(&s->upload, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(fail(PSSGPU_ECUDA, "stream creation failed"));
+    for (uint32_t i = 0; i < cfg->workers; ++i) {
+        Worker* wk = new Worker;
+        wk->srv = s;
+        s->workers.push_back(wk);
+        if ((rc = ctx_create(device, &wk->ctx))) return bail(rc);
+        {
+            std::lock_guard<std::mutex> lk(wk->ctx->mu);
+            if ((rc = ensure_workspace(wk->ctx, cfg->max_batch_strings))) return bail(rc);
+        }
+        if ((rc = worker_grow(wk, cfg->max_batch_strings, 1024))) return bail(rc);
+    }
+    if (cudaDeviceSynchronize() != cudaSuccess) return bail(fail(PSSGPU_ECUDA, "set-up failed"));
+    s->admitter = std::thread(admit_loop, s);
+    for (Worker* wk : s->workers) wk->th = std::thread(worker_loop, wk);
+    *out = reinterpret_cast<pssgpu_server*>(s);
+    return PSSGPU_OK;
+}
+
+void pssgpu_server_destroy(pssgpu_server* srv)
+{
+    Server* s = reinterpret_cast<Server*>(srv);
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stopping = true;
+    }
+    s->cv_pending.notify_all();
+    s->cv_space.notify_all();
+    if (s->admitter.joinable()) s->admitter.join();
+    s->cv_ready.notify_all();
+    for (Worker* wk : s->workers) {
+        if (wk->th.joinable()) wk->th.join();
+    }
+    cudaSetDevice(s->device);
+    for (Worker* wk : s->workers) {
+        if (wk->d_offs) cudaFree(wk->d_offs);
+        if (wk->d_perm) cudaFree(wk->d_perm);
+        if (wk->d_lcp) cudaFree(wk->d_lcp);
+        if (wk->d_parts) cudaFree(wk->d_parts);
+        if (wk->h_parts) cudaFreeHost(wk->h_parts);
+        ctx_destroy(wk->ctx);
+        delete wk;
+    }
+    for (auto& kv : s->requests) {
+        if (kv.second->uploaded) cudaEventDestroy(kv.second->uploaded);
+        delete kv.second;
+    }
+    if (s->slab) cudaFree(s->slab);
+    if (s->upload) cudaStreamDestroy(s->upload);
+    delete s;
+}
+
+int pssgpu_server_submit(pssgpu_server* srv, const uint8_t* chars, uint64_t nchars,
+                         const uint64_t* offs, uint64_t offs_base, uint64_t n, uint32_t* perm,
+                         uint32_t* lcp, uint64_t* ticket)
+{
+    Server* s = reinterpret_cast<Server*>(srv);
+    if (!s || !ticket) return fail(PSSGPU_EINVAL, "null argument");
+    if (n && (!chars || !offs || !perm || nchars == 0)) return fail(PSSGPU_EINVAL, "null buffer");
+    if (n > s->max_batch_strings) return fail(PSSGPU_EBUDGET, "request above max_batch_strings");
+    if (n && chars[nchars - 1] != 0) return fail(PSSGPU_EINVAL, "arena does not end with NUL");
+    for (uint64_t i = 0; i < n; ++i)
+        if (offs[i] - offs_base >= nchars) return fail(PSSGPU_EINVAL, "offset outside the arena");
+    Request* r = new Request;
+    r->h_chars = chars;
+    r->nchars = nchars;
+    r->h_offs = offs;
+    r->offs_base = offs_base;
+    r->n = n;
+    r->h_perm = perm;
+    r->h_lcp = lcp;
+    r->region_bytes = request_bytes(nchars, n);
+    if (r->region_bytes > s->slab_size - 256) {
+        delete r;
+        return fail(PSSGPU_EBUDGET, "request larger than the serving budget");
+    }
+    if (cudaEventCreateWithFlags(&r->uploaded, cudaEventDisableTiming) != cudaSuccess) {
+        delete r;
+        return fail(PSSGPU_ECUDA, "event creation failed");
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    r->ticket = s->next_ticket++;
+    r->t_submit = now_ns();
+    s->requests[r->ticket] = r;
+    if (n == 0) {
+        r->t_admit = r->t_start = r->t_done = r->t_submit;
+        r->done = true;
+    } else {
+        s->pending.push_back(r);
+        s->cv_pending.notify_one();
+    }
+    *ticket = r->ticket;
+    return PSSGPU_OK;
+}
+
+int pssgpu_server_wait(pssgpu_server* srv, uint64_t ticket, pssgpu_request_info* info)
+{
+    Server* s = reinterpret_cast<Server*>(srv);
+    if (!s) return fail(PSSGPU_EINVAL, "null server");
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->requests.find(ticket);
+    if (it == s->requests.end()) return fail(PSSGPU_EINVAL, "unknown ticket");
+    Request* r = it->second;
+    s->cv_done.wait(lk, [&] { return r->done; });
+    const int rc = r->status;
+    if (info) {
+        info->status = r->status;
+        info->batch_requests = r->batch_requests;
+        info->batch_strings = r->batch_strings;
+        info->t_submit_ns = r->t_submit;
+        info->t_admit_ns = r->t_admit;
+        info->t_start_ns = r->t_start;
+        info->t_done_ns = r->t_done;
+    }
+    s->requests.erase(it);
+    lk.unlock();
+    cudaEventDestroy(r->uploaded);
+    delete r;
+    return rc ? fail(rc, "request failed") : PSSGPU_OK;
+}
+
+int pssgpu_server_get_stats(pssgpu_server* srv, pssgpu_server_stats* out)
+{
+    Server* s = reinterpret_cast<Server*>(srv);
+    if (!s || !out) return fail(PSSGPU_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    out->slab_bytes = s->slab_size;
+    out->slab_peak_bytes = s->peak_used;
+    out->batches = s->batches;
+    out->batched_requests = s->batched_requests;
+    out->pending = s->pending.size();
+    out->ready = s->ready.size();
+    return PSSGPU_OK;
+}
 
 const char* pssgpu_last_error(void) { return g_last_error.c_str(); }
 

@@ -61,6 +61,42 @@ def test_batched_small(pkg):
     assert set(np.unique(body).tolist()) <= set(range(32, 127)) | {0}
 
 
+def test_serving_stream_and_driver_with_a_fake_server(pkg):
+    """Host logic of the serving driver (arrivals, request cutting, the
+    submit / wait hand-off, latency figures) against a server stand-in."""
+    from importlib import import_module
+    serving = import_module("pss_b200.serving")
+    pools = serving.make_pools(bytes_per_pool=1 << 20, seed=1)
+    reqs = serving.make_stream(pools, rate=2000, duration=0.05, min_bytes=1 << 10,
+                               max_bytes=64 << 10, seed=2)
+    assert len(reqs) > 40
+    for r in reqs:
+        p = pools[r.alphabet]
+        assert r.i1 > r.i0
+        assert p.chars[r.start + r.nchars - 1] == 0  # the request ends with a NUL
+        assert int(p.offs[r.i0]) == r.start
+
+    class FakeServer:
+        def __init__(self):
+            self.t = {}
+
+        def submit(self, ptr, nchars, offs, base, perm, lcp):
+            k = len(self.t) + 1
+            perm[:] = np.arange(perm.shape[0], dtype=np.uint32)
+            self.t[k] = 1000 * k
+            return k
+
+        def wait(self, ticket):
+            t = self.t[ticket]
+            return {"status": 0, "batch_requests": 1, "batch_strings": 1,
+                    "t_submit_ns": t, "t_admit_ns": t, "t_start_ns": t + 10,
+                    "t_done_ns": t + 2_000_000}
+
+    res = serving.run_stream(FakeServer(), pools, reqs, want_lcp=True)
+    assert res["requests"] == len(reqs)
+    assert abs(res["p50_ms"] - 2.0) < 1e-9 and abs(res["p99_ms"] - 2.0) < 1e-9
+
+
 def test_alg_bytes_hand_count(pkg):
     # 40 strings tied at depth 0 (one group > 32) splitting into singletons
     lcp = np.zeros(40, np.uint32)

@@ -14,7 +14,7 @@ namespace pssgpu {
 // Error bits OR-ed into the device error word and mapped to status codes.
 enum : uint32_t {
     ERR_OFFSET = 1u,     // a string offset lies outside the arena
-    ERR_TIMEOUT = 2u,    // a look-back wait exceeded its iteration cap
+    ERR_TIMEOUT = 2u,    // a bounded device-side wait gave up (no kernel waits at present)
     ERR_OVERFLOW = 4u,   // a work list exceeded its capacity
     ERR_INTERNAL = 8u,   // an internal invariant failed (index out of range)
 };
@@ -31,7 +31,6 @@ enum : uint32_t {
     META_BUF = 1u,    // which ping-pong buffer holds the segment
     META_VALID = 2u,  // keys at `depth` are cached in keys[buf]
     META_FINAL = 4u,  // all strings equal: copy out, LCP inside = depth
-    META_NOTIE = 8u,  // skip the common-prefix jump (it made no progress)
 };
 
 __device__ __forceinline__ uint64_t bswap64(uint64_t x)

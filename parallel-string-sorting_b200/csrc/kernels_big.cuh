@@ -7,17 +7,19 @@
 //   k_classify   key gather + ClassifyTreeSimple::find_bkt + CountJob
 //                (src/sequential/bingmann-sample_sortBTC.hpp:45-72, hpp:1414-1435)
 //   k_bstart     count_finished: bucket prefix sums (hpp:1437-1460)
-//   k_scatter    distribute: decoupled look-back + shared-memory staged scatter
-//                (hpp:1464-1490)
+//   k_chunk_sum, k_chunk_scan, k_tile_offsets
+//                count_finished over (tile, bucket) counts: every tile's first
+//                destination per bucket (hpp:1437-1460)
+//   k_scatter    distribute: shared-memory staged scatter (hpp:1464-1490)
 //   k_children   distribute_finished: next segments, finished buckets, split
 //                boundaries for the LCP array (hpp:1492-1584, 311-396)
 //
-// A segment whose samples are all equal takes the common-prefix jump instead
-// of a classification: k_classify measures, for every string, the chars it
-// shares with the segment's first string beyond the current depth; the
-// segment then continues at depth + min (or is finished when all strings are
-// equal). pS5 advances such a tied group 8 bytes per step (hpp:1527-1528,
-// 1555-1556); the jump reaches the same depth in one pass.
+// A segment whose samples all share more chars beyond the current depth
+// takes a common-prefix jump inside its pass: k_sample measures the shared
+// chunks (up to JMAX_CHUNKS) and builds the tree behind them; k_classify
+// checks every string against the shared chunks and sends the few that leave
+// the prefix early to two extra buckets. pS5 advances such a tied group 8
+// bytes per step (hpp:1527-1528, 1555-1556).
 #pragma once
 
 #include "block_util.cuh"
@@ -52,21 +54,52 @@ __global__ void k_tile_scan(Work w, uint32_t nbig)
     const Seg* big = w.list[L_BIG][w.cur];
     const uint32_t per = (nbig + blockDim.x - 1) / blockDim.x;
     const uint32_t lo = min(threadIdx.x * per, nbig), hi = min(lo + per, nbig);
-    uint32_t s = 0;
-    for (uint32_t i = lo; i < hi; ++i) s += (big[i].size + TILE - 1) / TILE;
-    uint32_t total;
+    auto tiles = [&](uint32_t i) { return (big[i].size + TILE - 1) / TILE; };
+    auto chunks = [&](uint32_t i) { return (tiles(i) + CHUNK - 1) / CHUNK; };
+    uint32_t s = 0, sc = 0;
+    for (uint32_t i = lo; i < hi; ++i) {
+        s += tiles(i);
+        sc += chunks(i);
+    }
+    uint32_t total, ctotal;
     uint32_t run = block_excl_sum<1024>(s, tmp, &total);
+    uint32_t crun = block_excl_sum<1024>(sc, tmp, &ctotal);
     for (uint32_t i = lo; i < hi; ++i) {
         w.tile_start[i] = run;
-        run += (big[i].size + TILE - 1) / TILE;
+        w.chunk_start[i] = crun;
+        run += tiles(i);
+        crun += chunks(i);
     }
-    if (threadIdx.x == 0) w.tile_start[nbig] = total;
+    if (threadIdx.x == 0) {
+        w.tile_start[nbig] = total;
+        w.chunk_start[nbig] = ctotal;
+    }
+}
+
+// In-place ascending bitonic sort of S (a power of two) keys in shared
+// memory by the whole block; synchronises before returning.
+__device__ __forceinline__ void bitonic_sort_block(uint64_t* a, uint32_t S)
+{
+    for (uint32_t kk = 2; kk <= S; kk <<= 1) {
+        for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = threadIdx.x; i < S / 2; i += blockDim.x) {
+                const uint32_t x0 = 2 * i - (i & (j - 1));
+                const uint32_t x1 = x0 + j;
+                const bool asc = (x0 & kk) == 0;
+                const uint64_t x = a[x0], y = a[x1];
+                if ((x > y) == asc) { a[x0] = y; a[x1] = x; }
+            }
+            __syncthreads();
+        }
+    }
 }
 
 // One block of 1024 threads per big segment.
 __global__ void __launch_bounds__(1024) k_sample(Work w)
 {
     __shared__ uint64_t samp[2 << MAX_TREE_BITS];
+    __shared__ uint64_t shnd[2 << MAX_TREE_BITS];
+    __shared__ uint32_t jrun;
     const int s = blockIdx.x;
     const Seg sg = w.list[L_BIG][w.cur][s];
     uint32_t* bc = w.bcount + (size_t)s * MAX_BKT;
@@ -74,6 +107,7 @@ __global__ void __launch_bounds__(1024) k_sample(Work w)
     if (sg.meta & META_FINAL) {
         if (threadIdx.x == 0) {
             w.tree_bits[s] = 0;
+            w.jump[s] = 0;
             atomicAdd(w.counters + C_P_FINAL, sg.size);
         }
         return;
@@ -86,36 +120,62 @@ __global__ void __launch_bounds__(1024) k_sample(Work w)
     for (uint32_t i = threadIdx.x; i < S; i += blockDim.x) {
         const uint64_t h = mix64(((uint64_t)sg.begin << 32) ^ ((uint64_t)sg.depth << 12) ^ i);
         const uint32_t r = sg.begin + (uint32_t)(h % sg.size);
-        samp[i] = valid ? w.keys[buf][r]
-                        : h_key(w, w.hnd[buf][r], sg.depth);
+        const uint64_t hd = w.hnd[buf][r];
+        shnd[i] = hd;
+        samp[i] = valid ? w.keys[buf][r] : h_key(w, hd, sg.depth);
     }
     __syncthreads();
-    // bitonic sort of the S samples
-    for (uint32_t kk = 2; kk <= S; kk <<= 1) {
-        for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
-            for (uint32_t i = threadIdx.x; i < S / 2; i += blockDim.x) {
-                const uint32_t a = 2 * i - (i & (j - 1));
-                const uint32_t b = a + j;
-                const bool asc = (a & kk) == 0;
-                const uint64_t x = samp[a], y = samp[b];
-                if ((x > y) == asc) { samp[a] = y; samp[b] = x; }
-            }
+    bitonic_sort_block(samp, S);
+    uint32_t J = 0;  // chunks of the common-prefix jump
+    if (samp[0] == samp[S - 1] && !key_terminated(samp[0])) {
+        // Every sample shares the chunk at the segment depth: count the
+        // further chunks they all share, four per round, up to JMAX_CHUNKS.
+        // pS5 would advance such a tied group one chunk per step
+        // (hpp:1527-1528, 1555-1556).
+        const uint64_t ref = h_off(w, shnd[0]) + sg.depth;
+        J = 1;
+        while (J < (uint32_t)JMAX_CHUNKS) {
+            if (threadIdx.x == 0) jrun = 4;
             __syncthreads();
+            uint64_t rk[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) rk[q] = load_key(w.chars, w.nchars, ref + 8ull * (J + q));
+            uint32_t mine = 4;
+            for (uint32_t i = threadIdx.x; i < S; i += blockDim.x) {
+                const uint64_t o = h_off(w, shnd[i]) + sg.depth;
+                uint32_t e = 0;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const uint64_t kq = load_key(w.chars, w.nchars, o + 8ull * (J + q));
+                    if (e == (uint32_t)q && kq == rk[q] && !key_terminated(kq)) e = q + 1;
+                }
+                mine = min(mine, e);
+            }
+            if (mine < 4) atomicMin(&jrun, mine);
+            __syncthreads();
+            const uint32_t e = jrun;
+            __syncthreads();
+            J += e;
+            if (e < 4) break;
         }
-    }
-    if (samp[0] == samp[S - 1] && !(sg.meta & META_NOTIE)) {
-        // all samples equal: most likely one tied group -> common-prefix jump
-        if (threadIdx.x == 0) {
-            w.tree_bits[s] = TREE_TIE;
-            w.jump_min[s] = 0xFFFFFFFFu;
-            w.jump_diff[s] = 0;
-            atomicAdd(w.counters + C_P_TIE, sg.size);
-        }
-        return;
+        J = min(J, (uint32_t)JMAX_CHUNKS);
+        // the shared chunks as keys, and the samples' keys behind them
+        uint64_t* jp = w.jpre + (size_t)s * JMAX_CHUNKS;
+        for (uint32_t c = threadIdx.x; c < J; c += blockDim.x)
+            jp[c] = load_key(w.chars, w.nchars, ref + 8ull * c);
+        for (uint32_t i = threadIdx.x; i < S; i += blockDim.x)
+            samp[i] = h_key(w, shnd[i], sg.depth + 8 * J);
+        __syncthreads();
+        bitonic_sort_block(samp, S);
     }
     if (threadIdx.x == 0) {
+        w.jump[s] = 8 * J;
         atomicAdd(w.counters + C_P_BIG, sg.size);
-        if (!valid) atomicAdd(w.counters + C_P_STALE, sg.size);
+        if (!valid || J) atomicAdd(w.counters + C_P_STALE, sg.size);
+        if (J) {
+            atomicAdd(w.counters + C_P_TIE, sg.size);
+            atomicAdd(w.counters + C_P_JCHUNKS, sg.size * J);
+        }
     }
     // splitters: every second sample; level-order tree over them
     uint64_t* spl = w.spl + (size_t)s * 1024;
@@ -130,44 +190,18 @@ __global__ void __launch_bounds__(1024) k_sample(Work w)
     if (threadIdx.x == 0) w.tree_bits[s] = (uint8_t)L;
 }
 
-// Chars the string behind handle h shares with the base string (at arena
-// offset boff, both from depth d on); *differs is set when the two strings
-// are not equal. Gives up (returning a value > stop) once the shared length
-// exceeds `stop`, which then cannot lower the segment minimum. Two 8-byte
-// chunks per step keep two loads of each string in flight.
-__device__ __forceinline__ uint32_t shared_chars(const Work& w, uint64_t boff, uint64_t h,
-                                                 uint32_t d, uint32_t stop, bool* differs)
-{
-    const uint64_t o = h_off(w, h) + d;
-    for (uint32_t c = 0;; c += 2) {
-        if (8u * c > stop) return 8u * c;
-        const uint64_t ka0 = load_key(w.chars, w.nchars, boff + 8ull * c);
-        const uint64_t kb0 = load_key(w.chars, w.nchars, o + 8ull * c);
-        const uint64_t ka1 = load_key(w.chars, w.nchars, boff + 8ull * c + 8);
-        const uint64_t kb1 = load_key(w.chars, w.nchars, o + 8ull * c + 8);
-        if (ka0 != kb0) {
-            *differs = true;
-            return 8u * c + lcp_key_type(ka0, kb0);
-        }
-        if (key_terminated(ka0)) return 8u * c + lcp_key_depth(ka0);
-        if (ka1 != kb1) {
-            *differs = true;
-            return 8u * c + 8 + lcp_key_type(ka1, kb1);
-        }
-        if (key_terminated(ka1)) return 8u * c + 8 + lcp_key_depth(ka1);
-    }
-}
-
 // One block per tile of a big segment: gather keys if stale, classify,
-// store bucket ids, add the tile histogram into the segment's counts.
-// Tiles of finished (all-equal) segments copy ids and LCPs to the output;
-// tiles of jump segments measure the common prefix.
+// store bucket ids and the tile histogram, add it into the segment's counts.
+// Behind a common-prefix jump a string first compares its chunks with the
+// shared ones (all loads of a string in flight at once): an earlier
+// difference puts it into the first or last bucket, else its key after the
+// prefix goes through the tree (bucket + 1).
+// Tiles of finished (all-equal) segments copy ids and LCPs to the output.
 __global__ void __launch_bounds__(TILE_THREADS) k_classify(Work w, uint32_t nbig)
 {
     __shared__ uint64_t tree[1024];
+    __shared__ uint64_t jp[JMAX_CHUNKS];
     __shared__ uint32_t hist[MAX_BKT];
-    __shared__ uint32_t best;
-    __shared__ uint32_t anydiff;
     const uint32_t t = blockIdx.x;
     const int s = find_tile_seg(w.tile_start, nbig, t);
     const Seg sg = w.list[L_BIG][w.cur][s];
@@ -183,65 +217,73 @@ __global__ void __launch_bounds__(TILE_THREADS) k_classify(Work w, uint32_t nbig
         return;
     }
     const uint32_t L = w.tree_bits[s];
-    if (L == TREE_TIE) {
-        if (threadIdx.x == 0) {
-            best = *((volatile uint32_t*)(w.jump_min + s));
-            anydiff = 0;
-        }
-        __syncthreads();
-        const uint64_t boff = h_off(w, hs[sg.begin]) + sg.depth;
-        bool differs = false;
-        for (uint32_t p = lo + threadIdx.x; p < hi; p += TILE_THREADS) {
-            const uint32_t stop = *((volatile uint32_t*)&best);
-            const uint32_t l = shared_chars(w, boff, hs[p], sg.depth, stop, &differs);
-            if (l < stop) atomicMin(&best, l);
-        }
-        if (differs) anydiff = 1;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            atomicMin(w.jump_min + s, best);
-            if (anydiff) atomicOr(w.jump_diff + s, 1u);
-        }
-        return;
-    }
+    const uint32_t J = w.jump[s];
+    const uint32_t nc = J / 8;
     const uint32_t k = (1u << L) - 1;
-    const uint32_t B = 2 * k + 1;
+    const uint32_t B = seg_buckets(w, s);
     const uint64_t* gtree = w.tree + (size_t)s * 1024;
     for (uint32_t v = threadIdx.x; v <= k; v += TILE_THREADS) tree[v] = gtree[v];
+    for (uint32_t c = threadIdx.x; c < nc; c += TILE_THREADS) jp[c] = w.jpre[(size_t)s * JMAX_CHUNKS + c];
     for (uint32_t b = threadIdx.x; b < B; b += TILE_THREADS) hist[b] = 0;
     __syncthreads();
-    const bool valid = sg.meta & META_VALID;
+    const bool valid = (sg.meta & META_VALID) && !J;
     uint64_t* keys = w.keys[buf];
     for (uint32_t p = lo + threadIdx.x; p < hi; p += TILE_THREADS) {
-        uint64_t key;
+        uint64_t key = 0;
+        int side = 0;  // -1: below the prefix, +1: above it
         if (valid) {
             key = keys[p];
-        } else {
+        } else if (!J) {
             key = h_key(w, hs[p], sg.depth);
             keys[p] = key;
+        } else {
+            const uint64_t o = h_off(w, hs[p]) + sg.depth;
+            for (uint32_t c0 = 0; c0 <= nc && !side; c0 += 4) {
+                uint64_t kk[4];
+#pragma unroll
+                for (uint32_t q = 0; q < 4; ++q)
+                    kk[q] = c0 + q <= nc ? load_key(w.chars, w.nchars, o + 8ull * (c0 + q)) : 0ull;
+#pragma unroll
+                for (uint32_t q = 0; q < 4; ++q) {
+                    const uint32_t c = c0 + q;
+                    if (side || c > nc) continue;
+                    if (c == nc) key = kk[q];
+                    else if (kk[q] != jp[c]) side = kk[q] < jp[c] ? -1 : 1;
+                }
+            }
+            keys[p] = key;
         }
-        uint32_t i = 1;
-        uint64_t cand = 0;
-        for (uint32_t l = 0; l < L; ++l) {
-            const uint64_t tv = tree[i];
-            const bool gt = key > tv;
-            cand = gt ? cand : tv;
-            i = 2 * i + (gt ? 1u : 0u);
+        uint32_t b;
+        if (side) {
+            b = side < 0 ? 0u : B - 1;
+        } else {
+            uint32_t i = 1;
+            uint64_t cand = 0;
+            for (uint32_t l = 0; l < L; ++l) {
+                const uint64_t tv = tree[i];
+                const bool gt = key > tv;
+                cand = gt ? cand : tv;
+                i = 2 * i + (gt ? 1u : 0u);
+            }
+            const uint32_t r = i - (1u << L);  // splitters < key
+            b = 2 * r + ((r < k && cand == key) ? 1u : 0u) + (J ? 1u : 0u);
         }
-        const uint32_t r = i - (1u << L);  // splitters < key
-        const uint32_t b = 2 * r + ((r < k && cand == key) ? 1u : 0u);
         w.bkt[p] = (uint16_t)b;
         atomicAdd(&hist[b], 1u);
     }
     __syncthreads();
     uint32_t* bc = w.bcount + (size_t)s * MAX_BKT;
-    for (uint32_t b = threadIdx.x; b < B; b += TILE_THREADS)
-        if (hist[b]) atomicAdd(bc + b, hist[b]);
+    uint32_t* row = w.tcount + (size_t)t * MAX_BKT;
+    for (uint32_t b = threadIdx.x; b < B; b += TILE_THREADS) {
+        const uint32_t h = hist[b];
+        row[b] = h;
+        if (h) atomicAdd(bc + b, h);
+    }
 }
 
 __device__ __forceinline__ bool classified(uint8_t L)
 {
-    return L != 0 && L != TREE_TIE;
+    return L != 0;
 }
 
 // Bucket starts (exclusive prefix over buckets) and the one-bucket test.
@@ -254,7 +296,7 @@ __global__ void __launch_bounds__(1024) k_bstart(Work w)
     const Seg sg = w.list[L_BIG][w.cur][s];
     const uint8_t L = w.tree_bits[s];
     if (!classified(L)) return;
-    const uint32_t B = (2u << L) - 1;
+    const uint32_t B = seg_buckets(w, s);
     const uint32_t* bc = w.bcount + (size_t)s * MAX_BKT;
     if (threadIdx.x == 0) one = 0;
     __syncthreads();
@@ -273,11 +315,93 @@ __global__ void __launch_bounds__(1024) k_bstart(Work w)
     }
 }
 
-// Decoupled look-back status word: epoch (16) | flag (2) | count (46).
-constexpr uint64_t LB_AGG = 1ull, LB_PRE = 2ull;
-__device__ __forceinline__ uint64_t lb_word(uint32_t epoch, uint64_t flag, uint64_t v)
+// The chunk of a scan kernel's block: segment s, tiles [t0, t1). False when
+// the block has no chunk or the segment is not scattered.
+__device__ __forceinline__ bool chunk_tiles(const Work& w, uint32_t nbig, uint32_t c, int* s,
+                                            uint32_t* t0, uint32_t* t1)
 {
-    return ((uint64_t)epoch << 48) | (flag << 46) | v;
+    if (c >= w.chunk_start[nbig]) return false;
+    *s = find_tile_seg(w.chunk_start, nbig, c);
+    if (!classified(w.tree_bits[*s]) || w.bflags[*s]) return false;
+    *t0 = w.tile_start[*s] + (c - w.chunk_start[*s]) * CHUNK;
+    *t1 = min(*t0 + CHUNK, w.tile_start[*s + 1]);
+    return true;
+}
+
+// Per chunk of a multi-chunk segment and slice of 256 buckets (blockIdx.y):
+// bucket sums over the chunk's tiles.
+__global__ void __launch_bounds__(256) k_chunk_sum(Work w, uint32_t nbig)
+{
+    const uint32_t c = blockIdx.x;
+    int s;
+    uint32_t t0, t1;
+    if (!chunk_tiles(w, nbig, c, &s, &t0, &t1)) return;
+    if (w.chunk_start[s + 1] - w.chunk_start[s] == 1) return;  // k_chunk_scan sets its base
+    const uint32_t B = seg_buckets(w, s);
+    const uint32_t b = blockIdx.y * 256 + threadIdx.x;
+    if (b >= B) return;
+    const uint32_t* col = w.tcount + (size_t)t0 * MAX_BKT + b;
+    const uint32_t nt = t1 - t0;
+    uint32_t sum = 0;
+#pragma unroll
+    for (uint32_t j = 0; j < (uint32_t)CHUNK; ++j)
+        if (j < nt) sum += col[(size_t)j * MAX_BKT];
+    w.ccount[(size_t)c * MAX_BKT + b] = sum;
+}
+
+// Per segment and slice of 128 buckets: exclusive scan of the chunk sums
+// over the segment's chunks, offset by the segment begin and bucket start.
+__global__ void __launch_bounds__(128) k_chunk_scan(Work w)
+{
+    const int s = blockIdx.x;
+    const uint8_t L = w.tree_bits[s];
+    if (!classified(L) || w.bflags[s]) return;
+    const uint32_t B = seg_buckets(w, s);
+    const uint32_t b = blockIdx.y * 128 + threadIdx.x;
+    if (b >= B) return;
+    const uint32_t c0 = w.chunk_start[s], C = w.chunk_start[s + 1] - c0;
+    uint32_t run = w.list[L_BIG][w.cur][s].begin + w.bstart[(size_t)s * MAX_BKT + b];
+    uint32_t* cc = w.ccount + (size_t)c0 * MAX_BKT + b;
+    if (C == 1) {
+        cc[0] = run;
+        return;
+    }
+    constexpr uint32_t U = 8;  // loads in flight per thread
+    for (uint32_t j = 0; j < C; j += U) {
+        uint32_t v[U];
+#pragma unroll
+        for (uint32_t q = 0; q < U; ++q) v[q] = j + q < C ? cc[(size_t)(j + q) * MAX_BKT] : 0u;
+#pragma unroll
+        for (uint32_t q = 0; q < U; ++q) {
+            if (j + q < C) cc[(size_t)(j + q) * MAX_BKT] = run;
+            run += v[q];
+        }
+    }
+}
+
+// Per chunk and slice of 256 buckets: each tile's first destination per
+// bucket (the chunk base plus the counts of the chunk's earlier tiles),
+// written over the tile counts.
+__global__ void __launch_bounds__(256) k_tile_offsets(Work w, uint32_t nbig)
+{
+    const uint32_t c = blockIdx.x;
+    int s;
+    uint32_t t0, t1;
+    if (!chunk_tiles(w, nbig, c, &s, &t0, &t1)) return;
+    const uint32_t B = seg_buckets(w, s);
+    const uint32_t b = blockIdx.y * 256 + threadIdx.x;
+    if (b >= B) return;
+    uint32_t* col = w.tcount + (size_t)t0 * MAX_BKT + b;
+    const uint32_t nt = t1 - t0;
+    uint32_t run = w.ccount[(size_t)c * MAX_BKT + b];
+    uint32_t v[CHUNK];
+#pragma unroll
+    for (uint32_t j = 0; j < (uint32_t)CHUNK; ++j) v[j] = j < nt ? col[(size_t)j * MAX_BKT] : 0u;
+#pragma unroll
+    for (uint32_t j = 0; j < (uint32_t)CHUNK; ++j) {
+        if (j < nt) col[(size_t)j * MAX_BKT] = run;
+        run += v[j];
+    }
 }
 
 struct ScatterSmem {
@@ -286,29 +410,25 @@ struct ScatterSmem {
     uint32_t lcount[MAX_BKT];  // per-bucket count in the tile, then its start
     uint32_t gdelta[MAX_BKT];  // per bucket: global position - tile slot
     uint32_t tmp[32];
-    uint32_t vt;
 };
 
-// One block per tile, tiles taken in ticket order so that every tile's
-// predecessors in its segment are already resident or done.
+// One block per tile: rank every string inside its bucket, stage the tile in
+// bucket order in shared memory, write bucket runs contiguously from the
+// tile's destinations (k_tile_offsets).
 __global__ void __launch_bounds__(TILE_THREADS) k_scatter(Work w, uint32_t nbig)
 {
     constexpr int PER = TILE / TILE_THREADS;
-    constexpr int NB = MAX_BKT / TILE_THREADS;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ScatterSmem& sm = *reinterpret_cast<ScatterSmem*>(smem_raw);
-    if (threadIdx.x == 0) sm.vt = atomicAdd(w.counters + C_TICKET, 1u);
-    __syncthreads();
-    const uint32_t vt = sm.vt;
-    const int s = find_tile_seg(w.tile_start, nbig, vt);
+    const uint32_t t = blockIdx.x;
+    const int s = find_tile_seg(w.tile_start, nbig, t);
     const Seg sg = w.list[L_BIG][w.cur][s];
     const uint8_t L = w.tree_bits[s];
     if (!classified(L) || w.bflags[s]) return;
-    const uint32_t tin = vt - w.tile_start[s];
-    const uint32_t lo = sg.begin + tin * TILE;
+    const uint32_t lo = sg.begin + (t - w.tile_start[s]) * TILE;
     const uint32_t hi = min(lo + TILE, sg.begin + sg.size);
     const uint32_t cnt = hi - lo;
-    const uint32_t B = (2u << L) - 1;
+    const uint32_t B = seg_buckets(w, s);
     const int buf = sg.meta & META_BUF;
     for (uint32_t b = threadIdx.x; b < B; b += TILE_THREADS) sm.lcount[b] = 0;
     __syncthreads();
@@ -324,70 +444,10 @@ __global__ void __launch_bounds__(TILE_THREADS) k_scatter(Work w, uint32_t nbig)
         }
     }
     __syncthreads();
-    // publish this tile's per-bucket counts, then look back for the prefix
-    volatile uint64_t* st = w.status + (size_t)vt * MAX_BKT;
-    const uint32_t ep = w.epoch;
-    for (uint32_t b = threadIdx.x; b < B; b += TILE_THREADS)
-        st[b] = lb_word(ep, tin == 0 ? LB_PRE : LB_AGG, sm.lcount[b]);
-    // Look back for every bucket this thread owns at once: each round issues
-    // one status load per unfinished bucket, so the chains overlap in memory.
-    uint64_t excl[NB];
-    uint32_t jb[NB];
-    uint32_t open = 0;  // bit i: bucket threadIdx.x + i * TILE_THREADS still walking
-#pragma unroll
-    for (int i = 0; i < NB; ++i) {
-        excl[i] = 0;
-        jb[i] = vt - 1;
-        const uint32_t b = threadIdx.x + i * TILE_THREADS;
-        if (tin > 0 && b < B) open |= 1u << i;
-    }
-    uint32_t spins = 0;
-    while (open) {
-        uint64_t wd[NB];
-#pragma unroll
-        for (int i = 0; i < NB; ++i)
-            if (open & (1u << i))
-                wd[i] = *((volatile uint64_t*)(w.status + (size_t)jb[i] * MAX_BKT + threadIdx.x +
-                                               i * TILE_THREADS));
-        bool waiting = false;
-#pragma unroll
-        for (int i = 0; i < NB; ++i) {
-            if (!(open & (1u << i))) continue;
-            const uint64_t flag = (wd[i] >> 46) & 3u;
-            if ((uint32_t)(wd[i] >> 48) != ep || flag == 0) {
-                waiting = true;
-                continue;
-            }
-            excl[i] += wd[i] & ((1ull << 46) - 1);
-            if (flag == LB_PRE) open &= ~(1u << i);
-            else --jb[i];
-        }
-        if (waiting) {
-            // bounded wait: give up (and make every later wait give up at
-            // once) after SPIN_CAP polls
-            if (++spins > SPIN_CAP || (*((volatile uint32_t*)(w.counters + C_ERR)) & ERR_TIMEOUT)) {
-                set_error(w.counters + C_ERR, ERR_TIMEOUT);
-                break;
-            }
-            if (spins > 64) __nanosleep(64);
-        }
-    }
-    if (tin > 0) {
-#pragma unroll
-        for (int i = 0; i < NB; ++i) {
-            const uint32_t b = threadIdx.x + i * TILE_THREADS;
-            if (b < B) st[b] = lb_word(ep, LB_PRE, excl[i] + sm.lcount[b]);
-        }
-    }
-    __syncthreads();
     block_scan_array<TILE_THREADS>(sm.lcount, (int)B, sm.tmp);  // counts -> tile starts
-    const uint32_t* bs = w.bstart + (size_t)s * MAX_BKT;
-#pragma unroll
-    for (int i = 0; i < NB; ++i) {
-        const uint32_t b = threadIdx.x + i * TILE_THREADS;
-        if (b < B) sm.gdelta[b] = sg.begin + bs[b] + (uint32_t)excl[i] - sm.lcount[b];
-    }
-    // stage keys in bucket order and write bucket runs contiguously; then ids
+    const uint32_t* dst = w.tcount + (size_t)t * MAX_BKT;
+    for (uint32_t b = threadIdx.x; b < B; b += TILE_THREADS) sm.gdelta[b] = dst[b] - sm.lcount[b];
+    // stage keys in bucket order and write bucket runs contiguously; then handles
     const uint64_t* ikeys = w.keys[buf];
 #pragma unroll
     for (int j = 0; j < PER; ++j) {
@@ -401,7 +461,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_scatter(Work w, uint32_t nbig)
     uint64_t* okeys = w.keys[buf ^ 1];
     for (uint32_t slot = threadIdx.x; slot < cnt; slot += TILE_THREADS) {
         const uint32_t dest = slot + sm.gdelta[sm.sbkt[slot]];
-        if (dest - sg.begin >= sg.size) {  // only after a failed look-back
+        if (dest - sg.begin >= sg.size) {  // counts and destinations disagree
             set_error(w.counters + C_ERR, ERR_INTERNAL);
             continue;
         }
@@ -441,8 +501,11 @@ __device__ __forceinline__ void push_seg(Work& w, int nxt, Seg c)
     else atomicAdd(w.counters + C_PAR * nxt + C_NSTR + cls, c.size);
 }
 
-// Children of each bucket, after the scatter has placed them; the next
-// segment of a jump segment.
+// Children of each bucket, after the scatter has placed them (hpp:1492-1584):
+// '<' buckets keep their depth and keys, '=' buckets go 8 chars deeper or
+// are finished when their splitter ends the string. Behind a common-prefix
+// jump the tree buckets sit at depth + jump, and the two prefix buckets stay
+// at the segment depth without keys.
 __global__ void __launch_bounds__(1024) k_children(Work w)
 {
     const int s = blockIdx.x;
@@ -450,18 +513,6 @@ __global__ void __launch_bounds__(1024) k_children(Work w)
     const uint8_t L = w.tree_bits[s];
     const int buf = sg.meta & META_BUF;
     const int nxt = w.cur ^ 1;
-    if (L == TREE_TIE) {
-        if (threadIdx.x == 0) {
-            const uint32_t mn = w.jump_min[s];
-            if (!w.jump_diff[s])  // every string equals the base
-                push_seg(w, nxt, Seg{sg.begin, sg.size, sg.depth + mn, (uint32_t)buf | META_FINAL});
-            else if (mn == 0)     // no shared char: classify at this depth
-                push_seg(w, nxt, Seg{sg.begin, sg.size, sg.depth, (uint32_t)buf | META_NOTIE});
-            else
-                push_seg(w, nxt, Seg{sg.begin, sg.size, sg.depth + mn, (uint32_t)buf});
-        }
-        return;
-    }
     if (!classified(L)) return;
     // block-aggregated appends: slots in shared memory first, then one
     // global reservation per list
@@ -470,7 +521,9 @@ __global__ void __launch_bounds__(1024) k_children(Work w)
     if (threadIdx.x < L_NCLASS) { lcnt[threadIdx.x] = 0; lstr[threadIdx.x] = 0; }
     if (threadIdx.x == 0) { ltiles = 0; lbnd = 0; }
     __syncthreads();
-    const uint32_t B = (2u << L) - 1;
+    const uint32_t J = w.jump[s];
+    const uint32_t B = seg_buckets(w, s);
+    const uint32_t dj = sg.depth + J;  // depth of the tree buckets
     const int nbuf = w.bflags[s] ? buf : buf ^ 1;
     const uint32_t* bc = w.bcount + (size_t)s * MAX_BKT;
     const uint32_t* bs = w.bstart + (size_t)s * MAX_BKT;
@@ -479,7 +532,7 @@ __global__ void __launch_bounds__(1024) k_children(Work w)
     constexpr int PER = (MAX_BKT + 1023) / 1024;
     Seg child[PER];
     int cls[PER];
-    uint32_t slot[PER], bslot[PER];
+    uint32_t slot[PER], bslot[PER], bdep[PER];
 #pragma unroll
     for (int j = 0; j < PER; ++j) {
         cls[j] = -1;
@@ -489,15 +542,24 @@ __global__ void __launch_bounds__(1024) k_children(Work w)
         const uint32_t c = bc[b];
         if (c == 0) continue;
         const uint32_t P = sg.begin + bs[b];
-        if (P > sg.begin && w.lcp) bslot[j] = atomicAdd(&lbnd, 1u);
+        const bool edge = J && (b == 0 || b == B - 1);  // a prefix bucket
+        if (P > sg.begin && w.lcp) {
+            bslot[j] = atomicAdd(&lbnd, 1u);
+            // the string before P is in a prefix bucket, or this one is: the
+            // two strings are only known to share the segment depth
+            bdep[j] = (J && (b == B - 1 || bs[b] == bc[0])) ? sg.depth : dj;
+        }
         if (c == 1) {
             w.perm[P] = h_id(w, hs[P]);
             continue;
         }
-        if (b & 1) {
-            const uint64_t key = spl[b >> 1];
+        const uint32_t tb = J ? b - 1 : b;  // tree bucket
+        if (edge) {
+            child[j] = Seg{P, c, sg.depth, (uint32_t)nbuf};
+        } else if (tb & 1) {
+            const uint64_t key = spl[tb >> 1];
             if (key_terminated(key)) {
-                const uint32_t v = sg.depth + lcp_key_depth(key);
+                const uint32_t v = dj + lcp_key_depth(key);
                 if (c <= FINAL_INLINE) {
                     for (uint32_t q = 0; q < c; ++q) {
                         w.perm[P + q] = h_id(w, hs[P + q]);
@@ -507,10 +569,10 @@ __global__ void __launch_bounds__(1024) k_children(Work w)
                 }
                 child[j] = Seg{P, c, v, (uint32_t)nbuf | META_FINAL};
             } else {
-                child[j] = Seg{P, c, sg.depth + 8, (uint32_t)nbuf};
+                child[j] = Seg{P, c, dj + 8, (uint32_t)nbuf};
             }
         } else {
-            child[j] = Seg{P, c, sg.depth, (uint32_t)nbuf | META_VALID};
+            child[j] = Seg{P, c, dj, (uint32_t)nbuf | META_VALID};
         }
         if (c > SMALL_MAX) cls[j] = L_BIG;
         else if (c > 256) cls[j] = L_SMALLB;
@@ -534,7 +596,7 @@ __global__ void __launch_bounds__(1024) k_children(Work w)
         if (b >= B) continue;
         if (bslot[j] != 0xFFFFFFFFu) {
             const uint32_t at = bbase + bslot[j];
-            if (at < w.bnd_cap) w.bnd[at] = make_uint2(sg.begin + bs[b], sg.depth);
+            if (at < w.bnd_cap) w.bnd[at] = make_uint2(sg.begin + bs[b], bdep[j]);
             else set_error(w.counters + C_ERR, ERR_OVERFLOW);
         }
         if (cls[j] >= 0) {
@@ -545,17 +607,25 @@ __global__ void __launch_bounds__(1024) k_children(Work w)
     }
 }
 
-// LCP at each split boundary: the two strings met at `depth` in different
-// buckets, so their keys at that depth differ (sample_sort_lcp, hpp:311-396).
+// LCP at each split boundary (sample_sort_lcp, hpp:311-396): the two strings
+// share at least `depth` chars and lie in different buckets; compare 8 chars
+// at a time from there (one step unless a common-prefix jump lies between).
 __global__ void k_boundary_lcp(Work w)
 {
     const uint32_t nb = min(w.counters[C_NBND], w.bnd_cap);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x) {
         const uint2 e = w.bnd[i];
-        const uint32_t P = e.x, d = e.y;
-        const uint64_t ka = gather_key(w.chars, w.nchars, w.offs, w.perm[P - 1], d);
-        const uint64_t kb = gather_key(w.chars, w.nchars, w.offs, w.perm[P], d);
-        w.lcp[P] = d + lcp_key_type(ka, kb);
+        const uint32_t P = e.x;
+        uint32_t d = e.y;
+        const uint32_t ia = w.perm[P - 1], ib = w.perm[P];
+        uint64_t ka, kb;
+        while (true) {
+            ka = gather_key(w.chars, w.nchars, w.offs, ia, d);
+            kb = gather_key(w.chars, w.nchars, w.offs, ib, d);
+            if (ka != kb || key_terminated(ka)) break;
+            d += 8;
+        }
+        w.lcp[P] = d + (ka != kb ? lcp_key_type(ka, kb) : lcp_key_depth(ka));
     }
 }
 

@@ -115,12 +115,13 @@ static uint64_t workspace_bytes(const Sizes& s)
     b += align256(8 * s.n);                        // boundary list
     for (int c = 0; c < L_NCLASS; ++c)
         b += 2 * align256(16 * s.cap[c]);          // segment lists
-    b += align256(4 * (big + 1));                  // tile starts
+    b += 2 * align256(4 * (big + 1));              // tile starts, chunk starts
     b += 2 * align256(big);                        // tree bits, one-bucket flags
-    b += 2 * align256(4 * big);                    // jump minimum, jump differs
+    b += align256(4 * big);                        // jump lengths
+    b += align256(8ull * JMAX_CHUNKS * big);       // jump prefixes
     b += 2 * align256(8ull * 1024 * big);          // trees, splitters
     b += 2 * align256(4ull * MAX_BKT * big);       // bucket counts, starts
-    b += align256(8ull * MAX_BKT * s.tile_cap);    // look-back status
+    b += 2 * align256(4ull * MAX_BKT * s.tile_cap);  // tile and chunk counts (chunks <= tiles)
     b += align256(4 * C_COUNT);                    // counters
     return b;
 }
@@ -149,7 +150,6 @@ struct Ctx {
     uint64_t ws_bytes = 0;
     Sizes cap{};
     Work base{};
-    uint32_t epoch = 0;
     uint32_t* host_counters = nullptr;  // pinned
     // staging for the host entry points
     unsigned char* io = nullptr;
@@ -167,6 +167,12 @@ struct Ctx {
     uint64_t inst_cap = 0;
     cudaEvent_t kev[2 * K_NCLASS] = {};
     KStat kstat[K_NCLASS];
+    // the small-segment classes of a pass run on their own streams, beside
+    // the big-segment chain on the caller's stream (disjoint ranges of the
+    // permutation); fork / join through events
+    cudaStream_t side[3] = {};
+    cudaEvent_t fork_ev = nullptr;
+    cudaEvent_t join_ev[3] = {};
 };
 
 // Record the start / end of a kernel class in profile mode.
@@ -223,19 +229,19 @@ static int ensure_workspace(Ctx* c, uint64_t n)
     }
     const uint64_t big = s.cap[L_BIG];
     w.tile_start = (uint32_t*)take(4 * (big + 1));
+    w.chunk_start = (uint32_t*)take(4 * (big + 1));
     w.tree_bits = (uint8_t*)take(big);
     w.bflags = (uint8_t*)take(big);
-    w.jump_min = (uint32_t*)take(4 * big);
-    w.jump_diff = (uint32_t*)take(4 * big);
+    w.jump = (uint32_t*)take(4 * big);
+    w.jpre = (uint64_t*)take(8ull * JMAX_CHUNKS * big);
     w.tree = (uint64_t*)take(8ull * 1024 * big);
     w.spl = (uint64_t*)take(8ull * 1024 * big);
     w.bcount = (uint32_t*)take(4ull * MAX_BKT * big);
     w.bstart = (uint32_t*)take(4ull * MAX_BKT * big);
-    w.status = (uint64_t*)take(8ull * MAX_BKT * s.tile_cap);
+    w.tcount = (uint32_t*)take(4ull * MAX_BKT * s.tile_cap);
+    w.ccount = (uint32_t*)take(4ull * MAX_BKT * s.tile_cap);
     w.tile_cap = (uint32_t)s.tile_cap;
     w.counters = (uint32_t*)take(4 * C_COUNT);
-    PSS_CUDA(cudaMemsetAsync(w.status, 0, 8ull * MAX_BKT * s.tile_cap, c->stream));
-    c->epoch = 0;
     return PSSGPU_OK;
 }
 
@@ -264,7 +270,7 @@ static int setup_kernels()
 static int map_device_error(uint32_t err)
 {
     if (err & ERR_OFFSET) return fail(PSSGPU_EINVAL, "a string offset lies outside the arena");
-    if (err & ERR_TIMEOUT) return fail(PSSGPU_ETIMEOUT, "a look-back wait exceeded its iteration cap");
+    if (err & ERR_TIMEOUT) return fail(PSSGPU_ETIMEOUT, "a bounded device-side wait gave up");
     if (err & ERR_OVERFLOW) return fail(PSSGPU_ECUDA, "an internal work list overflowed");
     return fail(PSSGPU_ECUDA, "internal device error");
 }
@@ -318,43 +324,52 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
         const int nxt = cur ^ 1;
         const uint32_t nbig = cnt[L_BIG];
         w.cur = cur;
-        if (nbig) {
-            if (++c->epoch >= 0xFFFFu) {
-                PSS_CUDA(cudaMemsetAsync(w.status, 0, 8ull * MAX_BKT * c->cap.tile_cap, st));
-                c->epoch = 1;
-            }
-            w.epoch = c->epoch;
-        }
         PSS_CUDA(cudaMemsetAsync(w.counters + C_PAR * nxt, 0, 4 * C_PAR, st));
-        PSS_CUDA(cudaMemsetAsync(w.counters + C_TICKET, 0, 4, st));
         PSS_CUDA(cudaMemsetAsync(w.counters + C_P_FIRST, 0, 4 * (C_P_LAST - C_P_FIRST + 1), st));
+        if (nbig && ntiles > c->cap.tile_cap) return fail(PSSGPU_ECUDA, "tile capacity exceeded");
+        // small classes: on the side streams (after everything queued on st
+        // so far), or serially on st in profile mode so that the per-class
+        // events time one class at a time
+        const bool fork = !c->profile && (cnt[L_TINY] || cnt[L_SMALLA] || cnt[L_SMALLB]);
+        if (fork) PSS_CUDA(cudaEventRecord(c->fork_ev, st));
+        bool joined[3] = {};
+        auto small_stream = [&](int q) -> cudaStream_t {
+            if (!fork) return st;
+            cudaStreamWaitEvent(c->side[q], c->fork_ev, 0);
+            joined[q] = true;
+            return c->side[q];
+        };
         if (cnt[L_TINY]) {
+            cudaStream_t s = small_stream(0);
             kt.begin(K_TINY);
             constexpr uint32_t per_block = TINY_WARPS * TINY_PER_WARP;
-            k_tiny<<<(cnt[L_TINY] + per_block - 1) / per_block, 32 * TINY_WARPS, 0, st>>>(
+            k_tiny<<<(cnt[L_TINY] + per_block - 1) / per_block, 32 * TINY_WARPS, 0, s>>>(
                 w, w.list[L_TINY][cur], cnt[L_TINY]);
             kt.end(K_TINY);
             c->kstat[K_TINY].launches += 1;
             stats.kernel_launches += 1;
         }
         if (cnt[L_SMALLA]) {
+            cudaStream_t s = small_stream(1);
             kt.begin(K_SMALLA);
-            K_BLOCK_A<<<cnt[L_SMALLA], SMALL_A_THREADS, sizeof(BlockSmem<SMALL_A>), st>>>(
+            K_BLOCK_A<<<cnt[L_SMALLA], SMALL_A_THREADS, sizeof(BlockSmem<SMALL_A>), s>>>(
                 w, w.list[L_SMALLA][cur]);
             kt.end(K_SMALLA);
             c->kstat[K_SMALLA].launches += 1;
             stats.kernel_launches += 1;
         }
         if (cnt[L_SMALLB]) {
+            cudaStream_t s = small_stream(2);
             kt.begin(K_SMALLB);
-            K_BLOCK_B<<<cnt[L_SMALLB], SMALL_THREADS, sizeof(BlockSmem<SMALL_MAX>), st>>>(
+            K_BLOCK_B<<<cnt[L_SMALLB], SMALL_THREADS, sizeof(BlockSmem<SMALL_MAX>), s>>>(
                 w, w.list[L_SMALLB][cur]);
             kt.end(K_SMALLB);
             c->kstat[K_SMALLB].launches += 1;
             stats.kernel_launches += 1;
         }
+        for (int q = 0; q < 3; ++q)
+            if (joined[q]) PSS_CUDA(cudaEventRecord(c->join_ev[q], c->side[q]));
         if (nbig) {
-            if (ntiles > c->cap.tile_cap) return fail(PSSGPU_ECUDA, "tile capacity exceeded");
             kt.begin(K_SAMPLE);
             k_tile_scan<<<1, 1024, 0, st>>>(w, nbig);
             k_sample<<<nbig, 1024, 0, st>>>(w);
@@ -364,6 +379,13 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
             kt.end(K_CLASSIFY);
             kt.begin(K_BSTART);
             k_bstart<<<nbig, 1024, 0, st>>>(w);
+            {
+                // chunks <= tiles, and <= one per CHUNK tiles plus one per segment
+                const uint32_t nchunk = std::min<uint32_t>(ntiles, ntiles / CHUNK + nbig);
+                k_chunk_sum<<<dim3(nchunk, (MAX_BKT + 255) / 256), 256, 0, st>>>(w, nbig);
+                k_chunk_scan<<<dim3(nbig, (MAX_BKT + 127) / 128), 128, 0, st>>>(w);
+                k_tile_offsets<<<dim3(nchunk, (MAX_BKT + 255) / 256), 256, 0, st>>>(w, nbig);
+            }
             kt.end(K_BSTART);
             kt.begin(K_SCATTER);
             k_scatter<<<ntiles, TILE_THREADS, sizeof(ScatterSmem), st>>>(w, nbig);
@@ -373,12 +395,14 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
             kt.end(K_CHILDREN);
             c->kstat[K_SAMPLE].launches += 2;
             c->kstat[K_CLASSIFY].launches += 1;
-            c->kstat[K_BSTART].launches += 1;
+            c->kstat[K_BSTART].launches += 4;
             c->kstat[K_SCATTER].launches += 1;
             c->kstat[K_CHILDREN].launches += 1;
-            stats.kernel_launches += 6;
+            stats.kernel_launches += 9;
             stats.passes += 1;
         }
+        for (int q = 0; q < 3; ++q)
+            if (joined[q]) PSS_CUDA(cudaStreamWaitEvent(st, c->join_ev[q], 0));
         PSS_CUDA(cudaGetLastError());
         PSS_CUDA(cudaMemcpyAsync(hc, w.counters, 4 * C_COUNT, cudaMemcpyDeviceToHost, st));
         PSS_CUDA(cudaStreamSynchronize(st));
@@ -387,14 +411,16 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
             // per-string algorithmic bytes of each kernel class: key gather
             // 4 id + 8 chars + 8 key write; classify 8 key read; scatter
             // 12 read + 12 write; base case 12 read + output
-            // (a jump string is charged like a gather: 4 id + 8 offset + 8 chars)
+            // (a string behind a common-prefix jump also reads 8 chars per
+            // shared chunk)
             const uint64_t big = hc[C_P_BIG], stale = hc[C_P_STALE], fin = hc[C_P_FINAL];
-            const uint64_t sc = hc[C_P_SCATTER], tie = hc[C_P_TIE];
-            stats.big_elements += big + tie;
-            c->kstat[K_SAMPLE].strings += big + tie;
-            c->kstat[K_CLASSIFY].strings += big + fin + tie;
+            const uint64_t jch = hc[C_P_JCHUNKS];
+            const uint64_t sc = hc[C_P_SCATTER];
+            stats.big_elements += big;
+            c->kstat[K_SAMPLE].strings += big;
+            c->kstat[K_CLASSIFY].strings += big + fin;
             c->kstat[K_CLASSIFY].alg_bytes +=
-                20 * stale + 8 * (big - stale) + (4 + out_bytes) * fin + 20 * tie;
+                20 * stale + 8 * (big - stale) + (4 + out_bytes) * fin + 8 * jch;
             c->kstat[K_SCATTER].strings += sc;
             c->kstat[K_SCATTER].alg_bytes += 24 * sc;
             const int sk[3] = {K_TINY, K_SMALLA, K_SMALLB};
@@ -460,6 +486,10 @@ static int ctx_create(int device, Ctx** out)
               cudaHostAlloc((void**)&c->host_counters, 4 * C_COUNT, cudaHostAllocDefault) ==
                   cudaSuccess;
     for (int k = 0; ok && k < 2 * K_NCLASS; ++k) ok = cudaEventCreate(&c->kev[k]) == cudaSuccess;
+    ok = ok && cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming) == cudaSuccess;
+    for (int q = 0; ok && q < 3; ++q)
+        ok = cudaStreamCreateWithFlags(&c->side[q], cudaStreamNonBlocking) == cudaSuccess &&
+             cudaEventCreateWithFlags(&c->join_ev[q], cudaEventDisableTiming) == cudaSuccess;
     if (!ok) {
         ctx_destroy(c);
         return fail(PSSGPU_ECUDA, "stream/event/pinned allocation failed");
@@ -480,6 +510,11 @@ static void ctx_destroy(Ctx* c)
     if (c->ev1) cudaEventDestroy(c->ev1);
     for (int k = 0; k < 2 * K_NCLASS; ++k)
         if (c->kev[k]) cudaEventDestroy(c->kev[k]);
+    if (c->fork_ev) cudaEventDestroy(c->fork_ev);
+    for (int q = 0; q < 3; ++q) {
+        if (c->join_ev[q]) cudaEventDestroy(c->join_ev[q]);
+        if (c->side[q]) cudaStreamDestroy(c->side[q]);
+    }
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }

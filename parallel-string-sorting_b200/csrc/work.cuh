@@ -8,13 +8,13 @@ namespace pssgpu {
 constexpr int TILE = 4096;          // strings per classify / scatter tile
 constexpr int TILE_THREADS = 256;   // 16 strings per thread
 constexpr int MAX_TREE_BITS = 10;   // 1023 splitters, 2047 buckets (pS5's DefaultTreebits)
-constexpr int MAX_BKT = 2048;       // bucket slots per big segment
+constexpr int MAX_BKT = 2056;       // bucket slots per big segment: 2047 + the two prefix buckets
+constexpr int JMAX_CHUNKS = 32;     // common-prefix jump of one pass: at most 32 8-byte chunks
 constexpr int SMALL_MAX = 2048;     // largest segment the block sorter takes
 constexpr int SMALL_THREADS = 256;
 constexpr int WARP_GROUP_MAX = 32;  // groups this small are finished by one warp
 constexpr int FINAL_INLINE = 64;    // equal-string buckets this small are copied inline
-constexpr uint32_t SPIN_CAP = 1u << 20;  // look-back wait limit (polls, ~0.1 s)
-constexpr uint8_t TREE_TIE = 0xFF;  // tree_bits marker: all samples equal, jump instead
+constexpr int CHUNK = 32;           // tiles per chunk of the destination scan
 
 // segment list classes
 enum : int { L_BIG = 0, L_TINY = 1, L_SMALLA = 2, L_SMALLB = 3, L_NCLASS = 4 };
@@ -25,7 +25,7 @@ enum : int {
     C_NTILES = 4,     // + C_PAR * parity: tiles of the big list
     C_NSTR = 4,       // + C_PAR * parity + class (1..3): strings in the small lists
     C_NBND = 16,      // boundary list length
-    C_TICKET = 17,    // scatter tile ticket
+    C_SPARE = 17,
     C_ERR = 18,       // error bits
     C_SMALLSEGS = 19, // statistics: segments finished by the block sorter
     // per-pass statistics, reset every pass
@@ -33,9 +33,10 @@ enum : int {
     C_P_STALE = 21,   // of those, strings whose key was gathered this pass
     C_P_FINAL = 22,   // strings copied out of big all-equal segments
     C_P_SCATTER = 23, // strings moved by the scatter
-    C_P_TIE = 24,     // strings of segments that took the common-prefix jump
+    C_P_TIE = 24,     // of the big strings, those classified behind a common-prefix jump
+    C_P_JCHUNKS = 25, // their prefix chunks: sum over jump segments of size * jump / 8
     C_P_FIRST = C_P_BIG,
-    C_P_LAST = C_P_TIE,
+    C_P_LAST = C_P_JCHUNKS,
     C_COUNT = 32
 };
 
@@ -67,22 +68,39 @@ struct Work {
     uint32_t cap[L_NCLASS];
     // per big segment of the current pass
     uint32_t* tile_start;  // [cap[L_BIG] + 1]
-    uint8_t* tree_bits;    // [cap[L_BIG]]; 0 = all-equal copy, TREE_TIE = jump
+    uint8_t* tree_bits;    // [cap[L_BIG]]; 0 = all-equal copy
     uint64_t* tree;        // [cap[L_BIG]][1024], level order, index 1..k
     uint64_t* spl;         // [cap[L_BIG]][1024], sorted splitters
     uint32_t* bcount;      // [cap[L_BIG]][MAX_BKT]
     uint32_t* bstart;      // [cap[L_BIG]][MAX_BKT]
     uint8_t* bflags;       // [cap[L_BIG]]: 1 = whole segment in one bucket
-    uint32_t* jump_min;    // [cap[L_BIG]]: min common prefix beyond depth (jump)
-    uint32_t* jump_diff;   // [cap[L_BIG]]: some string differs from the base
-    uint64_t* status;      // [tile_cap][MAX_BKT] decoupled look-back words
+    // Common-prefix jump: when every sample shares more chars beyond the
+    // segment depth, jump[s] = that many chars (a multiple of 8) and jpre holds
+    // them as keys; the tree then splits at depth + jump, and strings that
+    // leave the prefix earlier go to a first ('<' prefix) or last ('>' prefix)
+    // bucket.
+    uint32_t* jump;        // [cap[L_BIG]]
+    uint64_t* jpre;        // [cap[L_BIG]][JMAX_CHUNKS]
+    // Scatter destinations, pS5's count / count_finished over parts (hpp:1414-1460)
+    // with tiles as parts: per tile and bucket the count, then (after the
+    // bucket-major, tile-minor exclusive scan) the tile's first destination.
+    // The scan runs in chunks of CHUNK tiles.
+    uint32_t* chunk_start;  // [cap[L_BIG] + 1]: first chunk of each big segment
+    uint32_t* tcount;       // [tile_cap][MAX_BKT]
+    uint32_t* ccount;       // [tile_cap][MAX_BKT]: chunk sums, then chunk bases
     uint32_t tile_cap;
-    uint32_t epoch;        // look-back epoch of this pass (1..65535)
     int cur;               // parity of the lists read in this pass
     // splitter-tree levels for a big segment of 2^k..2^(k+1)-1 strings
     // (0: the default rule), set from a tuning table
     uint8_t tree_bits_by_size[33];
 };
+
+// buckets of a classified big segment: the tree's 2^(L+1) - 1, plus the two
+// prefix buckets of a jump segment
+__device__ __forceinline__ uint32_t seg_buckets(const Work& w, int s)
+{
+    return (2u << w.tree_bits[s]) - 1 + (w.jump[s] ? 2u : 0u);
+}
 
 __device__ __forceinline__ uint64_t h_make(const Work& w, uint32_t id, uint64_t off)
 {

@@ -76,12 +76,15 @@ def _rand_tails(n, k, seed):
 
 
 @pytest.mark.parametrize("case", ["all_equal_big", "long_prefix_big", "few_differ_early",
-                                  "one_differs_first_char"])
+                                  "one_differs_first_char", "prefix_outliers",
+                                  "outliers_past_one_jump"])
 def test_common_prefix_jump(pkg, orc, ctx, case):
-    """Big segments whose samples are all equal take the common-prefix jump:
-    all strings equal (finished by the jump), a long shared prefix, a few
-    strings leaving the prefix early, one string differing at char 0 (the
-    jump makes no progress and the segment is classified instead)."""
+    """Big segments whose samples all share a prefix jump over it inside the
+    pass: all strings equal, a long shared prefix (several jumps of at most
+    256 chars), a few strings leaving the prefix early, one string differing
+    at char 0, rare strings below and above the prefix (shorter ones, smaller
+    and larger chars: the two prefix buckets, at the segment depth), and
+    outliers that leave a 600-char prefix beyond the first jump."""
     if case == "all_equal_big":
         strings = [b"q" * 500] * 100000
     elif case == "long_prefix_big":
@@ -89,6 +92,13 @@ def test_common_prefix_jump(pkg, orc, ctx, case):
     elif case == "few_differ_early":
         strings = [b"r" * 300 + t for t in _rand_tails(30000, 2, 2)]
         strings += [b"r" * 5 + b"a" + t for t in _rand_tails(10, 4, 3)]
+    elif case == "prefix_outliers":
+        strings = [b"m" * 60 + t for t in _rand_tails(100000, 3, 4)]
+        strings += [b"m" * 20, b"m" * 33 + b"a", b"m" * 59 + b"z", b"m" * 45 + b"zz",
+                    b"m" * 8 + b"\x01", b"m" * 60, b"m" * 61 + b"\xff"]
+    elif case == "outliers_past_one_jump":
+        strings = [b"k" * 600 + t for t in _rand_tails(60000, 3, 5)]
+        strings += [b"k" * 300 + b"a", b"k" * 270 + b"z", b"k" * 100, b"k" * 700, b"k" * 599]
     else:
         strings = [b"s" * 40] * 20000 + [b"a"]
     chars, offs = pkg.pack_strings(strings)

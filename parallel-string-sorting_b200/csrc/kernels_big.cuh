@@ -76,24 +76,6 @@ __global__ void k_tile_scan(Work w, uint32_t nbig)
     }
 }
 
-// In-place ascending bitonic sort of S (a power of two) keys in shared
-// memory by the whole block; synchronises before returning.
-__device__ __forceinline__ void bitonic_sort_block(uint64_t* a, uint32_t S)
-{
-    for (uint32_t kk = 2; kk <= S; kk <<= 1) {
-        for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
-            for (uint32_t i = threadIdx.x; i < S / 2; i += blockDim.x) {
-                const uint32_t x0 = 2 * i - (i & (j - 1));
-                const uint32_t x1 = x0 + j;
-                const bool asc = (x0 & kk) == 0;
-                const uint64_t x = a[x0], y = a[x1];
-                if ((x > y) == asc) { a[x0] = y; a[x1] = x; }
-            }
-            __syncthreads();
-        }
-    }
-}
-
 // One block of 1024 threads per big segment.
 __global__ void __launch_bounds__(1024) k_sample(Work w)
 {

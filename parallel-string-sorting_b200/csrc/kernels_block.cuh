@@ -18,18 +18,27 @@ namespace pssgpu {
 
 constexpr int BLK_MAX_BITS = 8;  // at most 255 splitters, 511 buckets per step
 
+// splitter-tree levels a block sorter of MAXN strings can use: about 8
+// strings per '<' bucket (the L rule in k_block), at most BLK_MAX_BITS
+__host__ __device__ constexpr int blk_bits(int maxn)
+{
+    int lg = 0;
+    while ((2 << lg) <= maxn) ++lg;
+    return lg - 3 < BLK_MAX_BITS ? lg - 3 : BLK_MAX_BITS;
+}
+
 template <int MAXN>
 struct BlockSmem {
+    static constexpr int NB = 2 << blk_bits(MAXN);  // bucket slots
     uint64_t key[MAXN];
     uint64_t hnd[MAXN];
-    uint64_t tmp[MAXN];                  // scatter staging
     uint16_t dst[MAXN];                  // bucket, then destination, per element
-    uint32_t cnt[2 << BLK_MAX_BITS];     // bucket counts, then bucket starts
-    uint32_t cur[2 << BLK_MAX_BITS];     // scatter cursors
-    uint64_t bmin[2 << BLK_MAX_BITS];
-    uint64_t bmax[2 << BLK_MAX_BITS];
-    uint64_t tree[1 << BLK_MAX_BITS];    // level order, index 1..k
-    uint64_t samp[2 << BLK_MAX_BITS];
+    uint32_t cnt[NB];                    // bucket counts, then bucket starts
+    uint32_t cur[NB];                    // scatter cursors
+    uint64_t bmin[NB];
+    uint64_t bmax[NB];
+    uint64_t tree[NB / 2];               // level order, index 1..k
+    uint64_t samp[NB];
     // groups larger than a warp, processed one at a time by the block
     uint16_t g_start[MAXN / 32];
     uint16_t g_len[MAXN / 32];
@@ -71,6 +80,7 @@ __global__ void __launch_bounds__(THREADS) k_block(Work w, const Seg* list)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     BlockSmem<MAXN>& sm = *reinterpret_cast<BlockSmem<MAXN>*>(smem_raw);
+    __shared__ uint32_t wscratch[THREADS / 32][32];
     const Seg sg = list[blockIdx.x];
     const uint32_t m = sg.size, begin = sg.begin;
     const int buf = sg.meta & META_BUF;
@@ -114,28 +124,33 @@ __global__ void __launch_bounds__(THREADS) k_block(Work w, const Seg* list)
         }
         // sample: 2^(L+1) keys at pseudo-random positions of the group
         const int lg = 31 - __clz((int)c);
-        const uint32_t L = (uint32_t)min(BLK_MAX_BITS, max(1, lg - 3));
+        const uint32_t L = (uint32_t)min(blk_bits(MAXN), max(1, lg - 3));
         const uint32_t k = (1u << L) - 1;
         const uint32_t S = 2u << L;
         __syncthreads();
         for (uint32_t i = threadIdx.x; i < S; i += THREADS) {
             const uint64_t h = mix64(((uint64_t)(begin + s) << 24) ^ ((uint64_t)d << 4) ^ i);
-            sm.samp[i] = sm.key[s + (uint32_t)(h % c)];
+            sm.samp[i] = sm.key[s + (uint32_t)(((h >> 32) * c) >> 32)];
         }
         __syncthreads();
-        // rank sort of the samples into tmp (ties by index): one barrier
-        // instead of a bitonic network's log^2 barriers
-        for (uint32_t i = threadIdx.x; i < S; i += THREADS) {
-            const uint64_t x = sm.samp[i];
+        if (S <= (uint32_t)THREADS) {
+            // rank sort in place (ties by index): two barriers
+            uint64_t x = 0;
             uint32_t r = 0;
-            for (uint32_t j = 0; j < S; ++j) {
-                const uint64_t y = sm.samp[j];
-                r += (y < x || (y == x && j < i)) ? 1u : 0u;
+            if (threadIdx.x < S) {
+                x = sm.samp[threadIdx.x];
+                for (uint32_t j = 0; j < S; ++j) {
+                    const uint64_t y = sm.samp[j];
+                    r += (y < x || (y == x && j < threadIdx.x)) ? 1u : 0u;
+                }
             }
-            sm.tmp[r] = x;
+            __syncthreads();
+            if (threadIdx.x < S) sm.samp[r] = x;
+            __syncthreads();
+        } else {
+            bitonic_sort_block(sm.samp, S);
         }
-        __syncthreads();
-        const uint64_t* sorted = sm.tmp;
+        const uint64_t* sorted = sm.samp;
         if (sorted[0] == sorted[S - 1] && !key_terminated(sorted[0])) {
             // likely one tied group: measure its common prefix in chunks
             if (threadIdx.x == 0) sm.jump = 0xFFFFFFFFu;
@@ -192,13 +207,31 @@ __global__ void __launch_bounds__(THREADS) k_block(Work w, const Seg* list)
         for (uint32_t i = threadIdx.x; i < c; i += THREADS)
             sm.dst[s + i] = (uint16_t)atomicAdd(&sm.cur[sm.dst[s + i]], 1u);
         __syncthreads();
-        for (uint32_t i = threadIdx.x; i < c; i += THREADS) sm.tmp[s + sm.dst[s + i]] = sm.key[s + i];
-        __syncthreads();
-        for (uint32_t i = threadIdx.x; i < c; i += THREADS) sm.key[s + i] = sm.tmp[s + i];
-        __syncthreads();
-        for (uint32_t i = threadIdx.x; i < c; i += THREADS) sm.tmp[s + sm.dst[s + i]] = sm.hnd[s + i];
-        __syncthreads();
-        for (uint32_t i = threadIdx.x; i < c; i += THREADS) sm.hnd[s + i] = sm.tmp[s + i];
+        {
+            // permute keys, then handles, through registers
+            constexpr int PER = MAXN / THREADS;
+            uint64_t v[PER];
+#pragma unroll
+            for (int j = 0; j < PER; ++j) {
+                const uint32_t i = threadIdx.x + j * THREADS;
+                if (i < c) v[j] = sm.key[s + i];
+            }
+            __syncthreads();
+#pragma unroll
+            for (int j = 0; j < PER; ++j) {
+                const uint32_t i = threadIdx.x + j * THREADS;
+                if (i < c) {
+                    sm.key[s + sm.dst[s + i]] = v[j];
+                    v[j] = sm.hnd[s + i];
+                }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int j = 0; j < PER; ++j) {
+                const uint32_t i = threadIdx.x + j * THREADS;
+                if (i < c) sm.hnd[s + sm.dst[s + i]] = v[j];
+            }
+        }
         // children and boundary LCPs; cnt now holds bucket starts
         for (uint32_t b = threadIdx.x; b < B; b += THREADS) {
             const uint32_t st = sm.cnt[b];
@@ -252,7 +285,8 @@ __global__ void __launch_bounds__(THREADS) k_block(Work w, const Seg* list)
         const bool real = mygrp < 32;
         const uint64_t h = real ? sm.hnd[start] : ~0ull;
         const uint64_t k0 = (real && valid) ? sm.key[start] : 0ull;
-        const uint64_t r = warp_window(w, h, mygrp, dep, begin + start, real && valid, k0);
+        const uint64_t r = warp_window(w, h, mygrp, dep, begin + start, real && valid, k0,
+                                       wscratch[warp]);
         if (real) sm.hnd[start] = r;
     });
     __syncthreads();

@@ -45,10 +45,11 @@ __device__ __forceinline__ uint32_t chunks_equal(const Work& w, uint64_t base, u
 // mygrp = lane index where the slot's group starts (32 for an unused lane),
 // mydep = chars the group shares, mypos = output position of the slot, and
 // the key at mydep when has_key. Returns the handle that sorts into this
-// lane's slot; LCPs inside groups are written to lcp[mypos].
+// lane's slot; LCPs inside groups are written to lcp[mypos]. scratch is 32
+// words of shared memory private to the warp.
 __device__ __forceinline__ uint64_t warp_window(const Work& w, uint64_t myh, uint32_t mygrp,
                                                 uint32_t mydep, uint32_t mypos, bool has_key,
-                                                uint64_t key0)
+                                                uint64_t key0, uint32_t* scratch)
 {
     const uint32_t lane = threadIdx.x & 31;
     uint32_t mystate = mygrp < 32 ? 0u : 1u;  // 0 active, 1 done
@@ -88,32 +89,55 @@ __device__ __forceinline__ uint64_t warp_window(const Work& w, uint64_t myh, uin
         }
         if (mystate == 0) mykey = (first && has_key) ? key0 : h_key(w, myh, mydep);
         first = false;
-        // sort (group, key, source lane) with a 32-lane bitonic network on
-        // three shuffled words, then fetch the rest from the source lane
-        uint32_t tag = (mygrp << 5) | lane;
-        uint64_t k = mykey;
+        // Groups are contiguous lane ranges; a group starts at the lane whose
+        // mygrp is itself, and unused lanes end the window. Sort the active
+        // groups by (key, lane): by rank inside the group when the largest
+        // active group is small, else with a 32-lane bitonic network.
+        const uint32_t GB = __ballot_sync(0xffffffffu, mygrp == lane || mygrp >= 32);
+        const uint32_t above = lane == 31 ? 0u : (GB & (0xFFFFFFFFu << (lane + 1)));
+        const uint32_t gend = above ? (uint32_t)(__ffs(above) - 1) : 32u;
+        const uint32_t glen = mystate == 0 ? gend - mygrp : 0u;
+        const uint32_t M = __reduce_max_sync(0xffffffffu, glen);
+        if (M > 16) {
+            uint32_t tag = (mygrp << 5) | lane;
+            uint64_t k = mykey;
 #pragma unroll
-        for (uint32_t kk = 2; kk <= 32; kk <<= 1) {
+            for (uint32_t kk = 2; kk <= 32; kk <<= 1) {
 #pragma unroll
-            for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
-                const uint32_t ot = __shfl_xor_sync(0xffffffffu, tag, j);
-                const uint64_t ok = __shfl_xor_sync(0xffffffffu, k, j);
-                const bool lower = (lane & j) == 0;
-                const bool asc = (lane & kk) == 0;
-                bool other_less;
-                if ((ot >> 5) != (tag >> 5)) other_less = (ot >> 5) < (tag >> 5);
-                else if (ok != k) other_less = ok < k;
-                else other_less = (ot & 31u) < (tag & 31u);
-                // the lower lane of an ascending pair keeps the smaller
-                if ((lower == asc) ? other_less : !other_less) { tag = ot; k = ok; }
+                for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
+                    const uint32_t ot = __shfl_xor_sync(0xffffffffu, tag, j);
+                    const uint64_t ok = __shfl_xor_sync(0xffffffffu, k, j);
+                    const bool lower = (lane & j) == 0;
+                    const bool asc = (lane & kk) == 0;
+                    bool other_less;
+                    if ((ot >> 5) != (tag >> 5)) other_less = (ot >> 5) < (tag >> 5);
+                    else if (ok != k) other_less = ok < k;
+                    else other_less = (ot & 31u) < (tag & 31u);
+                    // the lower lane of an ascending pair keeps the smaller
+                    if ((lower == asc) ? other_less : !other_less) { tag = ot; k = ok; }
+                }
             }
+            const uint32_t src = tag & 31u;
+            myh = __shfl_sync(0xffffffffu, myh, src);
+            mydep = __shfl_sync(0xffffffffu, mydep, src);
+            mystate = __shfl_sync(0xffffffffu, mystate, src);
+            mygrp = tag >> 5;
+            mykey = k;
+        } else if (M > 1) {
+            uint32_t rank = 0;
+            for (uint32_t j = 0; j < M; ++j) {
+                const uint32_t src = (mygrp + j) & 31u;
+                const uint64_t kj = __shfl_sync(0xffffffffu, mykey, src);
+                if (j < glen && (kj < mykey || (kj == mykey && mygrp + j < lane))) ++rank;
+            }
+            scratch[mystate == 0 ? mygrp + rank : lane] = lane;
+            __syncwarp();
+            const uint32_t src = scratch[lane];
+            __syncwarp();
+            myh = __shfl_sync(0xffffffffu, myh, src);
+            mydep = __shfl_sync(0xffffffffu, mydep, src);
+            mykey = __shfl_sync(0xffffffffu, mykey, src);
         }
-        const uint32_t src = tag & 31u;
-        myh = __shfl_sync(0xffffffffu, myh, src);
-        mydep = __shfl_sync(0xffffffffu, mydep, src);
-        mystate = __shfl_sync(0xffffffffu, mystate, src);
-        mygrp = tag >> 5;
-        mykey = k;
         const uint32_t pg = __shfl_up_sync(0xffffffffu, mygrp, 1);
         const uint64_t pk = __shfl_up_sync(0xffffffffu, mykey, 1);
         const bool ns = lane == 0 || mygrp != pg || mykey != pk;
@@ -162,6 +186,7 @@ constexpr int TINY_WARPS = 8;
 constexpr int TINY_PER_WARP = 8;
 __global__ void __launch_bounds__(32 * TINY_WARPS) k_tiny(Work w, const Seg* list, uint32_t count)
 {
+    __shared__ uint32_t scratch[TINY_WARPS][32];
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t g0 = (blockIdx.x * TINY_WARPS + (threadIdx.x >> 5)) * TINY_PER_WARP;
     if (g0 >= count) return;  // whole warp
@@ -182,7 +207,7 @@ __global__ void __launch_bounds__(32 * TINY_WARPS) k_tiny(Work w, const Seg* lis
         const uint64_t h = real ? w.hnd[buf][pos] : ~0ull;
         const bool hk = real && (sg.meta & META_VALID);
         const uint64_t k0 = hk ? w.keys[buf][pos] : 0ull;
-        const uint64_t r = warp_window(w, h, mygrp, sg.depth, pos, hk, k0);
+        const uint64_t r = warp_window(w, h, mygrp, sg.depth, pos, hk, k0, scratch[threadIdx.x >> 5]);
         if (real) w.perm[pos] = h_id(w, r);
     });
 }

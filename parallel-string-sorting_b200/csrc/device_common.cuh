@@ -61,6 +61,39 @@ __device__ __forceinline__ uint64_t load_key(const uint8_t* __restrict__ chars,
     return bswap64(raw);
 }
 
+// Keys of the cnt (<= NB) consecutive 8-char chunks at p, p + 8, ... into
+// out[0, cnt): cnt + 1 aligned word loads instead of two per chunk. Same
+// values as load_key at each position (chars at or beyond nchars read as
+// NUL); out[cnt, NB) are left 0.
+template <int NB>
+__device__ __forceinline__ void load_chunks(const uint8_t* __restrict__ chars, uint64_t nchars,
+                                            uint64_t p, uint32_t cnt, uint64_t* out)
+{
+    const uint64_t a = p & ~7ull;
+    const unsigned sh = (unsigned)(p & 7) * 8u;
+    uint64_t wd[NB + 1];
+#pragma unroll
+    for (int i = 0; i <= NB; ++i) {
+        const uint64_t ai = a + 8ull * i;
+        uint64_t v = 0;
+        if ((uint32_t)i <= cnt && ai < nchars) {
+            v = __ldg(reinterpret_cast<const uint64_t*>(chars + ai));
+            if (ai + 8 > nchars) v &= ~0ull >> (64u - 8u * (unsigned)(nchars - ai));
+        }
+        wd[i] = v;
+    }
+#pragma unroll
+    for (int i = 0; i < NB; ++i) {
+        uint64_t raw = sh ? ((wd[i] >> sh) | (wd[i + 1] << (64u - sh))) : wd[i];
+        const uint64_t z = (raw - 0x0101010101010101ull) & ~raw & 0x8080808080808080ull;
+        if (z) {
+            const unsigned nb = (unsigned)(__ffsll((long long)z) - 1) >> 3;
+            raw = nb ? (raw & (~0ull >> (64u - 8u * nb))) : 0ull;
+        }
+        out[i] = (uint32_t)i < cnt ? bswap64(raw) : 0ull;
+    }
+}
+
 __device__ __forceinline__ uint64_t gather_key(const uint8_t* __restrict__ chars,
                                                uint64_t nchars,
                                                const uint64_t* __restrict__ offs,

@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(1024) k_sample(Work w)
 // difference puts it into the first or last bucket, else its key after the
 // prefix goes through the tree (bucket + 1).
 // Tiles of finished (all-equal) segments copy ids and LCPs to the output.
-__global__ void __launch_bounds__(TILE_THREADS) k_classify(Work w, uint32_t nbig)
+__global__ void __launch_bounds__(TILE_THREADS, 6) k_classify(Work w, uint32_t nbig)
 {
     __shared__ uint64_t tree[1024];
     __shared__ uint64_t jp[JMAX_CHUNKS];
@@ -220,13 +220,12 @@ __global__ void __launch_bounds__(TILE_THREADS) k_classify(Work w, uint32_t nbig
             keys[p] = key;
         } else {
             const uint64_t o = h_off(w, hs[p]) + sg.depth;
-            for (uint32_t c0 = 0; c0 <= nc && !side; c0 += 4) {
-                uint64_t kk[4];
+            constexpr uint32_t NB = 7;  // chunks per batch: a 6-chunk prefix and its key
+            for (uint32_t c0 = 0; c0 <= nc && !side; c0 += NB) {
+                uint64_t kk[NB];
+                load_chunks<NB>(w.chars, w.nchars, o + 8ull * c0, min(NB, nc + 1 - c0), kk);
 #pragma unroll
-                for (uint32_t q = 0; q < 4; ++q)
-                    kk[q] = c0 + q <= nc ? load_key(w.chars, w.nchars, o + 8ull * (c0 + q)) : 0ull;
-#pragma unroll
-                for (uint32_t q = 0; q < 4; ++q) {
+                for (uint32_t q = 0; q < NB; ++q) {
                     const uint32_t c = c0 + q;
                     if (side || c > nc) continue;
                     if (c == nc) key = kk[q];
@@ -389,8 +388,8 @@ __global__ void __launch_bounds__(256) k_tile_offsets(Work w, uint32_t nbig)
 struct ScatterSmem {
     uint64_t stage[TILE];      // the tile's keys in bucket order, then its handles
     uint16_t sbkt[TILE];       // bucket of each staged slot
-    uint32_t lcount[MAX_BKT];  // per-bucket count in the tile, then its start
-    uint32_t gdelta[MAX_BKT];  // per bucket: global position - tile slot
+    uint32_t lcount[MAX_BKT];  // per bucket: count in the tile, then its first slot,
+                               // then global position - slot
     uint32_t tmp[32];
 };
 
@@ -400,6 +399,7 @@ struct ScatterSmem {
 __global__ void __launch_bounds__(TILE_THREADS) k_scatter(Work w, uint32_t nbig)
 {
     constexpr int PER = TILE / TILE_THREADS;
+    constexpr int NBT = (MAX_BKT + TILE_THREADS - 1) / TILE_THREADS;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ScatterSmem& sm = *reinterpret_cast<ScatterSmem*>(smem_raw);
     const uint32_t t = blockIdx.x;
@@ -412,6 +412,14 @@ __global__ void __launch_bounds__(TILE_THREADS) k_scatter(Work w, uint32_t nbig)
     const uint32_t cnt = hi - lo;
     const uint32_t B = seg_buckets(w, s);
     const int buf = sg.meta & META_BUF;
+    // this tile's first destination per bucket, loaded early
+    const uint32_t* dst = w.tcount + (size_t)t * MAX_BKT;
+    uint32_t first[NBT];
+#pragma unroll
+    for (int i = 0; i < NBT; ++i) {
+        const uint32_t b = threadIdx.x + i * TILE_THREADS;
+        first[i] = b < B ? dst[b] : 0u;
+    }
     for (uint32_t b = threadIdx.x; b < B; b += TILE_THREADS) sm.lcount[b] = 0;
     __syncthreads();
     // rank of every string inside its bucket in this tile: (bucket << 16) | rank
@@ -426,23 +434,29 @@ __global__ void __launch_bounds__(TILE_THREADS) k_scatter(Work w, uint32_t nbig)
         }
     }
     __syncthreads();
-    block_scan_array<TILE_THREADS>(sm.lcount, (int)B, sm.tmp);  // counts -> tile starts
-    const uint32_t* dst = w.tcount + (size_t)t * MAX_BKT;
-    for (uint32_t b = threadIdx.x; b < B; b += TILE_THREADS) sm.gdelta[b] = dst[b] - sm.lcount[b];
-    // stage keys in bucket order and write bucket runs contiguously; then handles
+    block_scan_array<TILE_THREADS>(sm.lcount, (int)B, sm.tmp);  // counts -> first slots
+    // stage keys in bucket order; pk becomes (bucket << 16) | slot
     const uint64_t* ikeys = w.keys[buf];
 #pragma unroll
     for (int j = 0; j < PER; ++j) {
         if (pk[j] == 0xFFFFFFFFu) continue;
         const uint32_t b = pk[j] >> 16;
         const uint32_t slot = sm.lcount[b] + (pk[j] & 0xFFFFu);
+        pk[j] = (b << 16) | slot;
         sm.stage[slot] = ikeys[lo + threadIdx.x + j * TILE_THREADS];
         sm.sbkt[slot] = (uint16_t)b;
     }
     __syncthreads();
+#pragma unroll
+    for (int i = 0; i < NBT; ++i) {
+        const uint32_t b = threadIdx.x + i * TILE_THREADS;
+        if (b < B) sm.lcount[b] = first[i] - sm.lcount[b];
+    }
+    __syncthreads();
+    // write bucket runs contiguously: keys, then handles
     uint64_t* okeys = w.keys[buf ^ 1];
     for (uint32_t slot = threadIdx.x; slot < cnt; slot += TILE_THREADS) {
-        const uint32_t dest = slot + sm.gdelta[sm.sbkt[slot]];
+        const uint32_t dest = slot + sm.lcount[sm.sbkt[slot]];
         if (dest - sg.begin >= sg.size) {  // counts and destinations disagree
             set_error(w.counters + C_ERR, ERR_INTERNAL);
             continue;
@@ -454,13 +468,12 @@ __global__ void __launch_bounds__(TILE_THREADS) k_scatter(Work w, uint32_t nbig)
 #pragma unroll
     for (int j = 0; j < PER; ++j) {
         if (pk[j] == 0xFFFFFFFFu) continue;
-        const uint32_t slot = sm.lcount[pk[j] >> 16] + (pk[j] & 0xFFFFu);
-        sm.stage[slot] = ihs[lo + threadIdx.x + j * TILE_THREADS];
+        sm.stage[pk[j] & 0xFFFFu] = ihs[lo + threadIdx.x + j * TILE_THREADS];
     }
     __syncthreads();
     uint64_t* ohs = w.hnd[buf ^ 1];
     for (uint32_t slot = threadIdx.x; slot < cnt; slot += TILE_THREADS) {
-        const uint32_t dest = slot + sm.gdelta[sm.sbkt[slot]];
+        const uint32_t dest = slot + sm.lcount[sm.sbkt[slot]];
         if (dest - sg.begin >= sg.size) continue;
         ohs[dest] = sm.stage[slot];
     }

@@ -197,8 +197,10 @@ __global__ void __launch_bounds__(THREADS) k_block(Work w, const Seg* list)
             const uint32_t b = 2 * r + ((r < k && cand == key) ? 1u : 0u);
             sm.dst[s + i] = (uint16_t)b;
             atomicAdd(&sm.cnt[b], 1u);
-            atomicMin((unsigned long long*)&sm.bmin[b], (unsigned long long)key);
-            atomicMax((unsigned long long*)&sm.bmax[b], (unsigned long long)key);
+            if (w.lcp) {  // bucket key ranges, for the LCPs at bucket boundaries
+                atomicMin((unsigned long long*)&sm.bmin[b], (unsigned long long)key);
+                atomicMax((unsigned long long*)&sm.bmax[b], (unsigned long long)key);
+            }
         }
         __syncthreads();
         block_scan_array<THREADS>(sm.cnt, (int)B, sm.tmp32);  // counts -> starts
@@ -245,7 +247,7 @@ __global__ void __launch_bounds__(THREADS) k_block(Work w, const Seg* list)
             }
             if (cb == 1) continue;
             if (b & 1) {
-                const uint64_t key = sm.bmin[b];
+                const uint64_t key = sorted[b];  // the splitter: sorted sample 2r + 1
                 if (key_terminated(key)) {
                     if (w.lcp) {
                         const uint32_t v = d + lcp_key_depth(key);

@@ -6,10 +6,10 @@
 //                src/sequential/bingmann-sample_sort_tree_builder.hpp:189-288)
 //   k_classify   key gather + ClassifyTreeSimple::find_bkt + CountJob
 //                (src/sequential/bingmann-sample_sortBTC.hpp:45-72, hpp:1414-1435)
-//   k_bstart     count_finished: bucket prefix sums (hpp:1437-1460)
-//   k_chunk_sum, k_chunk_scan, k_tile_offsets
-//                count_finished over (tile, bucket) counts: every tile's first
+//   k_bstart     count_finished: bucket prefix sums and every tile's first
 //                destination per bucket (hpp:1437-1460)
+//   k_chunk_sum, k_chunk_scan, k_tile_offsets
+//                the same for segments of more than CHUNK tiles, in chunks
 //   k_scatter    distribute: shared-memory staged scatter (hpp:1464-1490)
 //   k_children   distribute_finished: next segments, finished buckets, split
 //                boundaries for the LCP array (hpp:1492-1584, 311-396)
@@ -267,8 +267,11 @@ __device__ __forceinline__ bool classified(uint8_t L)
     return L != 0;
 }
 
-// Bucket starts (exclusive prefix over buckets) and the one-bucket test.
-__global__ void __launch_bounds__(1024) k_bstart(Work w)
+// Bucket starts (exclusive prefix over buckets) and the one-bucket test. For
+// a segment of at most CHUNK tiles also every tile's first destination per
+// bucket (count_finished over (tile, bucket), hpp:1437-1460); longer
+// segments take the chunked scan below.
+__global__ void __launch_bounds__(256) k_bstart(Work w)
 {
     __shared__ uint32_t a[MAX_BKT];
     __shared__ uint32_t tmp[32];
@@ -281,107 +284,121 @@ __global__ void __launch_bounds__(1024) k_bstart(Work w)
     const uint32_t* bc = w.bcount + (size_t)s * MAX_BKT;
     if (threadIdx.x == 0) one = 0;
     __syncthreads();
-    for (uint32_t b = threadIdx.x; b < MAX_BKT; b += 1024) {
-        const uint32_t c = b < B ? bc[b] : 0u;
+    for (uint32_t b = threadIdx.x; b < B; b += 256) {
+        const uint32_t c = bc[b];
         a[b] = c;
         if (c == sg.size) one = 1;
     }
     __syncthreads();
-    block_scan_array<1024>(a, MAX_BKT, tmp);
+    block_scan_array<256>(a, (int)B, tmp);
     uint32_t* bs = w.bstart + (size_t)s * MAX_BKT;
-    for (uint32_t b = threadIdx.x; b < MAX_BKT; b += 1024) bs[b] = a[b];
+    for (uint32_t b = threadIdx.x; b < B; b += 256) bs[b] = a[b];
     if (threadIdx.x == 0) {
         w.bflags[s] = (uint8_t)one;
         if (!one) atomicAdd(w.counters + C_P_SCATTER, sg.size);
     }
+    const uint32_t t0 = w.tile_start[s], nt = w.tile_start[s + 1] - t0;
+    if (one || nt > (uint32_t)CHUNK) return;
+    for (uint32_t b = threadIdx.x; b < B; b += 256) {
+        uint32_t run = sg.begin + a[b];
+        uint32_t* col = w.tcount + (size_t)t0 * MAX_BKT + b;
+        constexpr uint32_t U = 8;  // loads in flight per thread
+        for (uint32_t j = 0; j < nt; j += U) {
+            uint32_t v[U];
+#pragma unroll
+            for (uint32_t q = 0; q < U; ++q) v[q] = j + q < nt ? col[(size_t)(j + q) * MAX_BKT] : 0u;
+#pragma unroll
+            for (uint32_t q = 0; q < U; ++q) {
+                if (j + q < nt) col[(size_t)(j + q) * MAX_BKT] = run;
+                run += v[q];
+            }
+        }
+    }
 }
 
-// The chunk of a scan kernel's block: segment s, tiles [t0, t1). False when
-// the block has no chunk or the segment is not scattered.
-__device__ __forceinline__ bool chunk_tiles(const Work& w, uint32_t nbig, uint32_t c, int* s,
-                                            uint32_t* t0, uint32_t* t1)
+// Segments of more than CHUNK tiles (rare: over CHUNK * TILE strings) scan
+// their (tile, bucket) counts in chunks of CHUNK tiles: chunk sums, their
+// scan per bucket, then the tiles inside each chunk. The kernels loop over
+// chunks / segments with a fixed grid and skip the short segments.
+__device__ __forceinline__ bool multi_chunk(const Work& w, int s)
 {
-    if (c >= w.chunk_start[nbig]) return false;
-    *s = find_tile_seg(w.chunk_start, nbig, c);
-    if (!classified(w.tree_bits[*s]) || w.bflags[*s]) return false;
-    *t0 = w.tile_start[*s] + (c - w.chunk_start[*s]) * CHUNK;
-    *t1 = min(*t0 + CHUNK, w.tile_start[*s + 1]);
-    return true;
+    return classified(w.tree_bits[s]) && !w.bflags[s] &&
+           w.chunk_start[s + 1] - w.chunk_start[s] > 1;
 }
 
 // Per chunk of a multi-chunk segment and slice of 256 buckets (blockIdx.y):
 // bucket sums over the chunk's tiles.
 __global__ void __launch_bounds__(256) k_chunk_sum(Work w, uint32_t nbig)
 {
-    const uint32_t c = blockIdx.x;
-    int s;
-    uint32_t t0, t1;
-    if (!chunk_tiles(w, nbig, c, &s, &t0, &t1)) return;
-    if (w.chunk_start[s + 1] - w.chunk_start[s] == 1) return;  // k_chunk_scan sets its base
-    const uint32_t B = seg_buckets(w, s);
-    const uint32_t b = blockIdx.y * 256 + threadIdx.x;
-    if (b >= B) return;
-    const uint32_t* col = w.tcount + (size_t)t0 * MAX_BKT + b;
-    const uint32_t nt = t1 - t0;
-    uint32_t sum = 0;
+    const uint32_t nchunk = w.chunk_start[nbig];
+    for (uint32_t c = blockIdx.x; c < nchunk; c += gridDim.x) {
+        const int s = find_tile_seg(w.chunk_start, nbig, c);
+        if (!multi_chunk(w, s)) continue;
+        const uint32_t B = seg_buckets(w, s);
+        const uint32_t b = blockIdx.y * 256 + threadIdx.x;
+        if (b >= B) continue;
+        const uint32_t t0 = w.tile_start[s] + (c - w.chunk_start[s]) * CHUNK;
+        const uint32_t nt = min(t0 + CHUNK, w.tile_start[s + 1]) - t0;
+        const uint32_t* col = w.tcount + (size_t)t0 * MAX_BKT + b;
+        uint32_t sum = 0;
 #pragma unroll
-    for (uint32_t j = 0; j < (uint32_t)CHUNK; ++j)
-        if (j < nt) sum += col[(size_t)j * MAX_BKT];
-    w.ccount[(size_t)c * MAX_BKT + b] = sum;
+        for (uint32_t j = 0; j < (uint32_t)CHUNK; ++j)
+            if (j < nt) sum += col[(size_t)j * MAX_BKT];
+        w.ccount[(size_t)c * MAX_BKT + b] = sum;
+    }
 }
 
-// Per segment and slice of 128 buckets: exclusive scan of the chunk sums
-// over the segment's chunks, offset by the segment begin and bucket start.
-__global__ void __launch_bounds__(128) k_chunk_scan(Work w)
+// Per multi-chunk segment and slice of 128 buckets: exclusive scan of the
+// chunk sums over the segment's chunks, offset by the segment begin and
+// bucket start.
+__global__ void __launch_bounds__(128) k_chunk_scan(Work w, uint32_t nbig)
 {
-    const int s = blockIdx.x;
-    const uint8_t L = w.tree_bits[s];
-    if (!classified(L) || w.bflags[s]) return;
-    const uint32_t B = seg_buckets(w, s);
-    const uint32_t b = blockIdx.y * 128 + threadIdx.x;
-    if (b >= B) return;
-    const uint32_t c0 = w.chunk_start[s], C = w.chunk_start[s + 1] - c0;
-    uint32_t run = w.list[L_BIG][w.cur][s].begin + w.bstart[(size_t)s * MAX_BKT + b];
-    uint32_t* cc = w.ccount + (size_t)c0 * MAX_BKT + b;
-    if (C == 1) {
-        cc[0] = run;
-        return;
-    }
-    constexpr uint32_t U = 8;  // loads in flight per thread
-    for (uint32_t j = 0; j < C; j += U) {
-        uint32_t v[U];
+    for (uint32_t s = blockIdx.x; s < nbig; s += gridDim.x) {
+        if (!multi_chunk(w, s)) continue;
+        const uint32_t B = seg_buckets(w, s);
+        const uint32_t b = blockIdx.y * 128 + threadIdx.x;
+        if (b >= B) continue;
+        const uint32_t c0 = w.chunk_start[s], C = w.chunk_start[s + 1] - c0;
+        uint32_t run = w.list[L_BIG][w.cur][s].begin + w.bstart[(size_t)s * MAX_BKT + b];
+        uint32_t* cc = w.ccount + (size_t)c0 * MAX_BKT + b;
+        constexpr uint32_t U = 8;  // loads in flight per thread
+        for (uint32_t j = 0; j < C; j += U) {
+            uint32_t v[U];
 #pragma unroll
-        for (uint32_t q = 0; q < U; ++q) v[q] = j + q < C ? cc[(size_t)(j + q) * MAX_BKT] : 0u;
+            for (uint32_t q = 0; q < U; ++q) v[q] = j + q < C ? cc[(size_t)(j + q) * MAX_BKT] : 0u;
 #pragma unroll
-        for (uint32_t q = 0; q < U; ++q) {
-            if (j + q < C) cc[(size_t)(j + q) * MAX_BKT] = run;
-            run += v[q];
+            for (uint32_t q = 0; q < U; ++q) {
+                if (j + q < C) cc[(size_t)(j + q) * MAX_BKT] = run;
+                run += v[q];
+            }
         }
     }
 }
 
-// Per chunk and slice of 256 buckets: each tile's first destination per
-// bucket (the chunk base plus the counts of the chunk's earlier tiles),
-// written over the tile counts.
+// Per chunk of a multi-chunk segment and slice of 256 buckets: each tile's
+// first destination per bucket (the chunk base plus the counts of the
+// chunk's earlier tiles), written over the tile counts.
 __global__ void __launch_bounds__(256) k_tile_offsets(Work w, uint32_t nbig)
 {
-    const uint32_t c = blockIdx.x;
-    int s;
-    uint32_t t0, t1;
-    if (!chunk_tiles(w, nbig, c, &s, &t0, &t1)) return;
-    const uint32_t B = seg_buckets(w, s);
-    const uint32_t b = blockIdx.y * 256 + threadIdx.x;
-    if (b >= B) return;
-    uint32_t* col = w.tcount + (size_t)t0 * MAX_BKT + b;
-    const uint32_t nt = t1 - t0;
-    uint32_t run = w.ccount[(size_t)c * MAX_BKT + b];
-    uint32_t v[CHUNK];
+    const uint32_t nchunk = w.chunk_start[nbig];
+    for (uint32_t c = blockIdx.x; c < nchunk; c += gridDim.x) {
+        const int s = find_tile_seg(w.chunk_start, nbig, c);
+        if (!multi_chunk(w, s)) continue;
+        const uint32_t B = seg_buckets(w, s);
+        const uint32_t b = blockIdx.y * 256 + threadIdx.x;
+        if (b >= B) continue;
+        const uint32_t t0 = w.tile_start[s] + (c - w.chunk_start[s]) * CHUNK;
+        const uint32_t nt = min(t0 + CHUNK, w.tile_start[s + 1]) - t0;
+        uint32_t* col = w.tcount + (size_t)t0 * MAX_BKT + b;
+        uint32_t run = w.ccount[(size_t)c * MAX_BKT + b];
+        uint32_t v[CHUNK];
 #pragma unroll
-    for (uint32_t j = 0; j < (uint32_t)CHUNK; ++j) v[j] = j < nt ? col[(size_t)j * MAX_BKT] : 0u;
+        for (uint32_t j = 0; j < (uint32_t)CHUNK; ++j) v[j] = j < nt ? col[(size_t)j * MAX_BKT] : 0u;
 #pragma unroll
-    for (uint32_t j = 0; j < (uint32_t)CHUNK; ++j) {
-        if (j < nt) col[(size_t)j * MAX_BKT] = run;
-        run += v[j];
+        for (uint32_t j = 0; j < (uint32_t)CHUNK; ++j) {
+            if (j < nt) col[(size_t)j * MAX_BKT] = run;
+            run += v[j];
+        }
     }
 }
 
@@ -492,8 +509,13 @@ __device__ __forceinline__ void push_seg(Work& w, int nxt, Seg c)
         return;
     }
     w.list[cls][nxt][at] = c;
-    if (cls == L_BIG) atomicAdd(w.counters + C_PAR * nxt + C_NTILES, (c.size + TILE - 1) / TILE);
-    else atomicAdd(w.counters + C_PAR * nxt + C_NSTR + cls, c.size);
+    if (cls == L_BIG) {
+        const uint32_t tiles = (c.size + TILE - 1) / TILE;
+        atomicAdd(w.counters + C_PAR * nxt + C_NTILES, tiles);
+        if (tiles > (uint32_t)CHUNK) atomicAdd(w.counters + C_MULTI + nxt, 1u);
+    } else {
+        atomicAdd(w.counters + C_PAR * nxt + C_NSTR + cls, c.size);
+    }
 }
 
 // Children of each bucket, after the scatter has placed them (hpp:1492-1584):
@@ -501,7 +523,7 @@ __device__ __forceinline__ void push_seg(Work& w, int nxt, Seg c)
 // are finished when their splitter ends the string. Behind a common-prefix
 // jump the tree buckets sit at depth + jump, and the two prefix buckets stay
 // at the segment depth without keys.
-__global__ void __launch_bounds__(1024) k_children(Work w)
+__global__ void __launch_bounds__(256) k_children(Work w)
 {
     const int s = blockIdx.x;
     const Seg sg = w.list[L_BIG][w.cur][s];
@@ -509,13 +531,10 @@ __global__ void __launch_bounds__(1024) k_children(Work w)
     const int buf = sg.meta & META_BUF;
     const int nxt = w.cur ^ 1;
     if (!classified(L)) return;
-    // block-aggregated appends: slots in shared memory first, then one
-    // global reservation per list
+    // block-aggregated appends, 256 buckets per round: slots in shared memory
+    // first, then one global reservation per list
     __shared__ uint32_t lcnt[L_NCLASS], gbase[L_NCLASS], lstr[L_NCLASS];
-    __shared__ uint32_t ltiles, lbnd, bbase;
-    if (threadIdx.x < L_NCLASS) { lcnt[threadIdx.x] = 0; lstr[threadIdx.x] = 0; }
-    if (threadIdx.x == 0) { ltiles = 0; lbnd = 0; }
-    __syncthreads();
+    __shared__ uint32_t ltiles, lmulti, lbnd, bbase;
     const uint32_t J = w.jump[s];
     const uint32_t B = seg_buckets(w, s);
     const uint32_t dj = sg.depth + J;  // depth of the tree buckets
@@ -524,81 +543,86 @@ __global__ void __launch_bounds__(1024) k_children(Work w)
     const uint32_t* bs = w.bstart + (size_t)s * MAX_BKT;
     const uint64_t* spl = w.spl + (size_t)s * 1024;
     const uint64_t* hs = w.hnd[nbuf];
-    constexpr int PER = (MAX_BKT + 1023) / 1024;
-    Seg child[PER];
-    int cls[PER];
-    uint32_t slot[PER], bslot[PER], bdep[PER];
-#pragma unroll
-    for (int j = 0; j < PER; ++j) {
-        cls[j] = -1;
-        bslot[j] = 0xFFFFFFFFu;
-        const uint32_t b = threadIdx.x + 1024u * j;
-        if (b >= B) continue;
-        const uint32_t c = bc[b];
-        if (c == 0) continue;
-        const uint32_t P = sg.begin + bs[b];
-        const bool edge = J && (b == 0 || b == B - 1);  // a prefix bucket
-        if (P > sg.begin && w.lcp) {
-            bslot[j] = atomicAdd(&lbnd, 1u);
-            // the string before P is in a prefix bucket, or this one is: the
-            // two strings are only known to share the segment depth
-            bdep[j] = (J && (b == B - 1 || bs[b] == bc[0])) ? sg.depth : dj;
-        }
-        if (c == 1) {
-            w.perm[P] = h_id(w, hs[P]);
-            continue;
-        }
-        const uint32_t tb = J ? b - 1 : b;  // tree bucket
-        if (edge) {
-            child[j] = Seg{P, c, sg.depth, (uint32_t)nbuf};
-        } else if (tb & 1) {
-            const uint64_t key = spl[tb >> 1];
-            if (key_terminated(key)) {
-                const uint32_t v = dj + lcp_key_depth(key);
-                if (c <= FINAL_INLINE) {
-                    for (uint32_t q = 0; q < c; ++q) {
-                        w.perm[P + q] = h_id(w, hs[P + q]);
-                        if (w.lcp && q) w.lcp[P + q] = v;
-                    }
-                    continue;
-                }
-                child[j] = Seg{P, c, v, (uint32_t)nbuf | META_FINAL};
-            } else {
-                child[j] = Seg{P, c, dj + 8, (uint32_t)nbuf};
+    for (uint32_t base = 0; base < B; base += 256) {
+        if (threadIdx.x < L_NCLASS) { lcnt[threadIdx.x] = 0; lstr[threadIdx.x] = 0; }
+        if (threadIdx.x == 0) { ltiles = 0; lmulti = 0; lbnd = 0; }
+        __syncthreads();
+        const uint32_t b = base + threadIdx.x;
+        Seg child{};
+        int cls = -1;
+        uint32_t slot = 0, bslot = 0xFFFFFFFFu, bdep = 0;
+        const uint32_t c = b < B ? bc[b] : 0u;
+        if (c) {
+            const uint32_t P = sg.begin + bs[b];
+            const bool edge = J && (b == 0 || b == B - 1);  // a prefix bucket
+            if (P > sg.begin && w.lcp) {
+                bslot = atomicAdd(&lbnd, 1u);
+                // the string before P is in a prefix bucket, or this one is:
+                // the two strings are only known to share the segment depth
+                bdep = (J && (b == B - 1 || bs[b] == bc[0])) ? sg.depth : dj;
             }
-        } else {
-            child[j] = Seg{P, c, dj, (uint32_t)nbuf | META_VALID};
+            if (c == 1) {
+                w.perm[P] = h_id(w, hs[P]);
+            } else {
+                const uint32_t tb = J ? b - 1 : b;  // tree bucket
+                bool inline_done = false;
+                if (edge) {
+                    child = Seg{P, c, sg.depth, (uint32_t)nbuf};
+                } else if (tb & 1) {
+                    const uint64_t key = spl[tb >> 1];
+                    if (key_terminated(key)) {
+                        const uint32_t v = dj + lcp_key_depth(key);
+                        if (c <= FINAL_INLINE) {
+                            for (uint32_t q = 0; q < c; ++q) {
+                                w.perm[P + q] = h_id(w, hs[P + q]);
+                                if (w.lcp && q) w.lcp[P + q] = v;
+                            }
+                            inline_done = true;
+                        } else {
+                            child = Seg{P, c, v, (uint32_t)nbuf | META_FINAL};
+                        }
+                    } else {
+                        child = Seg{P, c, dj + 8, (uint32_t)nbuf};
+                    }
+                } else {
+                    child = Seg{P, c, dj, (uint32_t)nbuf | META_VALID};
+                }
+                if (!inline_done) {
+                    if (c > SMALL_MAX) cls = L_BIG;
+                    else if (c > 256) cls = L_SMALLB;
+                    else if (c > WARP_GROUP_MAX) cls = L_SMALLA;
+                    else cls = L_TINY;
+                    slot = atomicAdd(&lcnt[cls], 1u);
+                    if (cls == L_BIG) {
+                        const uint32_t tiles = (c + TILE - 1) / TILE;
+                        atomicAdd(&ltiles, tiles);
+                        if (tiles > (uint32_t)CHUNK) atomicAdd(&lmulti, 1u);
+                    } else {
+                        atomicAdd(&lstr[cls], c);
+                    }
+                }
+            }
         }
-        if (c > SMALL_MAX) cls[j] = L_BIG;
-        else if (c > 256) cls[j] = L_SMALLB;
-        else if (c > WARP_GROUP_MAX) cls[j] = L_SMALLA;
-        else cls[j] = L_TINY;
-        slot[j] = atomicAdd(&lcnt[cls[j]], 1u);
-        if (cls[j] == L_BIG) atomicAdd(&ltiles, (c + TILE - 1) / TILE);
-        else atomicAdd(&lstr[cls[j]], c);
-    }
-    __syncthreads();
-    if (threadIdx.x < L_NCLASS && lcnt[threadIdx.x])
-        gbase[threadIdx.x] = atomicAdd(w.counters + C_PAR * nxt + threadIdx.x, lcnt[threadIdx.x]);
-    if (threadIdx.x == 32 && ltiles) atomicAdd(w.counters + C_PAR * nxt + C_NTILES, ltiles);
-    if (threadIdx.x >= 33 && threadIdx.x < 32 + L_NCLASS && lstr[threadIdx.x - 32])
-        atomicAdd(w.counters + C_PAR * nxt + C_NSTR + (threadIdx.x - 32), lstr[threadIdx.x - 32]);
-    if (threadIdx.x == 64 && lbnd) bbase = atomicAdd(w.counters + C_NBND, lbnd);
-    __syncthreads();
-#pragma unroll
-    for (int j = 0; j < PER; ++j) {
-        const uint32_t b = threadIdx.x + 1024u * j;
-        if (b >= B) continue;
-        if (bslot[j] != 0xFFFFFFFFu) {
-            const uint32_t at = bbase + bslot[j];
-            if (at < w.bnd_cap) w.bnd[at] = make_uint2(sg.begin + bs[b], bdep[j]);
+        __syncthreads();
+        if (threadIdx.x < L_NCLASS && lcnt[threadIdx.x])
+            gbase[threadIdx.x] = atomicAdd(w.counters + C_PAR * nxt + threadIdx.x, lcnt[threadIdx.x]);
+        if (threadIdx.x == 32 && ltiles) atomicAdd(w.counters + C_PAR * nxt + C_NTILES, ltiles);
+        if (threadIdx.x == 33 && lmulti) atomicAdd(w.counters + C_MULTI + nxt, lmulti);
+        if (threadIdx.x >= 64 + 1 && threadIdx.x < 64 + L_NCLASS && lstr[threadIdx.x - 64])
+            atomicAdd(w.counters + C_PAR * nxt + C_NSTR + (threadIdx.x - 64), lstr[threadIdx.x - 64]);
+        if (threadIdx.x == 96 && lbnd) bbase = atomicAdd(w.counters + C_NBND, lbnd);
+        __syncthreads();
+        if (bslot != 0xFFFFFFFFu) {
+            const uint32_t at = bbase + bslot;
+            if (at < w.bnd_cap) w.bnd[at] = make_uint2(sg.begin + bs[b], bdep);
             else set_error(w.counters + C_ERR, ERR_OVERFLOW);
         }
-        if (cls[j] >= 0) {
-            const uint32_t at = gbase[cls[j]] + slot[j];
-            if (at < w.cap[cls[j]]) w.list[cls[j]][nxt][at] = child[j];
+        if (cls >= 0) {
+            const uint32_t at = gbase[cls] + slot;
+            if (at < w.cap[cls]) w.list[cls][nxt][at] = child;
             else set_error(w.counters + C_ERR, ERR_OVERFLOW);
         }
+        __syncthreads();
     }
 }
 

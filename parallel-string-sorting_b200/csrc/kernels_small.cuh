@@ -214,6 +214,6 @@ __global__ void __launch_bounds__(32 * TINY_WARPS) k_tiny(Work w, const Seg* lis
 
 // the block-sorted size classes (kernels_block.cuh)
 constexpr int SMALL_A = 256;
-constexpr int SMALL_A_THREADS = 128;
+constexpr int SMALL_A_THREADS = 64;
 
 }  // namespace pssgpu

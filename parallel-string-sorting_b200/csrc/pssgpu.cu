@@ -316,6 +316,7 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
         nstr[k] = k == L_BIG ? 0u : hc[C_NSTR + k];
     }
     uint32_t ntiles = hc[C_NTILES];
+    uint32_t nmulti = hc[C_MULTI];
     uint64_t small_segments = 0;
     uint32_t err = hc[C_ERR];
     int cur = 0;
@@ -325,6 +326,7 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
         const uint32_t nbig = cnt[L_BIG];
         w.cur = cur;
         PSS_CUDA(cudaMemsetAsync(w.counters + C_PAR * nxt, 0, 4 * C_PAR, st));
+        PSS_CUDA(cudaMemsetAsync(w.counters + C_MULTI + nxt, 0, 4, st));
         PSS_CUDA(cudaMemsetAsync(w.counters + C_P_FIRST, 0, 4 * (C_P_LAST - C_P_FIRST + 1), st));
         if (nbig && ntiles > c->cap.tile_cap) return fail(PSSGPU_ECUDA, "tile capacity exceeded");
         // small classes: on the side streams (after everything queued on st
@@ -378,27 +380,32 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
             k_classify<<<ntiles, TILE_THREADS, 0, st>>>(w, nbig);
             kt.end(K_CLASSIFY);
             kt.begin(K_BSTART);
-            k_bstart<<<nbig, 1024, 0, st>>>(w);
-            {
+            k_bstart<<<nbig, 256, 0, st>>>(w);
+            if (nmulti) {
+                // segments of more than CHUNK tiles: chunked destination scan;
                 // chunks <= tiles, and <= one per CHUNK tiles plus one per segment
                 const uint32_t nchunk = std::min<uint32_t>(ntiles, ntiles / CHUNK + nbig);
-                k_chunk_sum<<<dim3(nchunk, (MAX_BKT + 255) / 256), 256, 0, st>>>(w, nbig);
-                k_chunk_scan<<<dim3(nbig, (MAX_BKT + 127) / 128), 128, 0, st>>>(w);
-                k_tile_offsets<<<dim3(nchunk, (MAX_BKT + 255) / 256), 256, 0, st>>>(w, nbig);
+                const uint32_t g = std::min<uint32_t>(nchunk, 1024);
+                k_chunk_sum<<<dim3(g, (MAX_BKT + 255) / 256), 256, 0, st>>>(w, nbig);
+                k_chunk_scan<<<dim3(std::min<uint32_t>(nbig, 256), (MAX_BKT + 127) / 128), 128, 0, st>>>(
+                    w, nbig);
+                k_tile_offsets<<<dim3(g, (MAX_BKT + 255) / 256), 256, 0, st>>>(w, nbig);
+                c->kstat[K_BSTART].launches += 3;
+                stats.kernel_launches += 3;
             }
             kt.end(K_BSTART);
             kt.begin(K_SCATTER);
             k_scatter<<<ntiles, TILE_THREADS, sizeof(ScatterSmem), st>>>(w, nbig);
             kt.end(K_SCATTER);
             kt.begin(K_CHILDREN);
-            k_children<<<nbig, 1024, 0, st>>>(w);
+            k_children<<<nbig, 256, 0, st>>>(w);
             kt.end(K_CHILDREN);
             c->kstat[K_SAMPLE].launches += 2;
             c->kstat[K_CLASSIFY].launches += 1;
-            c->kstat[K_BSTART].launches += 4;
+            c->kstat[K_BSTART].launches += 1;
             c->kstat[K_SCATTER].launches += 1;
             c->kstat[K_CHILDREN].launches += 1;
-            stats.kernel_launches += 9;
+            stats.kernel_launches += 6;
             stats.passes += 1;
         }
         for (int q = 0; q < 3; ++q)
@@ -437,6 +444,7 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
             nstr[k] = k == L_BIG ? 0u : hc[C_PAR * nxt + C_NSTR + k];
         }
         ntiles = hc[C_PAR * nxt + C_NTILES];
+        nmulti = hc[C_MULTI + nxt];
         err = hc[C_ERR];
         cur = nxt;
     }

@@ -37,6 +37,7 @@ enum : int {
     C_P_JCHUNKS = 25, // their prefix chunks: sum over jump segments of size * jump / 8
     C_P_FIRST = C_P_BIG,
     C_P_LAST = C_P_JCHUNKS,
+    C_MULTI = 26,     // + parity: big segments of more than CHUNK tiles in the list
     C_COUNT = 32
 };
 

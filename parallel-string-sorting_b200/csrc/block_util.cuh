@@ -91,21 +91,78 @@ __device__ __forceinline__ uint32_t block_scan_array(uint32_t* a, int N, uint32_
     return total;
 }
 
+// Compiler fence that pins the values of v in registers at this point: the
+// loads that produced them are issued (all in flight at once) before any
+// memory access that follows.
+template <int N>
+__device__ __forceinline__ void hold_loaded(uint32_t (&v)[N])
+{
+    static_assert(N % 8 == 0, "multiple of 8");
+#pragma unroll
+    for (int i = 0; i < N; i += 8)
+        asm volatile("" : "+r"(v[i]), "+r"(v[i + 1]), "+r"(v[i + 2]), "+r"(v[i + 3]), "+r"(v[i + 4]),
+                     "+r"(v[i + 5]), "+r"(v[i + 6]), "+r"(v[i + 7])::"memory");
+}
+
+// Bitonic stages (kk, j) with j <= 32 for kk in [kk_from, kk_to], on every
+// 64-key chunk of a[0, S) in registers: each warp takes whole chunks, two
+// keys per lane (positions e0 = 64 c + 2 lane and e0 + 1), partners by
+// shuffle. Directions follow the global positions, as in the full network.
+__device__ __forceinline__ void bitonic_chunk_stages(uint64_t* a, uint32_t S, uint32_t kk_from,
+                                                     uint32_t kk_to)
+{
+    const uint32_t lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (uint32_t c = threadIdx.x >> 5; c < S / 64; c += nw) {
+        const uint32_t e0 = c * 64 + 2 * lane;
+        uint64_t x0 = a[e0], x1 = a[e0 + 1];
+        for (uint32_t kk = kk_from; kk <= kk_to; kk <<= 1) {
+            const bool asc = (e0 & kk) == 0;  // e0 and e0 + 1 agree for kk >= 2
+            for (uint32_t j = min(kk >> 1, 32u); j > 0; j >>= 1) {
+                if (j == 1) {
+                    const uint64_t lo = min(x0, x1), hi = max(x0, x1);
+                    x0 = asc ? lo : hi;
+                    x1 = asc ? hi : lo;
+                } else {
+                    const uint64_t y0 = __shfl_xor_sync(0xffffffffu, x0, j >> 1);
+                    const uint64_t y1 = __shfl_xor_sync(0xffffffffu, x1, j >> 1);
+                    const bool keep_min = ((e0 & j) == 0) == asc;
+                    x0 = keep_min ? min(x0, y0) : max(x0, y0);
+                    x1 = keep_min ? min(x1, y1) : max(x1, y1);
+                }
+            }
+        }
+        a[e0] = x0;
+        a[e0 + 1] = x1;
+    }
+}
+
 // In-place ascending bitonic sort of S (a power of two) keys in shared
-// memory by the whole block; synchronises before returning.
+// memory by the whole block (a multiple of 32 threads); synchronises before
+// returning. Partner distances of 64 and more go through shared memory with
+// a barrier per stage, shorter ones run in registers inside a warp.
 __device__ __forceinline__ void bitonic_sort_block(uint64_t* a, uint32_t S)
 {
-    for (uint32_t kk = 2; kk <= S; kk <<= 1) {
-        for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
-            for (uint32_t i = threadIdx.x; i < S / 2; i += blockDim.x) {
-                const uint32_t x0 = 2 * i - (i & (j - 1));
-                const uint32_t x1 = x0 + j;
-                const bool asc = (x0 & kk) == 0;
-                const uint64_t x = a[x0], y = a[x1];
-                if ((x > y) == asc) { a[x0] = y; a[x1] = x; }
-            }
-            __syncthreads();
+    auto smem_stage = [&](uint32_t kk, uint32_t j) {
+        for (uint32_t i = threadIdx.x; i < S / 2; i += blockDim.x) {
+            const uint32_t x0 = 2 * i - (i & (j - 1));
+            const uint32_t x1 = x0 + j;
+            const bool asc = (x0 & kk) == 0;
+            const uint64_t x = a[x0], y = a[x1];
+            if ((x > y) == asc) { a[x0] = y; a[x1] = x; }
         }
+        __syncthreads();
+    };
+    if (S < 64) {
+        for (uint32_t kk = 2; kk <= S; kk <<= 1)
+            for (uint32_t j = kk >> 1; j > 0; j >>= 1) smem_stage(kk, j);
+        return;
+    }
+    bitonic_chunk_stages(a, S, 2, 64);
+    __syncthreads();
+    for (uint32_t kk = 128; kk <= S; kk <<= 1) {
+        for (uint32_t j = kk >> 1; j >= 64; j >>= 1) smem_stage(kk, j);
+        bitonic_chunk_stages(a, S, kk, kk);
+        __syncthreads();
     }
 }
 

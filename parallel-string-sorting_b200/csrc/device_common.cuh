@@ -61,13 +61,13 @@ __device__ __forceinline__ uint64_t load_key(const uint8_t* __restrict__ chars,
     return bswap64(raw);
 }
 
-// Keys of the cnt (<= NB) consecutive 8-char chunks at p, p + 8, ... into
-// out[0, cnt): cnt + 1 aligned word loads instead of two per chunk. Same
-// values as load_key at each position (chars at or beyond nchars read as
-// NUL); out[cnt, NB) are left 0.
+// The raw little-endian 8-char windows at p, p + 8, ... (cnt <= NB of them)
+// into raw[0, cnt): cnt + 1 aligned word loads instead of two per window.
+// Chars at or beyond nchars read as 0; raw[cnt, NB) are left 0. A window
+// becomes load_key's value through finish_key.
 template <int NB>
-__device__ __forceinline__ void load_chunks(const uint8_t* __restrict__ chars, uint64_t nchars,
-                                            uint64_t p, uint32_t cnt, uint64_t* out)
+__device__ __forceinline__ void load_raw_chunks(const uint8_t* __restrict__ chars, uint64_t nchars,
+                                                uint64_t p, uint32_t cnt, uint64_t* raw)
 {
     const uint64_t a = p & ~7ull;
     const unsigned sh = (unsigned)(p & 7) * 8u;
@@ -83,15 +83,19 @@ __device__ __forceinline__ void load_chunks(const uint8_t* __restrict__ chars, u
         wd[i] = v;
     }
 #pragma unroll
-    for (int i = 0; i < NB; ++i) {
-        uint64_t raw = sh ? ((wd[i] >> sh) | (wd[i + 1] << (64u - sh))) : wd[i];
-        const uint64_t z = (raw - 0x0101010101010101ull) & ~raw & 0x8080808080808080ull;
-        if (z) {
-            const unsigned nb = (unsigned)(__ffsll((long long)z) - 1) >> 3;
-            raw = nb ? (raw & (~0ull >> (64u - 8u * nb))) : 0ull;
-        }
-        out[i] = (uint32_t)i < cnt ? bswap64(raw) : 0ull;
+    for (int i = 0; i < NB; ++i)
+        raw[i] = (uint32_t)i < cnt ? (sh ? ((wd[i] >> sh) | (wd[i + 1] << (64u - sh))) : wd[i]) : 0ull;
+}
+
+// Big-endian key of a raw window: chars after its first NUL read as NUL.
+__device__ __forceinline__ uint64_t finish_key(uint64_t raw)
+{
+    const uint64_t z = (raw - 0x0101010101010101ull) & ~raw & 0x8080808080808080ull;
+    if (z) {
+        const unsigned nb = (unsigned)(__ffsll((long long)z) - 1) >> 3;
+        raw = nb ? (raw & (~0ull >> (64u - 8u * nb))) : 0ull;
     }
+    return bswap64(raw);
 }
 
 __device__ __forceinline__ uint64_t gather_key(const uint8_t* __restrict__ chars,

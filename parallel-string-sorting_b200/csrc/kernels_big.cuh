@@ -76,11 +76,12 @@ __global__ void k_tile_scan(Work w, uint32_t nbig)
     }
 }
 
-// One block of 1024 threads per big segment.
-__global__ void __launch_bounds__(1024) k_sample(Work w)
+// One block of 256 threads per big segment.
+__global__ void __launch_bounds__(256) k_sample(Work w)
 {
     __shared__ uint64_t samp[2 << MAX_TREE_BITS];
     __shared__ uint64_t shnd[2 << MAX_TREE_BITS];
+    __shared__ uint64_t smin, smax;
     __shared__ uint32_t jrun;
     const int s = blockIdx.x;
     const Seg sg = w.list[L_BIG][w.cur][s];
@@ -99,22 +100,54 @@ __global__ void __launch_bounds__(1024) k_sample(Work w)
     const uint32_t S = 2u << L;  // oversampling factor 2 (hpp:1388)
     const int buf = sg.meta & META_BUF;
     const bool valid = sg.meta & META_VALID;
+    // handles (and cached keys) of the samples, then the keys of stale ones:
+    // every load of a round is independent
+#pragma unroll 8
     for (uint32_t i = threadIdx.x; i < S; i += blockDim.x) {
         const uint64_t h = mix64(((uint64_t)sg.begin << 32) ^ ((uint64_t)sg.depth << 12) ^ i);
-        const uint32_t r = sg.begin + (uint32_t)(h % sg.size);
-        const uint64_t hd = w.hnd[buf][r];
-        shnd[i] = hd;
-        samp[i] = valid ? w.keys[buf][r] : h_key(w, hd, sg.depth);
+        const uint32_t r = sg.begin + (uint32_t)(((h >> 32) * sg.size) >> 32);
+        shnd[i] = w.hnd[buf][r];
+        if (valid) samp[i] = w.keys[buf][r];
+    }
+    if (!valid) {
+        __syncthreads();
+#pragma unroll 8
+        for (uint32_t i = threadIdx.x; i < S; i += blockDim.x) samp[i] = h_key(w, shnd[i], sg.depth);
+    }
+    // all samples equal? (a min / max reduction; the sort comes once the
+    // depth of the splitters is known)
+    if (threadIdx.x == 0) {
+        smin = ~0ull;
+        smax = 0;
     }
     __syncthreads();
-    bitonic_sort_block(samp, S);
+    {
+        uint64_t mn = ~0ull, mx = 0;
+        for (uint32_t i = threadIdx.x; i < S; i += blockDim.x) {
+            mn = min(mn, samp[i]);
+            mx = max(mx, samp[i]);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+            mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicMin((unsigned long long*)&smin, (unsigned long long)mn);
+            atomicMax((unsigned long long*)&smax, (unsigned long long)mx);
+        }
+    }
+    __syncthreads();
     uint32_t J = 0;  // chunks of the common-prefix jump
-    if (samp[0] == samp[S - 1] && !key_terminated(samp[0])) {
+    if (smin == smax && !key_terminated(smin)) {
         // Every sample shares the chunk at the segment depth: count the
-        // further chunks they all share, four per round, up to JMAX_CHUNKS.
-        // pS5 would advance such a tied group one chunk per step
-        // (hpp:1527-1528, 1555-1556).
+        // further chunks that the first (up to blockDim) samples share with
+        // sample 0, four per round, up to JMAX_CHUNKS. pS5 would advance such
+        // a tied group one chunk per step (hpp:1527-1528, 1555-1556). Any
+        // jump that sample 0 has is correct: strings leaving its prefix go
+        // to the two prefix buckets, and splitters may be any keys.
         const uint64_t ref = h_off(w, shnd[0]) + sg.depth;
+        const uint32_t JS = min(S, blockDim.x);
         J = 1;
         while (J < (uint32_t)JMAX_CHUNKS) {
             if (threadIdx.x == 0) jrun = 4;
@@ -123,8 +156,8 @@ __global__ void __launch_bounds__(1024) k_sample(Work w)
 #pragma unroll
             for (int q = 0; q < 4; ++q) rk[q] = load_key(w.chars, w.nchars, ref + 8ull * (J + q));
             uint32_t mine = 4;
-            for (uint32_t i = threadIdx.x; i < S; i += blockDim.x) {
-                const uint64_t o = h_off(w, shnd[i]) + sg.depth;
+            if (threadIdx.x < JS) {
+                const uint64_t o = h_off(w, shnd[threadIdx.x]) + sg.depth;
                 uint32_t e = 0;
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
@@ -145,11 +178,12 @@ __global__ void __launch_bounds__(1024) k_sample(Work w)
         uint64_t* jp = w.jpre + (size_t)s * JMAX_CHUNKS;
         for (uint32_t c = threadIdx.x; c < J; c += blockDim.x)
             jp[c] = load_key(w.chars, w.nchars, ref + 8ull * c);
+#pragma unroll 8
         for (uint32_t i = threadIdx.x; i < S; i += blockDim.x)
             samp[i] = h_key(w, shnd[i], sg.depth + 8 * J);
         __syncthreads();
-        bitonic_sort_block(samp, S);
     }
+    bitonic_sort_block(samp, S);
     if (threadIdx.x == 0) {
         w.jump[s] = 8 * J;
         atomicAdd(w.counters + C_P_BIG, sg.size);
@@ -182,7 +216,8 @@ __global__ void __launch_bounds__(1024) k_sample(Work w)
 __global__ void __launch_bounds__(TILE_THREADS, 6) k_classify(Work w, uint32_t nbig)
 {
     __shared__ uint64_t tree[1024];
-    __shared__ uint64_t jp[JMAX_CHUNKS];
+    __shared__ uint64_t jp[JMAX_CHUNKS];   // the shared chunks as keys
+    __shared__ uint64_t jpr[JMAX_CHUNKS];  // and as raw windows
     __shared__ uint32_t hist[MAX_BKT];
     const uint32_t t = blockIdx.x;
     const int s = find_tile_seg(w.tile_start, nbig, t);
@@ -205,7 +240,11 @@ __global__ void __launch_bounds__(TILE_THREADS, 6) k_classify(Work w, uint32_t n
     const uint32_t B = seg_buckets(w, s);
     const uint64_t* gtree = w.tree + (size_t)s * 1024;
     for (uint32_t v = threadIdx.x; v <= k; v += TILE_THREADS) tree[v] = gtree[v];
-    for (uint32_t c = threadIdx.x; c < nc; c += TILE_THREADS) jp[c] = w.jpre[(size_t)s * JMAX_CHUNKS + c];
+    for (uint32_t c = threadIdx.x; c < nc; c += TILE_THREADS) {
+        const uint64_t kc = w.jpre[(size_t)s * JMAX_CHUNKS + c];
+        jp[c] = kc;
+        jpr[c] = bswap64(kc);  // no NUL inside a shared chunk
+    }
     for (uint32_t b = threadIdx.x; b < B; b += TILE_THREADS) hist[b] = 0;
     __syncthreads();
     const bool valid = (sg.meta & META_VALID) && !J;
@@ -222,14 +261,20 @@ __global__ void __launch_bounds__(TILE_THREADS, 6) k_classify(Work w, uint32_t n
             const uint64_t o = h_off(w, hs[p]) + sg.depth;
             constexpr uint32_t NB = 7;  // chunks per batch: a 6-chunk prefix and its key
             for (uint32_t c0 = 0; c0 <= nc && !side; c0 += NB) {
-                uint64_t kk[NB];
-                load_chunks<NB>(w.chars, w.nchars, o + 8ull * c0, min(NB, nc + 1 - c0), kk);
+                uint64_t raw[NB];
+                load_raw_chunks<NB>(w.chars, w.nchars, o + 8ull * c0, min(NB, nc + 1 - c0), raw);
 #pragma unroll
                 for (uint32_t q = 0; q < NB; ++q) {
                     const uint32_t c = c0 + q;
                     if (side || c > nc) continue;
-                    if (c == nc) key = kk[q];
-                    else if (kk[q] != jp[c]) side = kk[q] < jp[c] ? -1 : 1;
+                    if (c == nc) {
+                        key = finish_key(raw[q]);
+                    } else if (raw[q] != jpr[c]) {
+                        // equal raw windows hold no NUL (the shared chunk has
+                        // none); the first unequal one decides the side
+                        const uint64_t kq = finish_key(raw[q]);
+                        side = kq < jp[c] ? -1 : 1;
+                    }
                 }
             }
             keys[p] = key;
@@ -271,8 +316,9 @@ __device__ __forceinline__ bool classified(uint8_t L)
 // a segment of at most CHUNK tiles also every tile's first destination per
 // bucket (count_finished over (tile, bucket), hpp:1437-1460); longer
 // segments take the chunked scan below.
-__global__ void __launch_bounds__(256) k_bstart(Work w)
+__global__ void __launch_bounds__(512) k_bstart(Work w)
 {
+    constexpr uint32_t T = 512;
     __shared__ uint32_t a[MAX_BKT];
     __shared__ uint32_t tmp[32];
     __shared__ int one;
@@ -284,34 +330,32 @@ __global__ void __launch_bounds__(256) k_bstart(Work w)
     const uint32_t* bc = w.bcount + (size_t)s * MAX_BKT;
     if (threadIdx.x == 0) one = 0;
     __syncthreads();
-    for (uint32_t b = threadIdx.x; b < B; b += 256) {
+    for (uint32_t b = threadIdx.x; b < B; b += T) {
         const uint32_t c = bc[b];
         a[b] = c;
         if (c == sg.size) one = 1;
     }
     __syncthreads();
-    block_scan_array<256>(a, (int)B, tmp);
+    block_scan_array<T>(a, (int)B, tmp);
     uint32_t* bs = w.bstart + (size_t)s * MAX_BKT;
-    for (uint32_t b = threadIdx.x; b < B; b += 256) bs[b] = a[b];
+    for (uint32_t b = threadIdx.x; b < B; b += T) bs[b] = a[b];
     if (threadIdx.x == 0) {
         w.bflags[s] = (uint8_t)one;
         if (!one) atomicAdd(w.counters + C_P_SCATTER, sg.size);
     }
     const uint32_t t0 = w.tile_start[s], nt = w.tile_start[s + 1] - t0;
     if (one || nt > (uint32_t)CHUNK) return;
-    for (uint32_t b = threadIdx.x; b < B; b += 256) {
+    for (uint32_t b = threadIdx.x; b < B; b += T) {
         uint32_t run = sg.begin + a[b];
         uint32_t* col = w.tcount + (size_t)t0 * MAX_BKT + b;
-        constexpr uint32_t U = 8;  // loads in flight per thread
-        for (uint32_t j = 0; j < nt; j += U) {
-            uint32_t v[U];
+        uint32_t v[CHUNK];  // all of the column's loads in flight
 #pragma unroll
-            for (uint32_t q = 0; q < U; ++q) v[q] = j + q < nt ? col[(size_t)(j + q) * MAX_BKT] : 0u;
+        for (uint32_t j = 0; j < (uint32_t)CHUNK; ++j) v[j] = j < nt ? col[(size_t)j * MAX_BKT] : 0u;
+        hold_loaded(v);
 #pragma unroll
-            for (uint32_t q = 0; q < U; ++q) {
-                if (j + q < nt) col[(size_t)(j + q) * MAX_BKT] = run;
-                run += v[q];
-            }
+        for (uint32_t j = 0; j < (uint32_t)CHUNK; ++j) {
+            if (j < nt) col[(size_t)j * MAX_BKT] = run;
+            run += v[j];
         }
     }
 }
@@ -361,11 +405,12 @@ __global__ void __launch_bounds__(128) k_chunk_scan(Work w, uint32_t nbig)
         const uint32_t c0 = w.chunk_start[s], C = w.chunk_start[s + 1] - c0;
         uint32_t run = w.list[L_BIG][w.cur][s].begin + w.bstart[(size_t)s * MAX_BKT + b];
         uint32_t* cc = w.ccount + (size_t)c0 * MAX_BKT + b;
-        constexpr uint32_t U = 8;  // loads in flight per thread
+        constexpr uint32_t U = 16;  // loads in flight per thread
         for (uint32_t j = 0; j < C; j += U) {
             uint32_t v[U];
 #pragma unroll
             for (uint32_t q = 0; q < U; ++q) v[q] = j + q < C ? cc[(size_t)(j + q) * MAX_BKT] : 0u;
+            hold_loaded(v);
 #pragma unroll
             for (uint32_t q = 0; q < U; ++q) {
                 if (j + q < C) cc[(size_t)(j + q) * MAX_BKT] = run;
@@ -394,6 +439,7 @@ __global__ void __launch_bounds__(256) k_tile_offsets(Work w, uint32_t nbig)
         uint32_t v[CHUNK];
 #pragma unroll
         for (uint32_t j = 0; j < (uint32_t)CHUNK; ++j) v[j] = j < nt ? col[(size_t)j * MAX_BKT] : 0u;
+        hold_loaded(v);
 #pragma unroll
         for (uint32_t j = 0; j < (uint32_t)CHUNK; ++j) {
             if (j < nt) col[(size_t)j * MAX_BKT] = run;

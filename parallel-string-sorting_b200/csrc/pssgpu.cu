@@ -374,13 +374,13 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
         if (nbig) {
             kt.begin(K_SAMPLE);
             k_tile_scan<<<1, 1024, 0, st>>>(w, nbig);
-            k_sample<<<nbig, 1024, 0, st>>>(w);
+            k_sample<<<nbig, 256, 0, st>>>(w);
             kt.end(K_SAMPLE);
             kt.begin(K_CLASSIFY);
             k_classify<<<ntiles, TILE_THREADS, 0, st>>>(w, nbig);
             kt.end(K_CLASSIFY);
             kt.begin(K_BSTART);
-            k_bstart<<<nbig, 256, 0, st>>>(w);
+            k_bstart<<<nbig, 512, 0, st>>>(w);
             if (nmulti) {
                 // segments of more than CHUNK tiles: chunked destination scan;
                 // chunks <= tiles, and <= one per CHUNK tiles plus one per segment

@@ -51,7 +51,11 @@ def parse():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--n", type=int, default=N_DEFAULT, help="strings per instance")
+    p.add_argument("--n", type=int, default=N_DEFAULT, help="strings per instance (prefixes)")
+    p.add_argument("--workload", choices=["prefixes", "digits", "dna"], default="prefixes",
+                   help="sort mode: prefixes = 64 Mi high-LCP strings (the headline), "
+                        "digits = the 10 MiB random-digit strings, dna = all suffixes of a "
+                        "32 MiB repetitive DNA text")
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--cpu-sample", type=int, default=CPU_SAMPLE)
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -67,11 +71,31 @@ def parse():
     return p.parse_args()
 
 
-def workload_config(n: int, nchars: int) -> dict:
+def workload_config(n: int, nchars, workload: str = "prefixes") -> dict:
+    if workload == "digits":
+        return {"workload": "digits-10MiB", "strings": n, "chars": nchars,
+                "lengths": "U[1,40]", "alphabet": "0-9", "seed": 1,
+                "l2": "256 MB written between timed steps (inputs fit in L2)",
+                "lcp_output": False}
+    if workload == "dna":
+        return {"workload": "dna-suffixes-32MiB", "strings": n, "chars": nchars,
+                "text": "32 MiB uniform ACGT, 5% overwritten by copies of earlier 1-10 KiB blocks",
+                "seed": 3, "l2": "256 MB written between timed steps",
+                "lcp_output": False}
     return {"workload": "prefixes-64Mi" if n == N_DEFAULT else f"prefixes-{n}",
             "strings": n, "chars": nchars, "prefixes": 4096, "prefix_len": 48,
             "zipf_s": 1.1, "suffix_len": "U[8,24]", "alphabet": "a-z", "seed": SEED,
             "l2": "inputs larger than L2 (126 MB)", "lcp_output": False}
+
+
+def make_workload(pkg, workload: str, n: int, seed_offset: int = 0, alloc=None):
+    """(chars, offs, nchars) of a sort-mode workload; n applies to prefixes."""
+    kw = {} if alloc is None else {"alloc": alloc}
+    if workload == "digits":
+        return pkg.workloads.digits(seed=1 + seed_offset, **kw)
+    if workload == "dna":
+        return pkg.workloads.dna_suffixes(seed=3 + seed_offset, **kw)
+    return pkg.workloads.prefixes(n=n, seed=SEED + seed_offset, **kw)
 
 
 def measured_peak() -> tuple:
@@ -132,16 +156,18 @@ def pinned_alloc(torch):
     return alloc
 
 
-def cpu_baseline(n_sample: int) -> dict:
+def cpu_baseline(n_sample: int, workload: str = "prefixes") -> dict:
     """Reference pS5 (parallel_sample_sortBTCUI) on the first n_sample strings
-    of the same generator, all host threads, best of 3."""
+    of the same generator (the whole input for digits and dna), all host
+    threads, best of 3."""
     from oracle import oracle as orc
     import __graft_entry__
     pkg = __graft_entry__.load_package()
     if not orc.ref_available():
         return {"value": None, "unit": "GB/s", "cores": os.cpu_count(), "kind": "reference",
                 "sample": "oracle/_ref/libps5ref.so not built"}
-    chars, offs, nchars = pkg.workloads.prefixes(n=n_sample, seed=SEED)
+    chars, offs, nchars = make_workload(pkg, workload, n_sample)
+    n_sample = offs.shape[0]
     threads = os.cpu_count()
     lib = orc.ref_lib()
     lib.ps5ref_set_threads(threads)
@@ -154,7 +180,7 @@ def cpu_baseline(n_sample: int) -> dict:
         times.append(time.perf_counter() - t0)
     t = min(times)
     return {"value": nchars / t / 1e9, "unit": "GB/s", "cores": threads, "kind": "reference",
-            "sample": f"first {n_sample} strings of the same generator ({nchars} chars), "
+            "sample": f"{n_sample} strings of the same generator ({nchars} chars), "
                       f"pS5-Unroll (parallel_sample_sortBTCUI) best of 3: {t * 1e3:.1f} ms",
             "strings_per_s": n_sample / t}
 
@@ -166,8 +192,8 @@ def run_reference(args):
     from oracle import oracle as orc
     import __graft_entry__
     pkg = __graft_entry__.load_package()
-    n = args.cpu_sample
-    chars, offs, nchars = pkg.workloads.prefixes(n=n, seed=SEED)
+    chars, offs, nchars = make_workload(pkg, args.workload, args.cpu_sample)
+    n = offs.shape[0]
     if not orc.ref_available():
         print(json.dumps({"impl": "reference", "unavailable":
                           "oracle/_ref/libps5ref.so (reference pS5 built from its sources) missing"}))
@@ -187,7 +213,7 @@ def run_reference(args):
         times.append(time.perf_counter() - t0)
     t = sum(times) / len(times)
     value = nchars / t / 1e9
-    cfg = workload_config(args.n, None)
+    cfg = workload_config(args.n if args.workload == "prefixes" else n, None, args.workload)
     cfg.update({"sample_strings": n, "sample_chars": nchars})
     line = {
         "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": args.gpus,
@@ -195,7 +221,7 @@ def run_reference(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
         "data": "synthetic", "config": cfg, "impl": "reference",
         "cpu_baseline": {"value": value, "unit": "GB/s", "cores": threads, "kind": "reference",
-                         "sample": f"first {n} strings of the workload generator ({nchars} chars), "
+                         "sample": f"{n} strings of the workload generator ({nchars} chars), "
                                    "pS5-Unroll (parallel_sample_sortBTCUI) from the reference "
                                    "sources, every host thread"},
         "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -387,9 +413,13 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.SUM)
         return float(t.item())
 
-    n = args.n
     alloc = pinned_alloc(torch)
-    h_chars, h_offs, nchars = pkg.workloads.prefixes(n=n, seed=SEED + rank, alloc=alloc)
+    h_chars, h_offs, nchars = make_workload(pkg, args.workload, args.n, rank, alloc)
+    n = h_offs.shape[0]
+    # inputs that fit in L2 are evicted between timed steps by writing a
+    # buffer twice the L2 size (outside the timed events)
+    flush = None if args.workload == "prefixes" else torch.empty(256 << 20, dtype=torch.uint8,
+                                                                  device="cuda")
     ctx = pkg.Context(local)
     stream = torch.cuda.current_stream()
     d_chars = torch.from_numpy(h_chars).cuda(non_blocking=True)
@@ -416,15 +446,27 @@ def main():
     torch.cuda.synchronize()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for _ in range(args.steps):
-        step()
-        launches += ctx.stats()["kernel_launches"]
-    ev1.record(stream)
-    torch.cuda.synchronize()
+    if flush is None:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+            launches += ctx.stats()["kernel_launches"]
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1) / args.steps
+    else:
+        tot = 0.0
+        for _ in range(args.steps):
+            flush.zero_()
+            ev0.record(stream)
+            step()
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            tot += ev0.elapsed_time(ev1)
+            launches += ctx.stats()["kernel_launches"]
+        ms = tot / args.steps
     barrier()
     clk = clocks.stop()
-    ms = ev0.elapsed_time(ev1) / args.steps
 
     # per-kernel-class split (profile mode: classes run one after another on
     # the stream, each between CUDA events), outside the timed region
@@ -465,14 +507,14 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(min(args.cpu_sample, n))
+        cpu = cpu_baseline(min(args.cpu_sample, n), args.workload)
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world,
             "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms_max,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
-            "data": "synthetic", "config": workload_config(n, nchars),
+            "data": "synthetic", "config": workload_config(n, nchars, args.workload),
             "strings_per_s": world * n / (ms_max / 1e3),
             "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": nchars + 8 * n,
                     "d2h_bytes_per_step": 4 * n, "ms_per_step": e2e_s * 1e3},

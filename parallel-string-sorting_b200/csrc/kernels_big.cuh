@@ -76,8 +76,9 @@ __global__ void k_tile_scan(Work w, uint32_t nbig)
     }
 }
 
-// One block of 256 threads per big segment.
-__global__ void __launch_bounds__(256) k_sample(Work w)
+// One block per big segment (256 threads, or 1024 when the pass has few
+// segments and each block's latency is the pass's).
+__global__ void __launch_bounds__(1024) k_sample(Work w)
 {
     __shared__ uint64_t samp[2 << MAX_TREE_BITS];
     __shared__ uint64_t shnd[2 << MAX_TREE_BITS];
@@ -569,7 +570,7 @@ __device__ __forceinline__ void push_seg(Work& w, int nxt, Seg c)
 // are finished when their splitter ends the string. Behind a common-prefix
 // jump the tree buckets sit at depth + jump, and the two prefix buckets stay
 // at the segment depth without keys.
-__global__ void __launch_bounds__(256) k_children(Work w)
+__global__ void __launch_bounds__(1024) k_children(Work w)
 {
     const int s = blockIdx.x;
     const Seg sg = w.list[L_BIG][w.cur][s];
@@ -577,8 +578,8 @@ __global__ void __launch_bounds__(256) k_children(Work w)
     const int buf = sg.meta & META_BUF;
     const int nxt = w.cur ^ 1;
     if (!classified(L)) return;
-    // block-aggregated appends, 256 buckets per round: slots in shared memory
-    // first, then one global reservation per list
+    // block-aggregated appends, blockDim.x (>= 128) buckets per round: slots
+    // in shared memory first, then one global reservation per list
     __shared__ uint32_t lcnt[L_NCLASS], gbase[L_NCLASS], lstr[L_NCLASS];
     __shared__ uint32_t ltiles, lmulti, lbnd, bbase;
     const uint32_t J = w.jump[s];
@@ -589,7 +590,7 @@ __global__ void __launch_bounds__(256) k_children(Work w)
     const uint32_t* bs = w.bstart + (size_t)s * MAX_BKT;
     const uint64_t* spl = w.spl + (size_t)s * 1024;
     const uint64_t* hs = w.hnd[nbuf];
-    for (uint32_t base = 0; base < B; base += 256) {
+    for (uint32_t base = 0; base < B; base += blockDim.x) {
         if (threadIdx.x < L_NCLASS) { lcnt[threadIdx.x] = 0; lstr[threadIdx.x] = 0; }
         if (threadIdx.x == 0) { ltiles = 0; lmulti = 0; lbnd = 0; }
         __syncthreads();

@@ -76,7 +76,7 @@ __device__ __forceinline__ void blk_push(BlockSmem<MAXN>& sm, uint32_t start, ui
 }
 
 template <int MAXN, int THREADS>
-__global__ void __launch_bounds__(THREADS) k_block(Work w, const Seg* list)
+__global__ void __launch_bounds__(THREADS, THREADS <= 64 ? 20 : 4) k_block(Work w, const Seg* list)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     BlockSmem<MAXN>& sm = *reinterpret_cast<BlockSmem<MAXN>*>(smem_raw);
@@ -156,10 +156,8 @@ __global__ void __launch_bounds__(THREADS) k_block(Work w, const Seg* list)
             if (threadIdx.x == 0) sm.jump = 0xFFFFFFFFu;
             __syncthreads();
             const uint64_t base = sm.hnd[s];
-            for (uint32_t i = 1 + threadIdx.x; i < c; i += THREADS) {
-                const uint32_t lim = *((volatile uint32_t*)&sm.jump);
-                atomicMin(&sm.jump, chunks_equal(w, base, sm.hnd[s + i], d, lim));
-            }
+            for (uint32_t i = 1 + threadIdx.x; i < c; i += THREADS)
+                atomicMin(&sm.jump, chunks_equal(w, base, sm.hnd[s + i], d, &sm.jump));
             __syncthreads();
             const uint32_t jmp = sm.jump;
             if (jmp > 0) {

@@ -14,9 +14,10 @@
 // A warp window holds up to 32 strings from one or more independent groups.
 // Each lane owns one output slot (a position of the permutation); groups
 // never leave their lanes. Every round sorts (group, key) over the 32 lanes,
-// splits runs of equal keys into groups one 8-byte round deeper, and lets a
-// last group that stops splitting jump ahead with a warp-wide 256-byte
-// compare, so deep repeats cost O(LCP / 256) rounds.
+// splits runs of equal keys into groups one 8-byte round deeper; after two
+// rounds in which no group split and no string finished, every group jumps to
+// its common prefix with warp-wide 512-byte compares, so deep repeats cost
+// O(LCP / 512) steps.
 #pragma once
 
 #include "block_util.cuh"
@@ -26,19 +27,27 @@ namespace pssgpu {
 
 // Common-prefix extension (in 8-byte chunks from depth d) of the string
 // behind handle `other` against the one behind `base`: the first chunk where
-// they differ or base ends, at most `limit`.
+// they differ or base ends. The search stops at *limit, which other threads
+// lower meanwhile (re-read every 4 chunks; the 4 chunks of both strings are
+// loaded at once), so one long shared repeat does not hold up the block once
+// another string has shown a shorter common prefix.
 __device__ __forceinline__ uint32_t chunks_equal(const Work& w, uint64_t base, uint64_t other,
-                                                 uint32_t d, uint32_t limit)
+                                                 uint32_t d, const volatile uint32_t* limit)
 {
-    uint32_t c = 0;
     const uint64_t ob = h_off(w, base) + d, oo = h_off(w, other) + d;
-    while (c < limit) {
-        const uint64_t ka = load_key(w.chars, w.nchars, ob + 8ull * c);
-        const uint64_t kb = load_key(w.chars, w.nchars, oo + 8ull * c);
-        if (ka != kb || key_terminated(ka)) break;
-        ++c;
+    for (uint32_t c = 0;; c += 4) {
+        if (c >= *limit) return c;
+        uint64_t ra[4], rb[4];
+        load_raw_chunks<4>(w.chars, w.nchars, ob + 8ull * c, 4, ra);
+        load_raw_chunks<4>(w.chars, w.nchars, oo + 8ull * c, 4, rb);
+#pragma unroll
+        for (uint32_t q = 0; q < 4; ++q) {
+            // equal windows without a NUL continue; any other pair of windows
+            // either differs before a NUL or ends base's string here
+            const uint64_t z = (ra[q] - 0x0101010101010101ull) & ~ra[q] & 0x8080808080808080ull;
+            if (ra[q] != rb[q] || z) return c + q;
+        }
     }
-    return c;
 }
 
 // Finish a warp window. Per lane on entry: the string handle of the slot,
@@ -55,37 +64,54 @@ __device__ __forceinline__ uint64_t warp_window(const Work& w, uint64_t myh, uin
     uint32_t mystate = mygrp < 32 ? 0u : 1u;  // 0 active, 1 done
     uint64_t mykey = 0;
     uint32_t prev_active = __popc(__ballot_sync(0xffffffffu, mystate == 0));
-    bool stalled = false;
+    uint32_t gstarts = __ballot_sync(0xffffffffu, mystate == 0 && mygrp == lane);
+    uint32_t prev_groups = __popc(gstarts);
+    uint32_t stalled = 0;  // rounds in a row without progress
     bool first = true;
     while (true) {
         const uint32_t A = __ballot_sync(0xffffffffu, mystate == 0);
         if (A == 0) break;
-        if (stalled) {
-            // exactly one active group left and it did not split: jump to
-            // its common prefix, 32 chunks of 8 bytes per step
-            const int f = __ffs(A) - 1;
-            const uint64_t base = __shfl_sync(0xffffffffu, myh, f);
-            const uint32_t dd = __shfl_sync(0xffffffffu, mydep, f);
-            uint32_t best = 0xFFFFFFFFu;
-            uint32_t rest = A & ~(1u << f);
-            const uint64_t ob = h_off(w, base) + dd;
-            while (rest) {
-                const int j = __ffs(rest) - 1;
-                rest &= rest - 1;
-                const uint64_t other = __shfl_sync(0xffffffffu, myh, j);
-                const uint64_t oo = h_off(w, other) + dd;
-                for (uint32_t t = 0; t * 32 < best; ++t) {
-                    const uint32_t ch = t * 32 + lane;
-                    const uint64_t ka = load_key(w.chars, w.nchars, ob + 8ull * ch);
-                    const uint64_t kb = load_key(w.chars, w.nchars, oo + 8ull * ch);
-                    const uint32_t bal = __ballot_sync(0xffffffffu, ka != kb || key_terminated(ka));
-                    if (bal) {
-                        best = min(best, t * 32 + (uint32_t)(__ffs(bal) - 1));
-                        break;
+        if (stalled >= 2) {
+            // the last two rounds neither split a group nor finished a
+            // string: move every active group to its common prefix, one
+            // group at a time, 64 chunks of 8 bytes per step
+            stalled = 0;
+            uint32_t todo = gstarts;
+            while (todo) {
+                const int f = __ffs(todo) - 1;
+                todo &= todo - 1;
+                const uint64_t base = __shfl_sync(0xffffffffu, myh, f);
+                const uint32_t dd = __shfl_sync(0xffffffffu, mydep, f);
+                const bool member = mystate == 0 && mygrp == (uint32_t)f;
+                uint32_t rest = __ballot_sync(0xffffffffu, member) & ~(1u << f);
+                uint32_t best = 0xFFFFFFFFu;
+                const uint64_t ob = h_off(w, base) + dd;
+                while (rest) {
+                    const int j = __ffs(rest) - 1;
+                    rest &= rest - 1;
+                    const uint64_t other = __shfl_sync(0xffffffffu, myh, j);
+                    const uint64_t oo = h_off(w, other) + dd;
+                    for (uint32_t t = 0; t * 64 < best; ++t) {
+                        // lane l compares chunks 64 t + 2 l and 64 t + 2 l + 1:
+                        // equal windows without a NUL continue
+                        const uint32_t ch = t * 64 + 2 * lane;
+                        uint64_t ra[2], rb[2];
+                        load_raw_chunks<2>(w.chars, w.nchars, ob + 8ull * ch, 2, ra);
+                        load_raw_chunks<2>(w.chars, w.nchars, oo + 8ull * ch, 2, rb);
+                        const uint64_t z0 = (ra[0] - 0x0101010101010101ull) & ~ra[0] & 0x8080808080808080ull;
+                        const uint64_t z1 = (ra[1] - 0x0101010101010101ull) & ~ra[1] & 0x8080808080808080ull;
+                        const bool m0 = ra[0] != rb[0] || z0, m1 = ra[1] != rb[1] || z1;
+                        const uint32_t bal = __ballot_sync(0xffffffffu, m0 || m1);
+                        if (bal) {
+                            const int fl = __ffs(bal) - 1;
+                            const uint32_t first0 = __ballot_sync(0xffffffffu, m0) >> fl & 1u;
+                            best = min(best, t * 64 + 2u * fl + (first0 ? 0u : 1u));
+                            break;
+                        }
                     }
                 }
+                if (member) mydep = dd + 8u * best;
             }
-            if (mystate == 0) mydep = dd + 8u * best;
         }
         if (mystate == 0) mykey = (first && has_key) ? key0 : h_key(w, myh, mydep);
         first = false;
@@ -159,8 +185,10 @@ __device__ __forceinline__ uint64_t warp_window(const Work& w, uint64_t myh, uin
         const uint32_t A2 = __ballot_sync(0xffffffffu, mystate == 0);
         const uint32_t G2 = __ballot_sync(0xffffffffu, mystate == 0 && rs == lane);
         const uint32_t na = __popc(A2);
-        stalled = (na == prev_active) && (__popc(G2) == 1);
+        stalled = (na == prev_active && __popc(G2) == prev_groups) ? stalled + 1 : 0;
         prev_active = na;
+        prev_groups = __popc(G2);
+        gstarts = G2;
     }
     return myh;
 }
@@ -184,7 +212,7 @@ __device__ __forceinline__ void for_each_window(uint32_t ngroups, SizeFn sizes, 
 // list entries and packs them into warp windows.
 constexpr int TINY_WARPS = 8;
 constexpr int TINY_PER_WARP = 8;
-__global__ void __launch_bounds__(32 * TINY_WARPS) k_tiny(Work w, const Seg* list, uint32_t count)
+__global__ void __launch_bounds__(32 * TINY_WARPS, 5) k_tiny(Work w, const Seg* list, uint32_t count)
 {
     __shared__ uint32_t scratch[TINY_WARPS][32];
     const uint32_t lane = threadIdx.x & 31;

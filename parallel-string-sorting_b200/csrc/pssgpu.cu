@@ -374,7 +374,9 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
         if (nbig) {
             kt.begin(K_SAMPLE);
             k_tile_scan<<<1, 1024, 0, st>>>(w, nbig);
-            k_sample<<<nbig, 256, 0, st>>>(w);
+            // few segments: the pass waits on single blocks, give them more threads
+            const uint32_t seg_threads = nbig < 2 * 148 ? 1024 : 256;
+            k_sample<<<nbig, seg_threads, 0, st>>>(w);
             kt.end(K_SAMPLE);
             kt.begin(K_CLASSIFY);
             k_classify<<<ntiles, TILE_THREADS, 0, st>>>(w, nbig);
@@ -398,7 +400,7 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
             k_scatter<<<ntiles, TILE_THREADS, sizeof(ScatterSmem), st>>>(w, nbig);
             kt.end(K_SCATTER);
             kt.begin(K_CHILDREN);
-            k_children<<<nbig, 256, 0, st>>>(w);
+            k_children<<<nbig, seg_threads, 0, st>>>(w);
             kt.end(K_CHILDREN);
             c->kstat[K_SAMPLE].launches += 2;
             c->kstat[K_CLASSIFY].launches += 1;

@@ -77,14 +77,16 @@ def _rand_tails(n, k, seed):
 
 @pytest.mark.parametrize("case", ["all_equal_big", "long_prefix_big", "few_differ_early",
                                   "one_differs_first_char", "prefix_outliers",
-                                  "outliers_past_one_jump"])
+                                  "outliers_past_one_jump", "many_deep_pairs"])
 def test_common_prefix_jump(pkg, orc, ctx, case):
     """Big segments whose samples all share a prefix jump over it inside the
     pass: all strings equal, a long shared prefix (several jumps of at most
     256 chars), a few strings leaving the prefix early, one string differing
     at char 0, rare strings below and above the prefix (shorter ones, smaller
-    and larger chars: the two prefix buckets, at the segment depth), and
-    outliers that leave a 600-char prefix beyond the first jump."""
+    and larger chars: the two prefix buckets, at the segment depth),
+    outliers that leave a 600-char prefix beyond the first jump, and many
+    pairs of strings sharing 1-3 KB each (several deep groups in one warp
+    window jump together)."""
     if case == "all_equal_big":
         strings = [b"q" * 500] * 100000
     elif case == "long_prefix_big":
@@ -99,6 +101,13 @@ def test_common_prefix_jump(pkg, orc, ctx, case):
     elif case == "outliers_past_one_jump":
         strings = [b"k" * 600 + t for t in _rand_tails(60000, 3, 5)]
         strings += [b"k" * 300 + b"a", b"k" * 270 + b"z", b"k" * 100, b"k" * 700, b"k" * 599]
+    elif case == "many_deep_pairs":
+        rng = np.random.default_rng(6)
+        strings = []
+        for _ in range(700):
+            x = bytes(rng.choice(np.frombuffer(b"ACGT", np.uint8), int(rng.integers(1000, 3000))))
+            strings += [x + b"A", x + b"C" + x[:5]]
+        strings += [bytes(rng.choice(np.frombuffer(b"ACGT", np.uint8), 20)) for _ in range(600)]
     else:
         strings = [b"s" * 40] * 20000 + [b"a"]
     chars, offs = pkg.pack_strings(strings)

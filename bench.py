@@ -98,6 +98,21 @@ def make_workload(pkg, workload: str, n: int, seed_offset: int = 0, alloc=None):
     return pkg.workloads.prefixes(n=n, seed=SEED + seed_offset, **kw)
 
 
+def profiled_traffic(kernel: str, workload: str, n: int):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu
+    summary (profiles/classify_prefixes.md), for the prefix workload at its
+    bench size; None otherwise."""
+    if kernel != "classify" or workload != "prefixes" or n != N_DEFAULT:
+        return None
+    f = ROOT / "profiles" / "classify_prefixes.md"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch_64Mi:"):
+            return int(line.split(":")[1])
+    return None
+
+
 def measured_peak() -> tuple:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -519,7 +534,8 @@ def main():
             "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": nchars + 8 * n,
                     "d2h_bytes_per_step": 4 * n, "ms_per_step": e2e_s * 1e3},
             "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                         "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": profiled_traffic(dom_name, args.workload, n),
                          "peak_kind": peak_kind,
                          "alg_bytes_per_launch": d["alg_bytes"] / max(d["launches"], 1),
                          "ms_per_launch": d["ms"] / max(d["launches"], 1),

@@ -133,7 +133,7 @@ __global__ void __launch_bounds__(THREADS, THREADS <= 64 ? 20 : 4) k_block(Work 
             sm.samp[i] = sm.key[s + (uint32_t)(((h >> 32) * c) >> 32)];
         }
         __syncthreads();
-        if (S <= (uint32_t)THREADS) {
+        if (S <= 64u && S <= (uint32_t)THREADS) {
             // rank sort in place (ties by index): two barriers
             uint64_t x = 0;
             uint32_t r = 0;
@@ -285,8 +285,10 @@ __global__ void __launch_bounds__(THREADS, THREADS <= 64 ? 20 : 4) k_block(Work 
         const bool real = mygrp < 32;
         const uint64_t h = real ? sm.hnd[start] : ~0ull;
         const uint64_t k0 = (real && valid) ? sm.key[start] : 0ull;
+        // stalled groups go to the deep-group list when there is one
         const uint64_t r = warp_window(w, h, mygrp, dep, begin + start, real && valid, k0,
-                                       wscratch[warp]);
+                                       wscratch[warp], w.deep[w.cur ^ 1] ? w.hnd[buf] : nullptr,
+                                       (uint32_t)buf);
         if (real) sm.hnd[start] = r;
     });
     __syncthreads();

@@ -56,9 +56,16 @@ __device__ __forceinline__ uint32_t chunks_equal(const Work& w, uint64_t base, u
 // the key at mydep when has_key. Returns the handle that sorts into this
 // lane's slot; LCPs inside groups are written to lcp[mypos]. scratch is 32
 // words of shared memory private to the warp.
+// With defer_hnd set (the block sorters), groups that stall on a long common
+// prefix are not walked here: their handles go to defer_hnd[mypos] and the
+// group to the deep-group list (segment meta defer_meta), and k_deep finishes
+// them in the next pass, one warp per group, while this block moves on; the
+// slots of such lanes are left to k_deep. jump_first starts with the jump.
 __device__ __forceinline__ uint64_t warp_window(const Work& w, uint64_t myh, uint32_t mygrp,
                                                 uint32_t mydep, uint32_t mypos, bool has_key,
-                                                uint64_t key0, uint32_t* scratch)
+                                                uint64_t key0, uint32_t* scratch,
+                                                uint64_t* defer_hnd = nullptr,
+                                                uint32_t defer_meta = 0, bool jump_first = false)
 {
     const uint32_t lane = threadIdx.x & 31;
     uint32_t mystate = mygrp < 32 ? 0u : 1u;  // 0 active, 1 done
@@ -66,17 +73,34 @@ __device__ __forceinline__ uint64_t warp_window(const Work& w, uint64_t myh, uin
     uint32_t prev_active = __popc(__ballot_sync(0xffffffffu, mystate == 0));
     uint32_t gstarts = __ballot_sync(0xffffffffu, mystate == 0 && mygrp == lane);
     uint32_t prev_groups = __popc(gstarts);
-    uint32_t stalled = 0;  // rounds in a row without progress
+    uint32_t stalled = jump_first ? 2u : 0u;  // rounds in a row without progress
     bool first = true;
     while (true) {
-        const uint32_t A = __ballot_sync(0xffffffffu, mystate == 0);
+        uint32_t A = __ballot_sync(0xffffffffu, mystate == 0);
         if (A == 0) break;
         if (stalled >= 2) {
             // the last two rounds neither split a group nor finished a
-            // string: move every active group to its common prefix, one
-            // group at a time, 64 chunks of 8 bytes per step
+            // string: defer the groups, or move every active group to its
+            // common prefix, one group at a time, 64 chunks of 8 bytes per step
             stalled = 0;
             uint32_t todo = gstarts;
+            if (defer_hnd) {
+                const int nxt = w.cur ^ 1;
+                const bool lead = mystate == 0 && mygrp == lane;
+                const uint32_t same = __match_any_sync(0xffffffffu, mystate == 0 ? mygrp : 64u + lane);
+                uint32_t at = 0xFFFFFFFFu;
+                if (lead) {
+                    at = atomicAdd(w.counters + C_DEEP + nxt, 1u);
+                    if (at < w.deep_cap)
+                        w.deep[nxt][at] = Seg{mypos, (uint32_t)__popc(same), mydep, defer_meta};
+                }
+                const uint32_t D = __ballot_sync(0xffffffffu, lead && at < w.deep_cap);
+                if (mystate == 0 && ((D >> mygrp) & 1u)) {
+                    defer_hnd[mypos] = myh;
+                    mystate = 1;
+                }
+                todo &= ~D;  // groups the full list could not take are walked here
+            }
             while (todo) {
                 const int f = __ffs(todo) - 1;
                 todo &= todo - 1;
@@ -238,6 +262,23 @@ __global__ void __launch_bounds__(32 * TINY_WARPS, 5) k_tiny(Work w, const Seg* 
         const uint64_t r = warp_window(w, h, mygrp, sg.depth, pos, hk, k0, scratch[threadIdx.x >> 5]);
         if (real) w.perm[pos] = h_id(w, r);
     });
+}
+
+// Deep groups handed over by the block sorters: one warp per group, which
+// starts with the common-prefix jump and then sorts the group to the end.
+__global__ void __launch_bounds__(32 * TINY_WARPS) k_deep(Work w, const Seg* list, uint32_t count)
+{
+    __shared__ uint32_t scratch[TINY_WARPS][32];
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t g = blockIdx.x * TINY_WARPS + (threadIdx.x >> 5);
+    if (g >= count) return;  // whole warp
+    const Seg sg = list[g];
+    const bool real = lane < sg.size;
+    const uint32_t pos = sg.begin + lane;
+    const uint64_t h = real ? w.hnd[sg.meta & META_BUF][pos] : ~0ull;
+    const uint64_t r = warp_window(w, h, real ? 0u : 32u, sg.depth, pos, false, 0ull,
+                                   scratch[threadIdx.x >> 5], nullptr, 0u, true);
+    if (real) w.perm[pos] = h_id(w, r);
 }
 
 // the block-sorted size classes (kernels_block.cuh)

@@ -87,7 +87,7 @@ static void set_handle_format(Work& w, bool force_indirect)
 }
 
 struct Sizes {
-    uint64_t n, cap[L_NCLASS], tile_cap;
+    uint64_t n, cap[L_NCLASS], tile_cap, deep_cap;
 };
 
 static Sizes sizes_for(uint64_t n)
@@ -100,6 +100,9 @@ static Sizes sizes_for(uint64_t n)
     s.cap[L_SMALLA] = s.n / (WARP_GROUP_MAX + 1) + 2;
     s.cap[L_TINY] = s.n / 2 + 2;
     s.tile_cap = s.n / TILE + s.cap[L_BIG] + 1;
+    // deep groups hold 2..32 strings; a fuller list falls back to walking
+    // the group inside the block sorter
+    s.deep_cap = s.n / 32 + 64;
     return s;
 }
 
@@ -122,16 +125,17 @@ static uint64_t workspace_bytes(const Sizes& s)
     b += 2 * align256(8ull * 1024 * big);          // trees, splitters
     b += 2 * align256(4ull * MAX_BKT * big);       // bucket counts, starts
     b += 2 * align256(4ull * MAX_BKT * s.tile_cap);  // tile and chunk counts (chunks <= tiles)
+    b += 2 * align256(16 * s.deep_cap);            // deep-group lists
     b += align256(4 * C_COUNT);                    // counters
     return b;
 }
 
 // Kernel classes reported by pssgpu_ctx_kernel_stats.
 enum KClass { K_INIT = 0, K_SAMPLE, K_CLASSIFY, K_BSTART, K_SCATTER, K_CHILDREN, K_TINY,
-              K_SMALLA, K_SMALLB, K_BOUNDARY, K_NCLASS };
+              K_SMALLA, K_SMALLB, K_DEEP, K_BOUNDARY, K_NCLASS };
 static const char* const kclass_name[K_NCLASS] = {
     "init", "sample", "classify", "bstart", "scatter", "children", "tiny",
-    "small256", "small2048", "boundary"};
+    "small256", "small2048", "deep", "boundary"};
 
 struct KStat {
     uint32_t launches = 0;
@@ -241,6 +245,8 @@ static int ensure_workspace(Ctx* c, uint64_t n)
     w.tcount = (uint32_t*)take(4ull * MAX_BKT * s.tile_cap);
     w.ccount = (uint32_t*)take(4ull * MAX_BKT * s.tile_cap);
     w.tile_cap = (uint32_t)s.tile_cap;
+    for (int i = 0; i < 2; ++i) w.deep[i] = (Seg*)take(16 * s.deep_cap);
+    w.deep_cap = (uint32_t)s.deep_cap;
     w.counters = (uint32_t*)take(4 * C_COUNT);
     return PSSGPU_OK;
 }
@@ -317,22 +323,26 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
     }
     uint32_t ntiles = hc[C_NTILES];
     uint32_t nmulti = hc[C_MULTI];
+    uint32_t ndeep = hc[C_DEEP];
     uint64_t small_segments = 0;
     uint32_t err = hc[C_ERR];
     int cur = 0;
-    auto pending = [&]() { return cnt[L_BIG] || cnt[L_TINY] || cnt[L_SMALLA] || cnt[L_SMALLB]; };
+    auto pending = [&]() {
+        return cnt[L_BIG] || cnt[L_TINY] || cnt[L_SMALLA] || cnt[L_SMALLB] || ndeep;
+    };
     while (!err && pending()) {
         const int nxt = cur ^ 1;
         const uint32_t nbig = cnt[L_BIG];
         w.cur = cur;
         PSS_CUDA(cudaMemsetAsync(w.counters + C_PAR * nxt, 0, 4 * C_PAR, st));
         PSS_CUDA(cudaMemsetAsync(w.counters + C_MULTI + nxt, 0, 4, st));
+        PSS_CUDA(cudaMemsetAsync(w.counters + C_DEEP + nxt, 0, 4, st));
         PSS_CUDA(cudaMemsetAsync(w.counters + C_P_FIRST, 0, 4 * (C_P_LAST - C_P_FIRST + 1), st));
         if (nbig && ntiles > c->cap.tile_cap) return fail(PSSGPU_ECUDA, "tile capacity exceeded");
         // small classes: on the side streams (after everything queued on st
         // so far), or serially on st in profile mode so that the per-class
         // events time one class at a time
-        const bool fork = !c->profile && (cnt[L_TINY] || cnt[L_SMALLA] || cnt[L_SMALLB]);
+        const bool fork = !c->profile && (cnt[L_TINY] || cnt[L_SMALLA] || cnt[L_SMALLB] || ndeep);
         if (fork) PSS_CUDA(cudaEventRecord(c->fork_ev, st));
         bool joined[3] = {};
         auto small_stream = [&](int q) -> cudaStream_t {
@@ -358,6 +368,18 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
                 w, w.list[L_SMALLA][cur]);
             kt.end(K_SMALLA);
             c->kstat[K_SMALLA].launches += 1;
+            stats.kernel_launches += 1;
+        }
+        if (ndeep) {
+            // groups the previous pass's block sorters handed over; the same
+            // stream as the block sorters, which add to the other list
+            cudaStream_t s = small_stream(2);
+            kt.begin(K_DEEP);
+            constexpr uint32_t per_block = TINY_WARPS;
+            k_deep<<<(std::min(ndeep, w.deep_cap) + per_block - 1) / per_block, 32 * TINY_WARPS, 0, s>>>(
+                w, w.deep[cur], std::min(ndeep, w.deep_cap));
+            kt.end(K_DEEP);
+            c->kstat[K_DEEP].launches += 1;
             stats.kernel_launches += 1;
         }
         if (cnt[L_SMALLB]) {
@@ -447,6 +469,7 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
         }
         ntiles = hc[C_PAR * nxt + C_NTILES];
         nmulti = hc[C_MULTI + nxt];
+        ndeep = hc[C_DEEP + nxt];
         err = hc[C_ERR];
         cur = nxt;
     }

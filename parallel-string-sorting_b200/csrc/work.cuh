@@ -38,6 +38,7 @@ enum : int {
     C_P_FIRST = C_P_BIG,
     C_P_LAST = C_P_JCHUNKS,
     C_MULTI = 26,     // + parity: big segments of more than CHUNK tiles in the list
+    C_DEEP = 28,      // + parity: length of the deep-group list
     C_COUNT = 32
 };
 
@@ -91,6 +92,12 @@ struct Work {
     uint32_t* ccount;       // [tile_cap][MAX_BKT]: chunk sums, then chunk bases
     uint32_t tile_cap;
     int cur;               // parity of the lists read in this pass
+    // Deep groups: groups of at most 32 strings that a block sorter's warp
+    // window found stuck on a long common prefix, handed to k_deep (one warp
+    // each) in the next pass; double-buffered by pass parity, null when not
+    // allocated
+    Seg* deep[2];
+    uint32_t deep_cap;
     // splitter-tree levels for a big segment of 2^k..2^(k+1)-1 strings
     // (0: the default rule), set from a tuning table
     uint8_t tree_bits_by_size[33];

@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(1024) k_sample(Work w)
 // difference puts it into the first or last bucket, else its key after the
 // prefix goes through the tree (bucket + 1).
 // Tiles of finished (all-equal) segments copy ids and LCPs to the output.
-__global__ void __launch_bounds__(TILE_THREADS, 6) k_classify(Work w, uint32_t nbig)
+__global__ void __launch_bounds__(TILE_THREADS, 1536 / TILE_THREADS) k_classify(Work w, uint32_t nbig)
 {
     __shared__ uint64_t tree[1024];
     __shared__ uint64_t jp[JMAX_CHUNKS];   // the shared chunks as keys

@@ -5,8 +5,8 @@
 
 namespace pssgpu {
 
-constexpr int TILE = 4096;          // strings per classify / scatter tile
-constexpr int TILE_THREADS = 256;   // 16 strings per thread
+constexpr int TILE = 8192;          // strings per classify / scatter tile
+constexpr int TILE_THREADS = 512;   // 16 strings per thread
 constexpr int MAX_TREE_BITS = 10;   // 1023 splitters, 2047 buckets (pS5's DefaultTreebits)
 constexpr int MAX_BKT = 2056;       // bucket slots per big segment: 2047 + the two prefix buckets
 constexpr int JMAX_CHUNKS = 32;     // common-prefix jump of one pass: at most 32 8-byte chunks

@@ -164,6 +164,42 @@ class Clocks:
                 "samples": len(sms), "reasons": sorted(reasons)}
 
 
+class Ranks:
+    """The replicas of a multi-GPU run: one process per GPU, each sorting its
+    own instance. The only collectives are the timing ones: a barrier around
+    the timed region, the maximum of the per-rank step times and the sum of
+    the ranks' chars. device is "cuda" under NCCL, "cpu" under gloo."""
+
+    def __init__(self, dist, world: int, device: str = "cuda"):
+        self.dist, self.world, self.device = dist, world, device
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier()
+
+    def _reduce(self, x: float, op) -> float:
+        if self.world == 1:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    def allmax(self, x: float) -> float:
+        return self._reduce(x, self.dist.ReduceOp.MAX)
+
+    def allsum(self, x: float) -> float:
+        return self._reduce(x, self.dist.ReduceOp.SUM)
+
+
+def replica_value(ranks: Ranks, chars: int, ms: float) -> tuple:
+    """Whole-job char GB/s of a replica run: every rank's chars over the
+    slowest rank's step time. Returns (value, ms_max, total_chars)."""
+    ms_max = ranks.allmax(ms)
+    total = ranks.allsum(float(chars))
+    return total / (ms_max / 1e3) / 1e9, ms_max, total
+
+
 def pinned_alloc(torch):
     def alloc(nbytes, dtype):
         t = torch.empty(int(nbytes), dtype=torch.uint8, pin_memory=True)
@@ -410,23 +446,9 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def allmax(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def allsum(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
+    ranks = Ranks(dist, world, "cuda")
+    barrier = ranks.barrier
+    allmax = ranks.allmax
 
     alloc = pinned_alloc(torch)
     h_chars, h_offs, nchars = make_workload(pkg, args.workload, args.n, rank, alloc)
@@ -495,9 +517,7 @@ def main():
                 a[f] += k[f]
     torch.cuda.synchronize()
     ctx.set_profile(False)
-    ms_max = allmax(ms)
-    total_chars = allsum(float(nchars))
-    value = total_chars / (ms_max / 1e3) / 1e9
+    value, ms_max, total_chars = replica_value(ranks, nchars, ms)
 
     # end to end through the C ABI: host arena in, host permutation out
     h_perm = alloc(4 * n, np.uint32)

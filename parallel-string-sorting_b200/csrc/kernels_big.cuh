@@ -493,22 +493,35 @@ __global__ void __launch_bounds__(TILE_THREADS) k_scatter(Work w, uint32_t nbig)
         const uint32_t p = lo + threadIdx.x + j * TILE_THREADS;
         pk[j] = 0xFFFFFFFFu;
         if (p < hi) {
-            const uint32_t b = w.bkt[p];
+            const uint32_t b = __ldg(w.bkt + p);
             pk[j] = (b << 16) | atomicAdd(&sm.lcount[b], 1u);
         }
     }
     __syncthreads();
     block_scan_array<TILE_THREADS>(sm.lcount, (int)B, sm.tmp);  // counts -> first slots
-    // stage keys in bucket order; pk becomes (bucket << 16) | slot
+    // stage keys in bucket order; pk becomes (bucket << 16) | slot. The
+    // loads of half the thread's elements are issued together (read-only
+    // loads, held in registers) before their shared-memory stores.
     const uint64_t* ikeys = w.keys[buf];
 #pragma unroll
     for (int j = 0; j < PER; ++j) {
         if (pk[j] == 0xFFFFFFFFu) continue;
         const uint32_t b = pk[j] >> 16;
-        const uint32_t slot = sm.lcount[b] + (pk[j] & 0xFFFFu);
-        pk[j] = (b << 16) | slot;
-        sm.stage[slot] = ikeys[lo + threadIdx.x + j * TILE_THREADS];
-        sm.sbkt[slot] = (uint16_t)b;
+        pk[j] = (b << 16) | (sm.lcount[b] + (pk[j] & 0xFFFFu));
+    }
+#pragma unroll
+    for (int h = 0; h < PER; h += PER / 2) {
+        uint64_t v[PER / 2];
+#pragma unroll
+        for (int j = 0; j < PER / 2; ++j)
+            v[j] = pk[h + j] != 0xFFFFFFFFu ? __ldg(ikeys + lo + threadIdx.x + (h + j) * TILE_THREADS) : 0ull;
+#pragma unroll
+        for (int j = 0; j < PER / 2; ++j) {
+            if (pk[h + j] == 0xFFFFFFFFu) continue;
+            const uint32_t slot = pk[h + j] & 0xFFFFu;
+            sm.stage[slot] = v[j];
+            sm.sbkt[slot] = (uint16_t)(pk[h + j] >> 16);
+        }
     }
     __syncthreads();
 #pragma unroll
@@ -530,9 +543,14 @@ __global__ void __launch_bounds__(TILE_THREADS) k_scatter(Work w, uint32_t nbig)
     __syncthreads();
     const uint64_t* ihs = w.hnd[buf];
 #pragma unroll
-    for (int j = 0; j < PER; ++j) {
-        if (pk[j] == 0xFFFFFFFFu) continue;
-        sm.stage[pk[j] & 0xFFFFu] = ihs[lo + threadIdx.x + j * TILE_THREADS];
+    for (int h = 0; h < PER; h += PER / 2) {
+        uint64_t v[PER / 2];
+#pragma unroll
+        for (int j = 0; j < PER / 2; ++j)
+            v[j] = pk[h + j] != 0xFFFFFFFFu ? __ldg(ihs + lo + threadIdx.x + (h + j) * TILE_THREADS) : 0ull;
+#pragma unroll
+        for (int j = 0; j < PER / 2; ++j)
+            if (pk[h + j] != 0xFFFFFFFFu) sm.stage[pk[h + j] & 0xFFFFu] = v[j];
     }
     __syncthreads();
     uint64_t* ohs = w.hnd[buf ^ 1];

@@ -95,8 +95,8 @@ __global__ void __launch_bounds__(THREADS, THREADS <= 64 ? 20 : 4) k_block(Work 
     }
     const bool valid0 = sg.meta & META_VALID;
     for (uint32_t i = threadIdx.x; i < m; i += THREADS) {
-        sm.hnd[i] = ghs[begin + i];
-        if (valid0) sm.key[i] = w.keys[buf][begin + i];
+        sm.hnd[i] = __ldg(ghs + begin + i);
+        if (valid0) sm.key[i] = __ldg(w.keys[buf] + begin + i);
     }
     if (threadIdx.x == 0) {
         sm.ng = 0;

@@ -136,7 +136,7 @@ int pssgpu_sort_batch_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t n
 
 /* Tuning table: splitter-tree levels (1..10) for big segments of
  * 2^k .. 2^(k+1)-1 strings, k < count <= 33; 0 keeps the default rule
- * (about 16 strings per bucket). Written by the autotuner. */
+ * (about 8 strings per bucket). Written by the autotuner. */
 int pssgpu_ctx_set_tree_bits(pssgpu_ctx* ctx, const uint8_t* tree_bits, int count);
 
 /* ---- serving ---------------------------------------------------------------

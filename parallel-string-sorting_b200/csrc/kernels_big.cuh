@@ -40,12 +40,12 @@ __device__ __forceinline__ int find_tile_seg(const uint32_t* tile_start, int nbi
 
 __device__ __forceinline__ uint32_t tree_bits_for(const Work& w, uint32_t m)
 {
-    // a tuned value for this size class, else about 16 strings per '<'
+    // a tuned value for this size class, else about 8 strings per '<'
     // bucket; at most pS5's 10 tree levels
     const int lg = 31 - __clz((int)m);
     const uint32_t tuned = w.tree_bits_by_size[lg];
     if (tuned) return min((uint32_t)MAX_TREE_BITS, tuned);
-    return (uint32_t)min(MAX_TREE_BITS, max(1, lg - 4));
+    return (uint32_t)min(MAX_TREE_BITS, max(1, lg - 3));
 }
 
 __global__ void k_tile_scan(Work w, uint32_t nbig)

@@ -23,7 +23,7 @@ from . import workloads
 from .api import Context
 
 TABLE_PATH = Path(__file__).resolve().parent / "tuning_b200.json"
-CLASSES = range(11, 21)  # big segments: more than 2048 strings
+CLASSES = range(10, 21)  # big segments: more than 1024 strings
 
 
 def _class_batch(k: int, strings: int, seed: int):

@@ -297,5 +297,7 @@ __global__ void __launch_bounds__(THREADS, THREADS <= 64 ? 20 : 4) k_block(Work 
 
 #define K_BLOCK_A k_block<SMALL_A, SMALL_A_THREADS>
 #define K_BLOCK_B k_block<SMALL_MAX, SMALL_THREADS>
+// the allocation-free entry point's sorter: up to 2048 strings in one block
+#define K_BLOCK_NOALLOC k_block<2048, 256>
 
 }  // namespace pssgpu

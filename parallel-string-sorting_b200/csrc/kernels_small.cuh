@@ -9,7 +9,7 @@
 // Size classes (push_seg in kernels_big.cuh picks the list):
 //   k_tiny            <= 32 strings (several segments share one warp window)
 //   k_block<256,128>  <= 256 strings, one block (kernels_block.cuh)
-//   k_block<2048,256> <= 2048 strings, one block (kernels_block.cuh)
+//   k_block<1024,256> <= 1024 strings, one block (kernels_block.cuh)
 //
 // A warp window holds up to 32 strings from one or more independent groups.
 // Each lane owns one output slot (a position of the permutation); groups

@@ -135,7 +135,7 @@ enum KClass { K_INIT = 0, K_SAMPLE, K_CLASSIFY, K_BSTART, K_SCATTER, K_CHILDREN,
               K_SMALLA, K_SMALLB, K_DEEP, K_BOUNDARY, K_NCLASS };
 static const char* const kclass_name[K_NCLASS] = {
     "init", "sample", "classify", "bstart", "scatter", "children", "tiny",
-    "small256", "small2048", "deep", "boundary"};
+    "small256", "small1024", "deep", "boundary"};
 
 struct KStat {
     uint32_t launches = 0;
@@ -1144,8 +1144,8 @@ extern "C" int pssgpu_sort_device_noalloc(const uint8_t* d_chars, uint64_t nchar
             void* p = nullptr;
             if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p)
                 return fail(PSSGPU_ECUDA, "symbol lookup");
-            if (cudaFuncSetAttribute(K_BLOCK_B, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)sizeof(BlockSmem<SMALL_MAX>)) != cudaSuccess)
+            if (cudaFuncSetAttribute(K_BLOCK_NOALLOC, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sizeof(BlockSmem<2048>)) != cudaSuccess)
                 return fail(PSSGPU_ECUDA, "smem limit");
             g_noalloc_addr[dev] = static_cast<NoAllocScratch*>(p);
         }
@@ -1170,7 +1170,7 @@ extern "C" int pssgpu_sort_device_noalloc(const uint8_t* d_chars, uint64_t nchar
     w.cur = 0;
     set_handle_format(w, false);
     k_noalloc_prep<<<1, SMALL_THREADS, 0, st>>>(w);
-    K_BLOCK_B<<<1, SMALL_THREADS, sizeof(BlockSmem<SMALL_MAX>), st>>>(w, &scratch->seg);
+    K_BLOCK_NOALLOC<<<1, 256, sizeof(BlockSmem<2048>), st>>>(w, &scratch->seg);
     uint32_t err = 0;
     if (cudaGetLastError() != cudaSuccess ||
         cudaMemcpyAsync(&err, scratch->counters + C_ERR, 4, cudaMemcpyDeviceToHost, st) !=

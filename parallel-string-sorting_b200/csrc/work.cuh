@@ -10,7 +10,7 @@ constexpr int TILE_THREADS = 512;   // 16 strings per thread
 constexpr int MAX_TREE_BITS = 10;   // 1023 splitters, 2047 buckets (pS5's DefaultTreebits)
 constexpr int MAX_BKT = 2056;       // bucket slots per big segment: 2047 + the two prefix buckets
 constexpr int JMAX_CHUNKS = 32;     // common-prefix jump of one pass: at most 32 8-byte chunks
-constexpr int SMALL_MAX = 2048;     // largest segment the block sorter takes
+constexpr int SMALL_MAX = 1024;     // largest segment the block sorters take
 constexpr int SMALL_THREADS = 256;
 constexpr int WARP_GROUP_MAX = 32;  // groups this small are finished by one warp
 constexpr int FINAL_INLINE = 64;    // equal-string buckets this small are copied inline

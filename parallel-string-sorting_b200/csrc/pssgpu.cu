@@ -330,7 +330,13 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
     auto pending = [&]() {
         return cnt[L_BIG] || cnt[L_TINY] || cnt[L_SMALLA] || cnt[L_SMALLB] || ndeep;
     };
+    // Every pass takes each open segment at least 8 chars deeper or splits
+    // it; the limit turns a pass structure that stops making progress into
+    // an error instead of an endless loop.
+    constexpr uint32_t MAX_PASSES = 1u << 20;
+    uint32_t npass = 0;
     while (!err && pending()) {
+        if (++npass > MAX_PASSES) return fail(PSSGPU_ETIMEOUT, "pass limit exceeded");
         const int nxt = cur ^ 1;
         const uint32_t nbig = cnt[L_BIG];
         w.cur = cur;

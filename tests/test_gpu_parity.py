@@ -58,8 +58,10 @@ def test_random_vs_oracle(pkg, orc, ctx, n, lmin, lmax, alpha, seed):
     [b"\xff" * 40] * 3000 + [b"\xff" * 39],
     [b"a" * k for k in range(0, 3000, 7)],
     [b"z" * 2000 + bytes([97 + i % 26]) + b"q" * (i % 5) for i in range(5000)],
+    [b"w" * 100 + bytes([97 + i % 26, 97 + (i // 26) % 26]) for i in range(3000)],
+    [bytes([97 + i % 3]) * (1 + i % 17) for i in range(4000)],
 ], ids=["empty", "one", "two", "all_empty", "all_equal", "ff_bytes", "prefix_chain",
-        "deep_shared_prefix"])
+        "deep_shared_prefix", "split_class_tied", "split_class_runs"])
 def test_edge_cases(pkg, orc, ctx, strings):
     chars, offs = pkg.pack_strings(strings)
     if len(strings) == 0:

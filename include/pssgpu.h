@@ -36,7 +36,7 @@ extern "C" {
 #define PSSGPU_EINVAL 1   /* bad argument: sizes, alignment, unterminated arena */
 #define PSSGPU_ENOMEM 2   /* device or host allocation failed */
 #define PSSGPU_ECUDA 3    /* a CUDA runtime call failed */
-#define PSSGPU_ETIMEOUT 4 /* a bounded device-side wait gave up */
+#define PSSGPU_ETIMEOUT 4 /* a bounded wait or the pass limit of a sort gave up */
 #define PSSGPU_ENODEV 5   /* no usable CUDA device */
 #define PSSGPU_EBUDGET 6  /* request exceeds the configured memory budget */
 

@@ -161,6 +161,9 @@ struct Ctx {
     pssgpu_stats stats{};
     // profile mode: events around every kernel class, per-class totals
     bool profile = false;
+    // PSSGPU_TRACE set in the environment: one line per pass on stderr
+    // (segments, tiles, strings per class; kernel-class times in profile mode)
+    bool trace = false;
     // carry bare ids and read offsets through offs[] (the path taken when
     // id and offset do not fit one 64-bit handle); settable for testing
     bool indirect_handles = false;
@@ -184,6 +187,7 @@ struct KTimer {
     Ctx* c;
     cudaStream_t st;
     bool used[K_NCLASS] = {};
+    float pass_ms[K_NCLASS] = {};  // times of the last collected pass
     void begin(int k)
     {
         if (c->profile) { cudaEventRecord(c->kev[2 * k], st); used[k] = true; }
@@ -197,10 +201,12 @@ struct KTimer {
     {
         if (!c->profile) return;
         for (int k = 0; k < K_NCLASS; ++k) {
+            pass_ms[k] = 0;
             if (!used[k]) continue;
             float ms = 0;
             cudaEventElapsedTime(&ms, c->kev[2 * k], c->kev[2 * k + 1]);
             c->kstat[k].ms += ms;
+            pass_ms[k] = ms;
             used[k] = false;
         }
     }
@@ -468,6 +474,19 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
                 small_segments += cnt[lk[q]];
             }
             c->kstat[K_CHILDREN].strings += big;
+            if (c->trace) {
+                std::fprintf(stderr,
+                             "pssgpu pass %u: big %u segs %u tiles %llu strings (%llu stale, %llu tied, "
+                             "%llu jump chunks, %llu final) | tiny %u/%u small256 %u/%u small1024 %u/%u deep %u",
+                             npass, nbig, ntiles, (unsigned long long)big, (unsigned long long)stale,
+                             (unsigned long long)hc[C_P_TIE], (unsigned long long)jch, (unsigned long long)fin,
+                             cnt[L_TINY], nstr[L_TINY], cnt[L_SMALLA], nstr[L_SMALLA], cnt[L_SMALLB],
+                             nstr[L_SMALLB], ndeep);
+                if (c->profile)
+                    for (int k = 0; k < K_NCLASS; ++k)
+                        if (kt.pass_ms[k] > 0) std::fprintf(stderr, " %s %.3f", kclass_name[k], kt.pass_ms[k]);
+                std::fprintf(stderr, "\n");
+            }
         }
         for (int k = 0; k < L_NCLASS; ++k) {
             cnt[k] = hc[C_PAR * nxt + k];
@@ -519,6 +538,7 @@ static int ctx_create(int device, Ctx** out)
     if (device < 0 || device >= count) return fail(PSSGPU_EINVAL, "device index out of range");
     PSS_CUDA(cudaSetDevice(device));
     Ctx* c = new Ctx;
+    c->trace = std::getenv("PSSGPU_TRACE") != nullptr;
     c->device = device;
     bool ok = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) == cudaSuccess &&
               cudaEventCreate(&c->ev0) == cudaSuccess && cudaEventCreate(&c->ev1) == cudaSuccess &&

@@ -117,6 +117,59 @@ def test_common_prefix_jump(pkg, orc, ctx, case):
     check_against_oracle(orc, chars, offs, perm, lcp)
 
 
+def _group_strings(case):
+    """Strings in groups that share a long prefix behind their first 8 chars,
+    with members that leave the prefix early (shorter, smaller or larger
+    chars at every position), shuffled."""
+    rng = np.random.default_rng({"groups_outliers": 41, "many_groups": 42, "groups_behind_jump": 43,
+                                 "groups_indirect": 44, "groups_offsets_shuffled": 45}[case])
+    lower = np.frombuffer(b"abcdefghijklmnopqrstuvwxyz", np.uint8)
+    ngroups = 400 if case == "many_groups" else 40
+    head = b"commonhead:0123456789" if case == "groups_behind_jump" else b""
+    strings = []
+    for g in range(ngroups):
+        pre = head + bytes(rng.choice(lower, int(rng.integers(20, 120))))
+        size = int(rng.integers(50, 300)) if case == "many_groups" else int(rng.integers(300, 4000))
+        for _ in range(size):
+            strings.append(pre + bytes(rng.choice(lower[:3], int(rng.integers(0, 4)))))
+        for pos in range(len(head) + 1, len(pre)):
+            if case == "many_groups" and pos % 7:
+                continue
+            strings.append(pre[:pos])
+            strings.append(pre[:pos] + b"\x01" + pre[pos + 1:])
+            strings.append(pre[:pos] + b"\xff" + pre[pos + 1:])
+            strings.append(pre[:pos] + bytes([pre[pos] - 1]) + b"zz")
+            strings.append(pre[:pos] + bytes([pre[pos] + 1]))
+    order = rng.permutation(len(strings))
+    return [strings[i] for i in order]
+
+
+@pytest.mark.parametrize("case", ["groups_outliers", "many_groups", "groups_behind_jump",
+                                  "groups_indirect", "groups_offsets_shuffled"])
+def test_group_jumps(pkg, orc, ctx, case):
+    """'=' buckets whose samples share more chunks behind the splitter take a
+    jump of their own: members that leave the group's chunks below or above
+    (at every position, ending early or with other chars) and members that
+    match them; more groups than a segment keeps; groups behind a common-prefix
+    jump of the whole input; the same with offsets read through the offset
+    array; offsets in an order unrelated to the arena (the first pass cannot
+    stage a warp's strings)."""
+    strings = _group_strings(case)
+    chars, offs = pkg.pack_strings(strings)
+    if case == "groups_offsets_shuffled":
+        offs = offs[np.random.default_rng(46).permutation(len(offs))].copy()
+    if case == "groups_indirect":
+        c = pkg.Context(0)
+        try:
+            c.set_option(c.OPT_INDIRECT_HANDLES, 1)
+            perm, lcp = c.sort_host(chars, offs, lcp=True)
+        finally:
+            c.close()
+    else:
+        perm, lcp = ctx.sort_host(chars, offs, lcp=True)
+    check_against_oracle(orc, chars, offs, perm, lcp)
+
+
 def test_deep_repeats_suffixes(pkg, orc, ctx):
     # a periodic text: suffix LCPs up to the text length
     text = (b"abcab" * 4000)[:19999] + b"\0"

@@ -12,6 +12,9 @@ instance.
   e2e        the same metric through the C ABI with host buffers: the H2D copy
              of arena + offsets from pinned memory and the D2H copy of the
              permutation are inside every timed step
+  e2e_text   the same through the text entry point: only the text (NUL ->
+             newline, or the DNA text for suffixes) is copied; lines and
+             offsets are made on the device
   roofline   the kernel class with the largest device time: its algorithmic
              bytes / its summed event time against the measured HBM copy
              bandwidth; roofline_sort does the same for the whole sort with
@@ -544,6 +547,41 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(min(args.cpu_sample, n), args.workload)
 
+    # the same end to end through the text entry point: only the text goes to
+    # the device (no offset array) and is split there, as psstest's loader
+    # splits a file (lines; suffixes for the DNA workload). The host arena
+    # becomes that text in place (NUL -> newline), after every other use.
+    e2e_text = None
+    if args.e2e_steps > 0:
+        import ctypes
+        mode = 1 if args.workload == "dna" else 0
+        if mode == 0:
+            for i in range(0, nchars, 1 << 28):
+                seg = h_chars[i:min(i + (1 << 28), nchars)]
+                seg[seg == 0] = 10
+        h_perm = alloc(4 * n, np.uint32)
+        nout = ctypes.c_uint64(0)
+        lib = pkg._native.gpu()
+
+        def text_step():
+            rc = lib.pssgpu_sort_text_host(ctx._h, h_chars.ctypes.data, nchars, mode,
+                                           h_perm.ctypes.data, None, n, ctypes.byref(nout))
+            if rc or nout.value != n:
+                raise RuntimeError(f"pssgpu_sort_text_host: status {rc}, {nout.value} strings")
+        text_step()  # warm
+        t_times = []
+        for _ in range(args.e2e_steps):
+            barrier()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            text_step()
+            t_times.append(time.perf_counter() - t0)
+        t_s = allmax(sum(t_times) / len(t_times))
+        e2e_text = {"value": total_chars / t_s / 1e9, "unit": "GB/s", "h2d_bytes_per_step": nchars,
+                    "d2h_bytes_per_step": 4 * n, "ms_per_step": t_s * 1e3,
+                    "entry": "pssgpu_sort_text_host, " + ("suffixes" if mode else "lines")}
+        del h_perm
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world,
@@ -553,6 +591,7 @@ def main():
             "strings_per_s": world * n / (ms_max / 1e3),
             "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": nchars + 8 * n,
                     "d2h_bytes_per_step": 4 * n, "ms_per_step": e2e_s * 1e3},
+            "e2e_text": e2e_text,
             "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak,
                          "traffic": profiled_traffic(dom_name, args.workload, n),

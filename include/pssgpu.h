@@ -117,6 +117,36 @@ int pssgpu_sort_device(pssgpu_ctx* ctx, const uint8_t* d_chars,
                        uint64_t nchars, const uint64_t* d_offs, uint64_t n,
                        uint32_t* d_perm, uint32_t* d_lcp, void* stream);
 
+/* ---- device-side input preparation ---------------------------------------
+ * A text becomes an arena and its offset array on the device, as psstest's
+ * plain-file loader and pointer-array build do it on the host
+ * (src/tools/input.hpp:255-297, src/psstest.cpp:479-518):
+ *   PSSGPU_TEXT_LINES     every '\n' and NUL byte ends a string and becomes
+ *                         NUL; n = 1 + such bytes in text[0, size - 1)
+ *   PSSGPU_TEXT_SUFFIXES  every position starts a string; n = size
+ * Both force the last byte, text[size - 1], to NUL.
+ *
+ * pssgpu_prepare_text_device: in place on device buffers. d_text must be
+ * 8-byte aligned, readable and writable for size + PSSGPU_ARENA_PAD bytes,
+ * the pad bytes zero. d_offs receives the n offsets. *n_out is set to n; if
+ * n exceeds offs_cap the call returns PSSGPU_EINVAL and changes nothing. The
+ * result sorts with pssgpu_sort_device(ctx, d_text, size, d_offs, n, ...).
+ *
+ * pssgpu_sort_text_host: copies the host text (size bytes, left unchanged)
+ * to the device, prepares it there and sorts it: perm receives the string
+ * ids (their order in the text), lcp (may be NULL) the LCP array, both for
+ * the n strings; cap is their capacity (n > cap: PSSGPU_EINVAL with *n_out =
+ * n, nothing written). No counterpart in the reference's sorter interface:
+ * it replaces psstest's loading and pointer-array steps before a run. */
+#define PSSGPU_TEXT_LINES 0
+#define PSSGPU_TEXT_SUFFIXES 1
+int pssgpu_prepare_text_device(pssgpu_ctx* ctx, uint8_t* d_text, uint64_t size,
+                               int mode, uint64_t* d_offs, uint64_t offs_cap,
+                               uint64_t* n_out, void* stream);
+int pssgpu_sort_text_host(pssgpu_ctx* ctx, const uint8_t* text, uint64_t size,
+                          int mode, uint32_t* perm, uint32_t* lcp, uint64_t cap,
+                          uint64_t* n_out);
+
 /* ---- batched sorts ---------------------------------------------------------
  * Many independent sort instances in one call: every instance becomes a
  * root segment of the same device passes, so instances of any size share

@@ -206,3 +206,41 @@ def ref_find_bkt(splitters_1023, keys) -> np.ndarray:
     out = np.zeros(keys.shape[0], dtype=np.uint16)
     ref_lib().ps5ref_find_bkt(s.ctypes.data, keys.ctypes.data, keys.shape[0], out.ctypes.data)
     return out
+
+
+def split_text(text, suffix: bool = False):
+    """psstest's plain-file loading and string pointer array, restated for
+    the device-side text preparation: src/tools/input.hpp:255-297 (every
+    '\\n' or NUL byte becomes NUL and, unless it is the last byte, starts a
+    new string; the last byte is forced to NUL; suffix mode leaves the bytes
+    and counts every position) and src/psstest.cpp:479-518 (strings start at
+    0 and behind every NUL; suffix mode: at every position).
+
+    Returns (arena: u8[size + 16], the text after the rewrite plus zero pad;
+    offsets: u64[n])."""
+    t = np.frombuffer(bytes(text), dtype=np.uint8).copy() if not isinstance(text, np.ndarray) \
+        else np.ascontiguousarray(text, dtype=np.uint8).copy()
+    size = t.shape[0]
+    if size == 0:
+        return np.zeros(16, np.uint8), np.zeros(0, np.uint64)
+    if suffix:
+        starts = np.arange(size, dtype=np.uint64)
+    else:
+        sep = (t == 10) | (t == 0)
+        t[sep] = 0
+        starts = np.concatenate([np.zeros(1, np.uint64),
+                                 np.flatnonzero(sep[: size - 1]).astype(np.uint64) + 1])
+    t[size - 1] = 0
+    return np.concatenate([t, np.zeros(16, np.uint8)]), starts
+
+
+def sorted_output(chars, offs, ids) -> bytes:
+    """psstest's -o output (src/psstest.cpp:696-703): every string of the
+    sorted order followed by a newline."""
+    raw = bytes(chars)
+    out = []
+    for i in np.asarray(ids):
+        o = int(offs[int(i)])
+        e = raw.index(b"\0", o)
+        out.append(raw[o:e] + b"\n")
+    return b"".join(out)

@@ -151,6 +151,38 @@ class Context:
                                                 addr(perm), addr(lcp), s))
 
 
+    TEXT_LINES = 0
+    TEXT_SUFFIXES = 1
+
+    def sort_text_host(self, text, mode: int = 0, lcp: bool = True):
+        """Sort the lines (mode TEXT_LINES) or suffixes (TEXT_SUFFIXES) of a
+        host text, split on the device as psstest's loader splits a file;
+        returns (perm u32[n], lcp u32[n] or None), ids in text order."""
+        t = np.ascontiguousarray(np.frombuffer(text, dtype=np.uint8) if isinstance(text, (bytes, bytearray))
+                                 else text, dtype=np.uint8)
+        size = t.shape[0]
+        n = C.c_uint64(0)
+        cap = size  # n <= size in both modes
+        perm = np.empty(max(cap, 1), dtype=np.uint32)
+        lcp_a = np.zeros(max(cap, 1), dtype=np.uint32) if lcp else None
+        _check(_native.gpu().pssgpu_sort_text_host(self._h, _ptr(t), size, mode, _ptr(perm),
+                                                   _ptr(lcp_a), cap, C.byref(n)))
+        k = n.value
+        return perm[:k], (lcp_a[:k] if lcp else None)
+
+    def prepare_text_device(self, text, size: int, mode: int, offs, stream=None) -> int:
+        """In place on device buffers (torch tensors or raw pointers): the
+        text becomes an arena, offs receives the string offsets; returns n."""
+        def addr(t):
+            return t if isinstance(t, int) else t.data_ptr()
+        cap = offs.numel() if hasattr(offs, "numel") else 0
+        n = C.c_uint64(0)
+        s = None if stream is None else (stream if isinstance(stream, int) else stream.cuda_stream)
+        _check(_native.gpu().pssgpu_prepare_text_device(self._h, addr(text), size, mode,
+                                                        addr(offs), cap, C.byref(n), s))
+        return n.value
+
+
 _default: Optional[Context] = None
 
 

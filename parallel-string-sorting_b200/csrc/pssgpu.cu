@@ -19,6 +19,7 @@
 #include "../../include/pssgpu.h"
 #include "kernels_big.cuh"
 #include "kernels_block.cuh"
+#include "prepare.cuh"
 
 namespace pssgpu {
 
@@ -158,6 +159,12 @@ struct Ctx {
     // staging for the host entry points
     unsigned char* io = nullptr;
     uint64_t io_bytes = 0;
+    // text entry point: offsets, perm and lcp beside the text in io;
+    // chunk counts and bases of the line split
+    unsigned char* io2 = nullptr;
+    uint64_t io2_bytes = 0;
+    unsigned char* prep = nullptr;
+    uint64_t prep_bytes = 0;
     pssgpu_stats stats{};
     // profile mode: events around every kernel class, per-class totals
     bool profile = false;
@@ -563,6 +570,8 @@ static void ctx_destroy(Ctx* c)
     cudaSetDevice(c->device);
     if (c->ws) cudaFree(c->ws);
     if (c->io) cudaFree(c->io);
+    if (c->io2) cudaFree(c->io2);
+    if (c->prep) cudaFree(c->prep);
     if (c->inst_buf) cudaFree(c->inst_buf);
     if (c->host_counters) cudaFreeHost(c->host_counters);
     if (c->ev0) cudaEventDestroy(c->ev0);
@@ -578,22 +587,78 @@ static void ctx_destroy(Ctx* c)
     delete c;
 }
 
-static int ensure_io(Ctx* c, uint64_t bytes)
+// A device buffer of at least `bytes`, grown (contents dropped) when short.
+static int ensure_buf(unsigned char** buf, uint64_t* have, uint64_t bytes)
 {
-    if (c->io && bytes <= c->io_bytes) return PSSGPU_OK;
-    if (c->io) {
-        cudaFree(c->io);
-        c->io = nullptr;
+    if (*buf && bytes <= *have) return PSSGPU_OK;
+    if (*buf) {
+        cudaFree(*buf);
+        *buf = nullptr;
+        *have = 0;
     }
-    PSS_CUDA(cudaMalloc(&c->io, bytes));
-    c->io_bytes = bytes;
+    PSS_CUDA(cudaMalloc(buf, bytes));
+    *have = bytes;
     return PSSGPU_OK;
 }
+
+static int ensure_io(Ctx* c, uint64_t bytes) { return ensure_buf(&c->io, &c->io_bytes, bytes); }
 
 static int check_args(uint64_t nchars, uint64_t n)
 {
     if (n > PSSGPU_MAX_STRINGS) return fail(PSSGPU_EINVAL, "too many strings for one call");
     if (n > 0 && nchars == 0) return fail(PSSGPU_EINVAL, "empty arena with strings");
+    return PSSGPU_OK;
+}
+
+// Text on the device -> arena + offsets (prepare.cuh), in two steps: the
+// string count (for lines: separators per chunk and their scan, kept in
+// c->prep for the second step), then the offsets and the NUL rewrite. Caller
+// holds c->mu; d_text is 8-byte aligned and readable / writable for size +
+// PSSGPU_ARENA_PAD bytes; size > 0.
+static int text_count(Ctx* c, const uint8_t* d_text, uint64_t size, int mode, uint64_t* n_out,
+                      cudaStream_t st)
+{
+    if (mode == PSSGPU_TEXT_SUFFIXES) {
+        *n_out = size;
+        return PSSGPU_OK;
+    }
+    const uint64_t nchunk = (size - 1 + PREP_CHUNK - 1) / PREP_CHUNK;
+    if (nchunk > 0xFFFFFFFFull) return fail(PSSGPU_EINVAL, "text too large");
+    const uint64_t b_cnt = align256(4 * nchunk), b_base = align256(8 * nchunk);
+    int rc;
+    if ((rc = ensure_buf(&c->prep, &c->prep_bytes, b_cnt + b_base + 256))) return rc;
+    uint64_t total = 0;
+    if (nchunk) {
+        uint32_t* d_cnt = (uint32_t*)c->prep;
+        uint64_t* d_base = (uint64_t*)(c->prep + b_cnt);
+        uint64_t* d_total = (uint64_t*)(c->prep + b_cnt + b_base);
+        uint64_t* h_total = reinterpret_cast<uint64_t*>(c->host_counters);
+        k_text_count<<<(unsigned)nchunk, PREP_THREADS, 0, st>>>(d_text, size, d_cnt);
+        k_text_scan<<<1, 1024, 0, st>>>(d_cnt, (uint32_t)nchunk, d_base, d_total);
+        PSS_CUDA(cudaGetLastError());
+        PSS_CUDA(cudaMemcpyAsync(h_total, d_total, 8, cudaMemcpyDeviceToHost, st));
+        PSS_CUDA(cudaStreamSynchronize(st));
+        total = *h_total;
+    }
+    *n_out = 1 + total;
+    return PSSGPU_OK;
+}
+
+// The second step, after text_count on the same text: d_offs holds n entries.
+static int text_write(Ctx* c, uint8_t* d_text, uint64_t size, int mode, uint64_t* d_offs,
+                      cudaStream_t st)
+{
+    if (mode == PSSGPU_TEXT_SUFFIXES) {
+        const uint64_t blocks = std::min<uint64_t>((size + 255) / 256, 148ull * 16);
+        k_text_suffixes<<<(unsigned)blocks, 256, 0, st>>>(d_offs, size);
+    } else {
+        const uint64_t nchunk = (size - 1 + PREP_CHUNK - 1) / PREP_CHUNK;
+        const uint64_t* d_base = (const uint64_t*)(c->prep + align256(4 * nchunk));
+        PSS_CUDA(cudaMemsetAsync(d_offs, 0, 8, st));  // string 0 starts at 0
+        if (nchunk) k_text_lines<<<(unsigned)nchunk, PREP_THREADS, 0, st>>>(d_text, size, d_base, d_offs);
+    }
+    PSS_CUDA(cudaGetLastError());
+    PSS_CUDA(cudaMemsetAsync(d_text + size - 1, 0, 1, st));  // the last string ends there
     return PSSGPU_OK;
 }
 
@@ -1001,6 +1066,69 @@ int pssgpu_sort_host(pssgpu_ctx* ctx, const uint8_t* chars, uint64_t nchars,
     Ctx* c = reinterpret_cast<Ctx*>(ctx);
     std::lock_guard<std::mutex> lk(c->mu);
     return sort_host_locked(c, chars, nchars, offs, n, perm, lcp);
+}
+
+int pssgpu_prepare_text_device(pssgpu_ctx* ctx, uint8_t* d_text, uint64_t size, int mode,
+                               uint64_t* d_offs, uint64_t offs_cap, uint64_t* n_out, void* stream)
+{
+    if (!ctx || !n_out) return fail(PSSGPU_EINVAL, "null context or count");
+    *n_out = 0;
+    if (mode != PSSGPU_TEXT_LINES && mode != PSSGPU_TEXT_SUFFIXES)
+        return fail(PSSGPU_EINVAL, "unknown text mode");
+    if (size == 0) return PSSGPU_OK;
+    if (!d_text || !d_offs) return fail(PSSGPU_EINVAL, "null buffer");
+    if (((uintptr_t)d_text & 7) != 0) return fail(PSSGPU_EINVAL, "text not 8-byte aligned");
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    std::lock_guard<std::mutex> lk(c->mu);
+    PSS_CUDA(cudaSetDevice(c->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    uint64_t n = 0;
+    int rc = text_count(c, d_text, size, mode, &n, st);
+    if (rc) return rc;
+    *n_out = n;
+    if (n > offs_cap) return fail(PSSGPU_EINVAL, "offset array too small");
+    if ((rc = text_write(c, d_text, size, mode, d_offs, st))) return rc;
+    PSS_CUDA(cudaStreamSynchronize(st));
+    return PSSGPU_OK;
+}
+
+int pssgpu_sort_text_host(pssgpu_ctx* ctx, const uint8_t* text, uint64_t size, int mode,
+                          uint32_t* perm, uint32_t* lcp, uint64_t cap, uint64_t* n_out)
+{
+    if (!ctx || !n_out) return fail(PSSGPU_EINVAL, "null context or count");
+    *n_out = 0;
+    if (mode != PSSGPU_TEXT_LINES && mode != PSSGPU_TEXT_SUFFIXES)
+        return fail(PSSGPU_EINVAL, "unknown text mode");
+    if (size == 0) return PSSGPU_OK;
+    if (!text || !perm) return fail(PSSGPU_EINVAL, "null buffer");
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    std::lock_guard<std::mutex> lk(c->mu);
+    PSS_CUDA(cudaSetDevice(c->device));
+    cudaStream_t st = c->stream;
+    const uint64_t b_text = align256(size + PSSGPU_ARENA_PAD);
+    int rc;
+    if ((rc = ensure_io(c, b_text))) return rc;
+    uint8_t* d_text = c->io;
+    PSS_CUDA(cudaMemcpyAsync(d_text, text, size, cudaMemcpyHostToDevice, st));
+    PSS_CUDA(cudaMemsetAsync(d_text + size, 0, b_text - size, st));
+    uint64_t n = 0;
+    if ((rc = text_count(c, d_text, size, mode, &n, st))) return rc;
+    *n_out = n;
+    if (n > cap) return fail(PSSGPU_EINVAL, "result arrays too small");
+    if ((rc = check_args(size, n))) return rc;
+    const uint64_t b_offs = align256(8 * n), b_perm = align256(4 * n);
+    const uint64_t b_lcp = lcp ? align256(4 * n) : 0;
+    if ((rc = ensure_buf(&c->io2, &c->io2_bytes, b_offs + b_perm + b_lcp))) return rc;
+    uint64_t* d_offs = (uint64_t*)c->io2;
+    uint32_t* d_perm = (uint32_t*)(c->io2 + b_offs);
+    uint32_t* d_lcp = lcp ? (uint32_t*)(c->io2 + b_offs + b_perm) : nullptr;
+    if ((rc = text_write(c, d_text, size, mode, d_offs, st))) return rc;
+    if ((rc = run_sort(c, d_text, size, d_offs, (uint32_t)n, d_perm, d_lcp, st))) return rc;
+    PSS_CUDA(cudaMemcpyAsync(perm, d_perm, 4 * n, cudaMemcpyDeviceToHost, st));
+    if (lcp && n > 1)
+        PSS_CUDA(cudaMemcpyAsync(lcp + 1, d_lcp + 1, 4 * (n - 1), cudaMemcpyDeviceToHost, st));
+    PSS_CUDA(cudaStreamSynchronize(st));
+    return PSSGPU_OK;
 }
 
 int pssgpu_sort_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nchars,

@@ -243,6 +243,75 @@ def test_device_api(pkg, orc, ctx):
     check_against_oracle(orc, chars, offs, perm, lcp)
 
 
+TEXT_GOLDEN = sorted((Path(__file__).parent / "golden" / "text").glob("*.npz"))
+
+
+@pytest.mark.parametrize("path", TEXT_GOLDEN, ids=[p.stem for p in TEXT_GOLDEN])
+def test_text_golden(pkg, orc, ctx, path):
+    """A text split into lines (or suffixes) on the device and sorted gives
+    the reference psstest's sorted output for the same file, and the LCP
+    array of the oracle."""
+    z = np.load(path)
+    text, suffix = z["text"].tobytes(), bool(z["suffix"])
+    perm, lcp = ctx.sort_text_host(text, ctx.TEXT_SUFFIXES if suffix else ctx.TEXT_LINES)
+    arena, offs = orc.split_text(text, suffix)
+    assert perm.shape[0] == offs.shape[0]
+    assert orc.sorted_output(arena, offs, perm) == z["output"].tobytes()
+    if perm.shape[0] > 1:
+        check_against_oracle(orc, arena, offs, perm, lcp)
+
+
+def _random_text(size, seed):
+    rng = np.random.default_rng(seed)
+    t = rng.choice(np.frombuffer(b"ab\n", np.uint8), size, p=[0.45, 0.45, 0.10]).astype(np.uint8)
+    t[rng.integers(0, size, max(1, size // 5000))] = 0  # NULs end strings too
+    return t
+
+
+@pytest.mark.parametrize("size,mode", [(3 << 20, 0), ((1 << 16) + 1, 0), ((1 << 16) + 8, 0),
+                                       (9, 0), (1, 0), (70001, 1)])
+def test_prepare_text_device(pkg, orc, ctx, size, mode):
+    """Device-side preparation equals the restated loader byte for byte and
+    offset for offset (many chunks, the last byte at a chunk or word
+    boundary, a one-byte text, suffixes); an offset array that is too small
+    is refused with the text left unchanged."""
+    import torch
+    t = _random_text(size, size)
+    dt = torch.zeros(size + 16, dtype=torch.uint8, device="cuda")
+    dt[:size] = torch.from_numpy(t).cuda()
+    arena, offs = orc.split_text(t, suffix=mode == 1)
+    n = offs.shape[0]
+    small = torch.zeros(max(n - 1, 1), dtype=torch.int64, device="cuda")
+    if n > 1:
+        with pytest.raises(pkg.SortError):
+            ctx.prepare_text_device(dt, size, mode, small)
+        assert np.array_equal(dt[:size].cpu().numpy(), t)
+    do = torch.zeros(n, dtype=torch.int64, device="cuda")
+    assert ctx.prepare_text_device(dt, size, mode, do) == n
+    assert np.array_equal(dt.cpu().numpy(), arena)
+    assert np.array_equal(do.cpu().numpy().view(np.uint64), offs)
+    dp = torch.empty(n, dtype=torch.int32, device="cuda")
+    dl = torch.zeros(n, dtype=torch.int32, device="cuda")
+    ctx.sort_device(dt, size, do, dp, dl)
+    if n > 1 and size < (1 << 20):
+        check_against_oracle(orc, arena, offs, dp.cpu().numpy().view(np.uint32),
+                             dl.cpu().numpy().view(np.uint32))
+
+
+def test_sort_text_digits_config_full(pkg, orc, ctx):
+    """The 10 MiB digits workload as a newline-separated text: split and
+    sorted on the device; order, permutation and LCPs checked in full."""
+    chars, offs0, nchars = pkg.workloads.digits(seed=1)
+    text = chars[:nchars].copy()
+    text[text == 0] = 10
+    perm, lcp = ctx.sort_text_host(text, ctx.TEXT_LINES)
+    arena, offs = orc.split_text(text)
+    assert offs.shape[0] == offs0.shape[0] and np.array_equal(offs, offs0)
+    assert orc.check_permutation(perm)
+    assert orc.check_order(arena, offs, perm) == -1
+    assert orc.check_lcp32(arena, offs, perm, lcp) == -1
+
+
 def test_pointer_array_dropins(pkg, orc):
     """The three psstest contestant signatures on a raw pointer array."""
     lib = pkg._native.gpu()

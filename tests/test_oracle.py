@@ -93,3 +93,28 @@ def test_distinguishing_prefix(pkg, orc):
     d, s = orc.dprefix(chars, offs, ids)
     assert s == 2 + 0 + 1  # lcp(abc,abd)=2, lcp(abd,b)=0, lcp(b,ba)=1
     assert d > 0
+
+
+TEXT_GOLDEN = sorted((Path(__file__).parent / "golden" / "text").glob("*.npz"))
+
+
+@pytest.mark.parametrize("path", TEXT_GOLDEN, ids=[p.stem for p in TEXT_GOLDEN])
+def test_text_split_matches_psstest(orc, path):
+    """The restated text loading (lines / suffixes, newline and NUL
+    separators, the forced last NUL) sorted by the oracle reproduces the
+    reference psstest's -o output on the same file."""
+    z = np.load(path)
+    arena, offs = orc.split_text(z["text"].tobytes(), bool(z["suffix"]))
+    ids = orc.sort_ids(arena, offs)
+    assert orc.sorted_output(arena, offs, ids) == z["output"].tobytes()
+
+
+def test_text_split_counts(orc):
+    # separators at 1, 2, 4, 6, 8 of 13 bytes; the last byte becomes NUL
+    arena, offs = orc.split_text(b"b\n\na\nc\0d\nlast")
+    assert offs.tolist() == [0, 2, 3, 5, 7, 9]
+    assert bytes(arena[:13]) == b"b\0\0a\0c\0d\0las\0"
+    arena, offs = orc.split_text(b"x\ny\n", suffix=True)
+    assert offs.tolist() == [0, 1, 2, 3] and bytes(arena[:4]) == b"x\ny\0"
+    assert orc.split_text(b"")[1].shape == (0,)
+    assert orc.split_text(b"\n")[1].tolist() == [0]

@@ -62,10 +62,13 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--cpu-sample", type=int, default=CPU_SAMPLE)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--mode", choices=["sort", "batched", "serving", "autotune"], default="sort",
+    p.add_argument("--mode", choices=["sort", "batched", "serving", "autotune", "merge"],
+                   default="sort",
                    help="sort: the headline line; batched: the 100k-instance batch "
                         "against one call per instance; serving: the request stream "
-                        "through the server; autotune: write the tuning table")
+                        "through the server; autotune: write the tuning table; merge: "
+                        "the device merge of sorted shards (--shards of --n prefixes)")
+    p.add_argument("--shards", type=int, default=8, help="merge mode: sorted runs to merge")
     p.add_argument("--duration", type=float, default=60.0, help="serving: seconds of arrivals")
     p.add_argument("--rate", type=float, default=2000.0, help="serving: requests per second")
     p.add_argument("--budget-gb", type=float, default=40.0, help="serving: HBM budget")
@@ -293,6 +296,53 @@ def run_autotune():
     print(json.dumps({"mode": "autotune", "table": res["table"]}))
 
 
+def run_merge(args):
+    """The reference's top-level composition, sorted shards merged into one
+    sorted sequence with its LCP array (eberle-ps5-parallel-toplevel-merge),
+    on one GPU: --shards contiguous shards of the prefix workload are sorted
+    with LCP output, then each timed step merges them on the device."""
+    import torch
+    import __graft_entry__
+    pkg = __graft_entry__.load_package()
+    n_req = args.n if args.n != N_DEFAULT else 16 * 1024 * 1024
+    chars, offs, nchars = pkg.workloads.prefixes(n=n_req, seed=SEED)
+    n = offs.shape[0]
+    ctx = pkg.Context(0)
+    dc = torch.from_numpy(chars).cuda()
+    do = torch.from_numpy(offs.view(np.int64)).cuda()
+    bounds = np.linspace(0, n, args.shards + 1).astype(np.uint64)
+    ids = torch.empty(n, dtype=torch.int32, device="cuda")
+    lcp = torch.zeros(n, dtype=torch.int32, device="cuda")
+    for k in range(args.shards):
+        b, e = int(bounds[k]), int(bounds[k + 1])
+        ctx.sort_device(dc, nchars, do[b:e], ids[b:e], lcp[b:e])
+        ids[b:e] += b
+    out = torch.empty_like(ids)
+    out_lcp = torch.zeros_like(lcp)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        ctx.merge_lcp_device(dc, nchars, do, bounds, ids, lcp, out, out_lcp, stream=stream)
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    print(json.dumps({
+        "mode": "merge", "metric": "merged char GB/s", "value": nchars / (ms / 1e3) / 1e9,
+        "unit": "GB/s", "ms_per_step": ms, "steps": args.steps, "warmup": max(args.warmup, 3),
+        "higher_is_better": True, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": f"prefixes-{n}", "strings": n, "chars": nchars,
+                   "shards": args.shards, "lcp_output": True},
+        "strings_per_s": n / (ms / 1e3)}))
+    ctx.close()
+
+
 def run_batched(args):
     """The batched workload (100k instances, <= 1 GiB of chars) sorted by one
     batched call, against one pssgpu_sort_device call per instance timed on a
@@ -434,6 +484,9 @@ def main():
         return
     if args.mode == "batched":
         run_batched(args)
+        return
+    if args.mode == "merge":
+        run_merge(args)
         return
     import torch
     import torch.distributed as dist

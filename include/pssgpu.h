@@ -147,6 +147,25 @@ int pssgpu_sort_text_host(pssgpu_ctx* ctx, const uint8_t* text, uint64_t size,
                           int mode, uint32_t* perm, uint32_t* lcp, uint64_t cap,
                           uint64_t* n_out);
 
+/* ---- merge of sorted runs ---------------------------------------------------
+ * pssgpu_merge_lcp_device merges nruns sorted runs of one arena into one
+ * sorted sequence with its LCP array: the step after per-shard sorts that
+ * the reference takes in its top-level merge of per-NUMA-node pS5 outputs
+ * (src/parallel/eberle-ps5-parallel-toplevel-merge.hpp:56-175 with the
+ * LCP-aware K-way merge of src/parallel/eberle-parallel-lcp-merge*.hpp).
+ * runs: host array of nruns + 1 boundaries into d_ids / d_lcp (runs[0] = 0,
+ * non-decreasing, runs[nruns] = n); run k is d_ids[runs[k], runs[k+1]),
+ * sorted, with d_lcp[q] the LCP of d_ids[q - 1] and d_ids[q] inside the run
+ * (the entry at a run's first position is ignored). d_ids_out receives the
+ * merged ids (equal strings keep the order of their runs), d_lcp_out (may be
+ * NULL; then d_lcp may be NULL too) its LCP array with d_lcp_out[0] left
+ * unchanged. Outputs must not overlap the inputs. All device buffers are on
+ * the context's device; the arena rules of pssgpu_sort_device apply. */
+int pssgpu_merge_lcp_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nchars,
+                            const uint64_t* d_offs, const uint64_t* runs, uint32_t nruns,
+                            const uint32_t* d_ids, const uint32_t* d_lcp,
+                            uint32_t* d_ids_out, uint32_t* d_lcp_out, void* stream);
+
 /* ---- batched sorts ---------------------------------------------------------
  * Many independent sort instances in one call: every instance becomes a
  * root segment of the same device passes, so instances of any size share

@@ -36,6 +36,9 @@ GPU_SIGNATURES = {
                                              C.c_void_p]),
     "pssgpu_sort_text_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_int, C.c_void_p,
                                         C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),
+    "pssgpu_merge_lcp_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p,
+                                          C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
+                                          C.c_void_p, C.c_void_p, C.c_void_p]),
     "pssgpu_sort_batch_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p,
                                          C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
     "pssgpu_sort_batch_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p,

@@ -183,6 +183,22 @@ class Context:
         return n.value
 
 
+    def merge_lcp_device(self, chars, nchars: int, offs, runs, ids, lcp, ids_out, lcp_out=None,
+                         stream=None) -> None:
+        """Merge sorted runs (runs: nruns + 1 boundaries into ids / lcp) into
+        ids_out and, if given, its LCP array lcp_out (device tensors)."""
+        runs = np.ascontiguousarray(runs, dtype=np.uint64)
+
+        def addr(t):
+            if t is None:
+                return None
+            return t if isinstance(t, int) else t.data_ptr()
+        s = None if stream is None else (stream if isinstance(stream, int) else stream.cuda_stream)
+        _check(_native.gpu().pssgpu_merge_lcp_device(
+            self._h, addr(chars), nchars, addr(offs), runs.ctypes.data, runs.shape[0] - 1,
+            addr(ids), addr(lcp), addr(ids_out), addr(lcp_out), s))
+
+
 _default: Optional[Context] = None
 
 

@@ -20,6 +20,7 @@
 #include "kernels_big.cuh"
 #include "kernels_block.cuh"
 #include "prepare.cuh"
+#include "merge.cuh"
 
 namespace pssgpu {
 
@@ -165,6 +166,9 @@ struct Ctx {
     uint64_t io2_bytes = 0;
     unsigned char* prep = nullptr;
     uint64_t prep_bytes = 0;
+    // merge rounds: ids / LCP ping-pong, source positions, run boundaries
+    unsigned char* mbuf = nullptr;
+    uint64_t mbuf_bytes = 0;
     pssgpu_stats stats{};
     // profile mode: events around every kernel class, per-class totals
     bool profile = false;
@@ -572,6 +576,7 @@ static void ctx_destroy(Ctx* c)
     if (c->io) cudaFree(c->io);
     if (c->io2) cudaFree(c->io2);
     if (c->prep) cudaFree(c->prep);
+    if (c->mbuf) cudaFree(c->mbuf);
     if (c->inst_buf) cudaFree(c->inst_buf);
     if (c->host_counters) cudaFreeHost(c->host_counters);
     if (c->ev0) cudaEventDestroy(c->ev0);
@@ -1127,6 +1132,85 @@ int pssgpu_sort_text_host(pssgpu_ctx* ctx, const uint8_t* text, uint64_t size, i
     PSS_CUDA(cudaMemcpyAsync(perm, d_perm, 4 * n, cudaMemcpyDeviceToHost, st));
     if (lcp && n > 1)
         PSS_CUDA(cudaMemcpyAsync(lcp + 1, d_lcp + 1, 4 * (n - 1), cudaMemcpyDeviceToHost, st));
+    PSS_CUDA(cudaStreamSynchronize(st));
+    return PSSGPU_OK;
+}
+
+int pssgpu_merge_lcp_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nchars,
+                            const uint64_t* d_offs, const uint64_t* runs, uint32_t nruns,
+                            const uint32_t* d_ids, const uint32_t* d_lcp, uint32_t* d_ids_out,
+                            uint32_t* d_lcp_out, void* stream)
+{
+    if (!ctx || !runs) return fail(PSSGPU_EINVAL, "null context or runs");
+    if (nruns == 0) return fail(PSSGPU_EINVAL, "no runs");
+    if (runs[0] != 0) return fail(PSSGPU_EINVAL, "run boundaries must start at 0");
+    for (uint32_t k = 0; k < nruns; ++k)
+        if (runs[k + 1] < runs[k]) return fail(PSSGPU_EINVAL, "run boundaries decrease");
+    const uint64_t n = runs[nruns];
+    int rc = check_args(nchars, n);
+    if (rc) return rc;
+    if (n == 0) return PSSGPU_OK;
+    if (!d_chars || !d_offs || !d_ids || !d_ids_out) return fail(PSSGPU_EINVAL, "null buffer");
+    if (d_lcp_out && !d_lcp) return fail(PSSGPU_EINVAL, "LCP output needs the runs' LCP arrays");
+    if (((uintptr_t)d_chars & 7) != 0) return fail(PSSGPU_EINVAL, "arena not 8-byte aligned");
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    std::lock_guard<std::mutex> lk(c->mu);
+    PSS_CUDA(cudaSetDevice(c->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    uint8_t last = 1;
+    PSS_CUDA(cudaMemcpyAsync(&last, d_chars + nchars - 1, 1, cudaMemcpyDeviceToHost, st));
+    PSS_CUDA(cudaStreamSynchronize(st));
+    if (last != 0) return fail(PSSGPU_EINVAL, "arena does not end with NUL");
+    if (nruns == 1) {
+        PSS_CUDA(cudaMemcpyAsync(d_ids_out, d_ids, 4 * n, cudaMemcpyDeviceToDevice, st));
+        if (d_lcp_out && n > 1)
+            PSS_CUDA(cudaMemcpyAsync(d_lcp_out + 1, d_lcp + 1, 4 * (n - 1), cudaMemcpyDeviceToDevice, st));
+        PSS_CUDA(cudaStreamSynchronize(st));
+        return PSSGPU_OK;
+    }
+    // boundaries of every round, uploaded at once: round i merges the runs
+    // of level i into those of level i + 1
+    std::vector<std::vector<uint64_t>> level{std::vector<uint64_t>(runs, runs + nruns + 1)};
+    while (level.back().size() > 2) {
+        const std::vector<uint64_t>& a = level.back();
+        const uint32_t K = (uint32_t)a.size() - 1, K2 = (K + 1) / 2;
+        std::vector<uint64_t> b(K2 + 1);
+        for (uint32_t p = 0; p < K2; ++p) b[p] = a[2 * p];
+        b[K2] = n;
+        level.push_back(std::move(b));
+    }
+    const size_t rounds = level.size() - 1;
+    std::vector<uint64_t> flat;
+    std::vector<uint64_t> at;
+    for (const auto& v : level) {
+        at.push_back(flat.size());
+        flat.insert(flat.end(), v.begin(), v.end());
+    }
+    const uint64_t b_v = align256(4 * n), b_runs = align256(8 * flat.size());
+    if ((rc = ensure_buf(&c->mbuf, &c->mbuf_bytes, 5 * b_v + b_runs))) return rc;
+    uint32_t* tid[2] = {(uint32_t*)c->mbuf, (uint32_t*)(c->mbuf + b_v)};
+    uint32_t* tlcp[2] = {(uint32_t*)(c->mbuf + 2 * b_v), (uint32_t*)(c->mbuf + 3 * b_v)};
+    uint32_t* src = (uint32_t*)(c->mbuf + 4 * b_v);
+    uint64_t* d_runs = (uint64_t*)(c->mbuf + 5 * b_v);
+    PSS_CUDA(cudaMemcpyAsync(d_runs, flat.data(), 8 * flat.size(), cudaMemcpyHostToDevice, st));
+    const unsigned blocks = (unsigned)std::min<uint64_t>((n + 255) / 256, 148ull * 16);
+    const uint32_t* in_ids = d_ids;
+    const uint32_t* in_lcp = d_lcp;
+    for (size_t i = 0; i < rounds; ++i) {
+        const bool lastr = i + 1 == rounds;
+        uint32_t* out_ids = lastr ? d_ids_out : tid[i & 1];
+        uint32_t* out_lcp = lastr ? d_lcp_out : tlcp[i & 1];
+        const uint32_t K_in = (uint32_t)level[i].size() - 1, K_out = (uint32_t)level[i + 1].size() - 1;
+        k_merge_place<<<blocks, 256, 0, st>>>(d_chars, nchars, d_offs, d_runs + at[i], K_in, in_ids,
+                                              out_ids, src, n);
+        if (d_lcp_out)
+            k_merge_lcp<<<blocks, 256, 0, st>>>(d_chars, nchars, d_offs, d_runs + at[i], K_in,
+                                                d_runs + at[i + 1], K_out, out_ids, src, in_lcp,
+                                                out_lcp, n);
+        PSS_CUDA(cudaGetLastError());
+        in_ids = out_ids;
+        in_lcp = out_lcp;
+    }
     PSS_CUDA(cudaStreamSynchronize(st));
     return PSSGPU_OK;
 }

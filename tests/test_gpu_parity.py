@@ -312,6 +312,84 @@ def test_sort_text_digits_config_full(pkg, orc, ctx):
     assert orc.check_lcp32(arena, offs, perm, lcp) == -1
 
 
+def _oracle_runs(orc, chars, offs, K, seed, empty_run=False):
+    """Strings dealt at random to K runs, each sorted with its LCP array by
+    the oracle: (ids, lcp, boundaries)."""
+    rng = np.random.default_rng(seed)
+    deal = rng.integers(0, K, offs.shape[0])
+    if empty_run:
+        deal[deal == 1] = 0
+    ids, lcps, runs = [], [], [0]
+    for k in range(K):
+        members = np.flatnonzero(deal == k).astype(np.uint32)
+        if members.shape[0]:
+            sub, sub_lcp = orc.sort_ids_lcp(chars, offs[members])
+            ids.append(members[sub])
+            lcps.append(sub_lcp.astype(np.uint32))
+        runs.append(runs[-1] + members.shape[0])
+    return np.concatenate(ids), np.concatenate(lcps), np.array(runs, np.uint64)
+
+
+def _merge_strings(case):
+    rng = np.random.default_rng(77)
+    if case == "deep":
+        base = bytes(rng.integers(97, 123, 300, dtype=np.uint8))
+        return ([base[: int(rng.integers(250, 301))] + bytes(rng.integers(97, 99, int(rng.integers(0, 5)),
+                                                                        dtype=np.uint8))
+                 for _ in range(6000)] + [base] * 50 + [b""] * 20)
+    return [bytes(rng.integers(97, 100, int(rng.integers(0, 14)), dtype=np.uint8)) for _ in range(30000)]
+
+
+@pytest.mark.parametrize("K,case", [(1, "rand"), (2, "rand"), (3, "rand"), (8, "rand"), (33, "rand"),
+                                    (5, "empty_run"), (4, "deep"), (2, "no_lcp")])
+def test_merge_lcp(pkg, orc, ctx, K, case):
+    """Sorted runs with their LCP arrays merge into the sorted sequence and
+    LCP array of all strings: pairs, odd run counts, many runs, an empty run,
+    runs sharing 250-300 char prefixes with duplicates and empty strings, and
+    the merge without LCP output."""
+    import torch
+    chars, offs = pkg.pack_strings(_merge_strings("deep" if case == "deep" else "rand"))
+    nchars = chars.shape[0]
+    ids, lcp, runs = _oracle_runs(orc, chars, offs, K, 90 + K, empty_run=case == "empty_run")
+    dc = torch.from_numpy(np.concatenate([chars, np.zeros(16, np.uint8)])).cuda()
+    do = torch.from_numpy(offs.view(np.int64)).cuda()
+    di = torch.from_numpy(ids.view(np.int32)).cuda()
+    dl = torch.from_numpy(lcp.view(np.int32)).cuda()
+    dio = torch.empty_like(di)
+    dlo = torch.zeros_like(dl) if case != "no_lcp" else None
+    ctx.merge_lcp_device(dc, nchars, do, runs, di, dl, dio, dlo)
+    perm = dio.cpu().numpy().view(np.uint32)
+    if dlo is None:
+        assert orc.check_permutation(perm)
+        assert orc.check_order(chars, offs, perm) == -1
+    else:
+        check_against_oracle(orc, chars, offs, perm, dlo.cpu().numpy().view(np.uint32))
+
+
+def test_sharded_sort_then_merge(pkg, orc, ctx):
+    """The top-level composition of the reference (per-shard pS5, then the
+    LCP merge): four shards of the prefix workload sorted by the GPU sort
+    with LCP output, merged on the device, checked against the oracle."""
+    import torch
+    chars, offs, nchars = pkg.workloads.prefixes(n=200000, seed=13)
+    n = offs.shape[0]
+    dc = torch.from_numpy(chars).cuda()
+    bounds = np.array([0, 37000, 90000, 150001, n], np.uint64)
+    ids = torch.empty(n, dtype=torch.int32, device="cuda")
+    lcp = torch.zeros(n, dtype=torch.int32, device="cuda")
+    for k in range(4):
+        b, e = int(bounds[k]), int(bounds[k + 1])
+        do = torch.from_numpy(offs[b:e].view(np.int64)).cuda()
+        ctx.sort_device(dc, nchars, do, ids[b:e], lcp[b:e])
+        ids[b:e] += b  # shard-local ids -> global ids
+    do = torch.from_numpy(offs.view(np.int64)).cuda()
+    out = torch.empty_like(ids)
+    out_lcp = torch.zeros_like(lcp)
+    ctx.merge_lcp_device(dc, nchars, do, bounds, ids, lcp, out, out_lcp)
+    check_against_oracle(orc, chars[:nchars], offs, out.cpu().numpy().view(np.uint32),
+                         out_lcp.cpu().numpy().view(np.uint32))
+
+
 def test_pointer_array_dropins(pkg, orc):
     """The three psstest contestant signatures on a raw pointer array."""
     lib = pkg._native.gpu()

@@ -5,13 +5,12 @@
 // LCP-aware K-way merge of src/parallel/eberle-parallel-lcp-merge*.hpp over
 // src/sequential/bingmann-lcp_losertree.hpp).
 //
-// Here the runs merge pairwise, ceil(log2 K) rounds, each a fixed number of
-// launches: every string finds its place in the merged pair by a binary
-// search of the partner run (its own rank plus the partner's strings that
-// precede it: strictly smaller for the left run, smaller or equal for the
-// right one, so equal strings keep the left run first), then every merged
-// position takes its LCP from the input when its predecessor was its
-// predecessor in the same input run, else from comparing the two strings.
+// Here the runs merge pairwise, ceil(log2 K) rounds of three launches: the
+// merge-path split of every piece of MERGE_PIECE outputs, the sequential
+// merge of each piece by one thread (equal strings keep the left run
+// first), then every merged position takes its LCP from the input when its
+// predecessor was its predecessor in the same input run, else from
+// comparing the two strings.
 #pragma once
 
 #include "device_common.cuh"
@@ -49,45 +48,86 @@ __device__ __forceinline__ uint32_t run_of(const uint64_t* runs, uint32_t K, uin
     return lo;
 }
 
-// One round: runs 2p and 2p + 1 of ids_in merge into [runs[2p], runs[2p+2])
-// of ids_out; src[pos] = the input position of the string placed at pos. An
-// unpaired last run is copied.
-__global__ void k_merge_place(const uint8_t* __restrict__ chars, uint64_t nchars,
-                              const uint64_t* __restrict__ offs, const uint64_t* __restrict__ runs,
-                              uint32_t K, const uint32_t* __restrict__ ids_in,
-                              uint32_t* __restrict__ ids_out, uint32_t* __restrict__ src, uint64_t n)
+// Merge-path form of a round. A pair is (a0, a1, b1): left run [a0, a1),
+// right run [a1, b1) (empty for an unpaired last run), merged into [a0, b1).
+// Its output is cut into pieces of MERGE_PIECE positions; task t of the
+// round is piece t - first[pair] of its pair. k_merge_split finds for every
+// piece how many left-run strings precede it (a binary search along the
+// piece's diagonal), k_merge_seq merges each piece sequentially from there.
+constexpr uint32_t MERGE_PIECE = 32;
+
+struct MergePair {
+    uint64_t a0, a1, b1;
+};
+
+__device__ __forceinline__ uint32_t pair_of(const uint64_t* first, uint32_t npair, uint64_t t)
 {
-    for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n;
-         q += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t r = run_of(runs, K, q);
-        const uint32_t x = ids_in[q];
-        uint64_t pos = q;
-        if ((r | 1u) < K) {  // the pair is complete
-            const uint64_t a0 = runs[r & ~1u], a1 = runs[(r & ~1u) + 1], b1 = runs[(r & ~1u) + 2];
-            const uint64_t ox = __ldg(offs + x);
+    uint32_t lo = 0, hi = npair;  // first[lo] <= t < first[hi]
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (first[mid] <= t) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void k_merge_split(const uint8_t* __restrict__ chars, uint64_t nchars,
+                              const uint64_t* __restrict__ offs, const MergePair* __restrict__ pairs,
+                              const uint64_t* __restrict__ first, uint32_t npair,
+                              const uint32_t* __restrict__ ids_in, uint64_t* __restrict__ split)
+{
+    const uint64_t ntask = first[npair];
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ntask;
+         t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t p = pair_of(first, npair, t);
+        const MergePair pr = pairs[p];
+        const uint64_t na = pr.a1 - pr.a0, nb = pr.b1 - pr.a1;
+        const uint64_t d = (t - first[p]) * MERGE_PIECE;
+        // left-run strings among the first d outputs: the first i with
+        // A[i] > B[d - i - 1] (ties go to the left run)
+        uint64_t lo = d > nb ? d - nb : 0, hi = min(d, na);
+        while (lo < hi) {
+            const uint64_t mid = (lo + hi) >> 1;
             uint32_t l;
-            if (!(r & 1u)) {
-                // left run: right-run strings strictly smaller than x
-                uint64_t lo = a1, hi = b1;
-                while (lo < hi) {
-                    const uint64_t mid = (lo + hi) >> 1;
-                    if (compare_lcp(chars, nchars, __ldg(offs + ids_in[mid]), ox, &l) < 0) lo = mid + 1;
-                    else hi = mid;
-                }
-                pos = q + (lo - a1);
-            } else {
-                // right run: left-run strings smaller than or equal to x
-                uint64_t lo = a0, hi = a1;
-                while (lo < hi) {
-                    const uint64_t mid = (lo + hi) >> 1;
-                    if (compare_lcp(chars, nchars, __ldg(offs + ids_in[mid]), ox, &l) <= 0) lo = mid + 1;
-                    else hi = mid;
-                }
-                pos = a0 + (q - a1) + (lo - a0);
-            }
+            const int c = compare_lcp(chars, nchars, __ldg(offs + ids_in[pr.a0 + mid]),
+                                      __ldg(offs + ids_in[pr.a1 + d - mid - 1]), &l);
+            if (c <= 0) lo = mid + 1; else hi = mid;
         }
-        ids_out[pos] = x;
-        src[pos] = (uint32_t)q;
+        split[t] = lo;
+    }
+}
+
+__global__ void k_merge_seq(const uint8_t* __restrict__ chars, uint64_t nchars,
+                            const uint64_t* __restrict__ offs, const MergePair* __restrict__ pairs,
+                            const uint64_t* __restrict__ first, uint32_t npair,
+                            const uint64_t* __restrict__ split, const uint32_t* __restrict__ ids_in,
+                            uint32_t* __restrict__ ids_out, uint32_t* __restrict__ src)
+{
+    const uint64_t ntask = first[npair];
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ntask;
+         t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t p = pair_of(first, npair, t);
+        const MergePair pr = pairs[p];
+        const uint64_t na = pr.a1 - pr.a0, nb = pr.b1 - pr.a1;
+        const uint64_t d0 = (t - first[p]) * MERGE_PIECE;
+        const uint64_t d1 = min(d0 + MERGE_PIECE, na + nb);
+        const uint64_t i0 = split[t];
+        const uint64_t i1 = t + 1 < first[p + 1] ? split[t + 1] : na;
+        uint64_t i = i0, j = d0 - i0;
+        const uint64_t j1 = d1 - i1;
+        for (uint64_t d = d0; d < d1; ++d) {
+            bool take_a;
+            if (i >= i1) take_a = false;
+            else if (j >= j1) take_a = true;
+            else {
+                uint32_t l;
+                take_a = compare_lcp(chars, nchars, __ldg(offs + ids_in[pr.a0 + i]),
+                                     __ldg(offs + ids_in[pr.a1 + j]), &l) <= 0;
+            }
+            const uint64_t q = take_a ? pr.a0 + i : pr.a1 + j;
+            ids_out[pr.a0 + d] = ids_in[q];
+            src[pr.a0 + d] = (uint32_t)q;
+            if (take_a) ++i; else ++j;
+        }
     }
 }
 

@@ -1168,8 +1168,8 @@ int pssgpu_merge_lcp_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nc
         PSS_CUDA(cudaStreamSynchronize(st));
         return PSSGPU_OK;
     }
-    // boundaries of every round, uploaded at once: round i merges the runs
-    // of level i into those of level i + 1
+    // boundaries, pairs and piece counts of every round, uploaded at once:
+    // round i merges the runs of level i into those of level i + 1
     std::vector<std::vector<uint64_t>> level{std::vector<uint64_t>(runs, runs + nruns + 1)};
     while (level.back().size() > 2) {
         const std::vector<uint64_t>& a = level.back();
@@ -1180,19 +1180,44 @@ int pssgpu_merge_lcp_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nc
         level.push_back(std::move(b));
     }
     const size_t rounds = level.size() - 1;
-    std::vector<uint64_t> flat;
-    std::vector<uint64_t> at;
-    for (const auto& v : level) {
-        at.push_back(flat.size());
-        flat.insert(flat.end(), v.begin(), v.end());
+    std::vector<uint64_t> flat;  // per level: boundaries; per round: pairs, piece starts
+    std::vector<uint64_t> at_runs, at_pairs, at_first, npairs;
+    uint64_t max_tasks = 0;
+    for (size_t i = 0; i <= rounds; ++i) {
+        at_runs.push_back(flat.size());
+        flat.insert(flat.end(), level[i].begin(), level[i].end());
+    }
+    for (size_t i = 0; i < rounds; ++i) {
+        const std::vector<uint64_t>& a = level[i];
+        const uint32_t K = (uint32_t)a.size() - 1, np = (K + 1) / 2;
+        at_pairs.push_back(flat.size());
+        for (uint32_t p = 0; p < np; ++p) {
+            const uint64_t a0 = a[2 * p], a1 = a[2 * p + 1];
+            const uint64_t b1 = 2 * p + 2 <= K ? a[2 * p + 2] : a1;  // an unpaired last run
+            flat.push_back(a0);
+            flat.push_back(a1);
+            flat.push_back(b1);
+        }
+        at_first.push_back(flat.size());
+        uint64_t t = 0;
+        for (uint32_t p = 0; p < np; ++p) {
+            flat.push_back(t);
+            const uint64_t m = flat[at_pairs.back() + 3 * p + 2] - flat[at_pairs.back() + 3 * p];
+            t += (m + MERGE_PIECE - 1) / MERGE_PIECE;
+        }
+        flat.push_back(t);
+        npairs.push_back(np);
+        max_tasks = std::max(max_tasks, t);
     }
     const uint64_t b_v = align256(4 * n), b_runs = align256(8 * flat.size());
-    if ((rc = ensure_buf(&c->mbuf, &c->mbuf_bytes, 5 * b_v + b_runs))) return rc;
+    const uint64_t b_split = align256(8 * (max_tasks + 1));
+    if ((rc = ensure_buf(&c->mbuf, &c->mbuf_bytes, 5 * b_v + b_runs + b_split))) return rc;
     uint32_t* tid[2] = {(uint32_t*)c->mbuf, (uint32_t*)(c->mbuf + b_v)};
     uint32_t* tlcp[2] = {(uint32_t*)(c->mbuf + 2 * b_v), (uint32_t*)(c->mbuf + 3 * b_v)};
     uint32_t* src = (uint32_t*)(c->mbuf + 4 * b_v);
-    uint64_t* d_runs = (uint64_t*)(c->mbuf + 5 * b_v);
-    PSS_CUDA(cudaMemcpyAsync(d_runs, flat.data(), 8 * flat.size(), cudaMemcpyHostToDevice, st));
+    uint64_t* d_flat = (uint64_t*)(c->mbuf + 5 * b_v);
+    uint64_t* split = (uint64_t*)(c->mbuf + 5 * b_v + b_runs);
+    PSS_CUDA(cudaMemcpyAsync(d_flat, flat.data(), 8 * flat.size(), cudaMemcpyHostToDevice, st));
     const unsigned blocks = (unsigned)std::min<uint64_t>((n + 255) / 256, 148ull * 16);
     const uint32_t* in_ids = d_ids;
     const uint32_t* in_lcp = d_lcp;
@@ -1201,11 +1226,15 @@ int pssgpu_merge_lcp_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nc
         uint32_t* out_ids = lastr ? d_ids_out : tid[i & 1];
         uint32_t* out_lcp = lastr ? d_lcp_out : tlcp[i & 1];
         const uint32_t K_in = (uint32_t)level[i].size() - 1, K_out = (uint32_t)level[i + 1].size() - 1;
-        k_merge_place<<<blocks, 256, 0, st>>>(d_chars, nchars, d_offs, d_runs + at[i], K_in, in_ids,
-                                              out_ids, src, n);
+        const MergePair* pairs = reinterpret_cast<const MergePair*>(d_flat + at_pairs[i]);
+        const uint64_t* first = d_flat + at_first[i];
+        const uint32_t np = (uint32_t)npairs[i];
+        k_merge_split<<<blocks, 256, 0, st>>>(d_chars, nchars, d_offs, pairs, first, np, in_ids, split);
+        k_merge_seq<<<blocks, 256, 0, st>>>(d_chars, nchars, d_offs, pairs, first, np, split, in_ids,
+                                            out_ids, src);
         if (d_lcp_out)
-            k_merge_lcp<<<blocks, 256, 0, st>>>(d_chars, nchars, d_offs, d_runs + at[i], K_in,
-                                                d_runs + at[i + 1], K_out, out_ids, src, in_lcp,
+            k_merge_lcp<<<blocks, 256, 0, st>>>(d_chars, nchars, d_offs, d_flat + at_runs[i], K_in,
+                                                d_flat + at_runs[i + 1], K_out, out_ids, src, in_lcp,
                                                 out_lcp, n);
         PSS_CUDA(cudaGetLastError());
         in_ids = out_ids;

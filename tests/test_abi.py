@@ -53,3 +53,16 @@ def test_no_device_is_a_status_not_a_crash(pkg):
     assert b"device" in pkg._native.gpu().pssgpu_last_error()
     with pytest.raises(pkg.SortError):
         pkg.Context(0)
+
+
+def test_build_tracks_every_cuda_source():
+    """Every CUDA source of the package is a dependency of the library build,
+    so that editing any of them rebuilds it."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "pss_build", ROOT / "parallel-string-sorting_b200" / "build.py")
+    build = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(build)
+    sources = {p.name for p in (ROOT / "parallel-string-sorting_b200" / "csrc").iterdir()
+               if p.suffix in (".cu", ".cuh")}
+    assert sources <= set(build.CUDA_DEPS)

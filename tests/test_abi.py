@@ -66,3 +66,35 @@ def test_build_tracks_every_cuda_source():
     sources = {p.name for p in (ROOT / "parallel-string-sorting_b200" / "csrc").iterdir()
                if p.suffix in (".cu", ".cuh")}
     assert sources <= set(build.CUDA_DEPS)
+
+
+def test_text_and_merge_arguments_checked_before_device_use(pkg):
+    """The text and merge entry points refuse bad arguments with
+    PSSGPU_EINVAL (and accept empty inputs) before they touch the context or
+    any device buffer, so these checks run without a GPU. The context handle
+    is a placeholder that the checked paths never dereference."""
+    lib = pkg._native.gpu()
+    fake = C.c_void_p(64)
+    n = C.c_uint64(99)
+    assert lib.pssgpu_prepare_text_device(None, None, 5, 0, None, 0, C.byref(n), None) == 1
+    assert lib.pssgpu_prepare_text_device(fake, None, 5, 7, None, 0, C.byref(n), None) == 1
+    assert lib.pssgpu_prepare_text_device(fake, None, 0, 0, None, 0, C.byref(n), None) == 0
+    assert n.value == 0
+    assert lib.pssgpu_prepare_text_device(fake, None, 5, 0, None, 9, C.byref(n), None) == 1
+    assert lib.pssgpu_prepare_text_device(fake, 9, 5, 0, 64, 9, C.byref(n), None) == 1  # unaligned
+    assert b"aligned" in lib.pssgpu_last_error()
+    assert lib.pssgpu_sort_text_host(fake, None, 5, 2, None, None, 0, C.byref(n)) == 1
+    assert lib.pssgpu_sort_text_host(fake, None, 0, 0, None, None, 0, C.byref(n)) == 0
+    assert lib.pssgpu_sort_text_host(fake, None, 5, 0, None, None, 5, C.byref(n)) == 1
+
+    def runs(*b):
+        return (C.c_uint64 * len(b))(*b)
+    merge = lib.pssgpu_merge_lcp_device
+    assert merge(fake, 64, 10, 64, runs(0), 0, 64, 64, 64, 64, None) == 1           # no runs
+    assert merge(fake, 64, 10, 64, runs(1, 2), 1, 64, 64, 64, 64, None) == 1        # not from 0
+    assert merge(fake, 64, 10, 64, runs(0, 5, 3), 2, 64, 64, 64, 64, None) == 1     # decreasing
+    assert merge(fake, 64, 0, 64, runs(0, 5), 1, 64, 64, 64, 64, None) == 1         # empty arena
+    assert merge(fake, None, 10, 64, runs(0, 5), 1, 64, 64, 64, 64, None) == 1      # null arena
+    assert merge(fake, 64, 10, 64, runs(0, 5), 1, 64, None, 64, 64, None) == 1      # LCP out, none in
+    assert merge(fake, 68, 10, 64, runs(0, 5), 1, 64, 64, 64, 64, None) == 1        # unaligned arena
+    assert merge(fake, 64, 10, 64, runs(0, 0, 0), 2, None, None, None, None, None) == 0  # nothing to merge

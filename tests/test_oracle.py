@@ -118,3 +118,41 @@ def test_text_split_counts(orc):
     assert offs.tolist() == [0, 1, 2, 3] and bytes(arena[:4]) == b"x\ny\0"
     assert orc.split_text(b"")[1].shape == (0,)
     assert orc.split_text(b"\n")[1].tolist() == [0]
+
+
+def _split_text_loops(text: bytes, suffix: bool):
+    """The loader and the pointer-array build as the reference writes them,
+    loop for loop (src/tools/input.hpp:275-297, src/psstest.cpp:479-518)."""
+    data = bytearray(text) + bytearray(9)
+    size = len(text)
+    count = 1
+    if not suffix:
+        for i in range(size):
+            if data[i] == 10 or data[i] == 0:
+                data[i] = 0
+                if i + 1 < size:
+                    count += 1
+    else:
+        count = size
+    data[size - 1] = 0
+    if not suffix:
+        starts = [i for i in range(size) if i == 0 or data[i - 1] == 0]
+    else:
+        starts = list(range(size))
+    assert len(starts) == count
+    return bytes(data[:size]), starts
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_text_split_matches_loop_restatement(orc, seed):
+    """The vectorised restatement equals the reference's loops on random
+    texts over {a, b, newline, NUL} of 1..300 bytes, in both modes."""
+    rng = np.random.default_rng(seed)
+    for _ in range(40):
+        size = int(rng.integers(1, 301))
+        text = bytes(rng.choice(np.frombuffer(b"ab\n\0", np.uint8), size, p=[0.4, 0.4, 0.15, 0.05]))
+        for suffix in (False, True):
+            arena, offs = orc.split_text(text, suffix)
+            data, starts = _split_text_loops(text, suffix)
+            assert bytes(arena[:size]) == data and not arena[size:].any()
+            assert offs.tolist() == starts

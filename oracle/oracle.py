@@ -244,3 +244,52 @@ def sorted_output(chars, offs, ids) -> bytes:
         e = raw.index(b"\0", o)
         out.append(raw[o:e] + b"\n")
     return b"".join(out)
+
+
+def lcp_merge2(chars, offs, a_ids, a_lcp, b_ids, b_lcp):
+    """Two-way LCP merge, restated from the reference's LCP loser tree
+    (src/sequential/bingmann-lcp_losertree.hpp:61-105 for the compare rule,
+    :156-185 for the output and the winner's successor): every head carries
+    its LCP with the last output; the head with the larger LCP is the smaller
+    string without reading a char; on equal LCPs the two compare from that
+    depth, and the loser keeps the LCP found. The winner's successor takes its
+    LCP from its run's LCP array; the output LCP is the winner's LCP. Ties go
+    to the first run.
+
+    Pure Python, for small inputs. Returns (ids, lcp, chars_read): lcp[0] = 0,
+    chars_read counts the char pairs compared."""
+    raw = bytes(chars)
+
+    def char_at(i, d):
+        o = int(offs[int(i)]) + d
+        return raw[o] if o < len(raw) else 0
+
+    runs = [(list(a_ids), list(a_lcp)), (list(b_ids), list(b_lcp))]
+    pos = [0, 0]
+    h = [0, 0]  # LCP of each head with the last output (0 before the first)
+    out_ids, out_lcp = [], []
+    reads = 0
+    while pos[0] < len(runs[0][0]) or pos[1] < len(runs[1][0]):
+        if pos[0] >= len(runs[0][0]):
+            w = 1
+        elif pos[1] >= len(runs[1][0]):
+            w = 0
+        elif h[0] != h[1]:
+            w = 0 if h[0] > h[1] else 1
+        else:
+            a, b = runs[0][0][pos[0]], runs[1][0][pos[1]]
+            d = h[0]
+            while True:
+                ca, cb = char_at(a, d), char_at(b, d)
+                reads += 1
+                if ca != cb or ca == 0:
+                    break
+                d += 1
+            w = 0 if ca <= cb else 1  # equal strings: the first run
+            h[1 - w] = d              # the loser's LCP with the new last output
+        out_ids.append(runs[w][0][pos[w]])
+        out_lcp.append(h[w] if out_ids[1:] else 0)
+        pos[w] += 1
+        if pos[w] < len(runs[w][0]):
+            h[w] = int(runs[w][1][pos[w]])  # against its predecessor, the last output
+    return np.array(out_ids, np.uint32), np.array(out_lcp, np.uint64), reads

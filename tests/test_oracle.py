@@ -156,3 +156,29 @@ def test_text_split_matches_loop_restatement(orc, seed):
             data, starts = _split_text_loops(text, suffix)
             assert bytes(arena[:size]) == data and not arena[size:].any()
             assert offs.tolist() == starts
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_lcp_merge_rule(pkg, orc, seed):
+    """The LCP rule of the reference's loser tree, restated for two runs:
+    merging two sorted runs with their LCP arrays gives the sorted order and
+    LCP array of all strings, and reads only the chars behind the LCPs (far
+    fewer than compares from char 0)."""
+    rng = np.random.default_rng(seed)
+    pre = bytes(rng.integers(97, 123, 30, dtype=np.uint8))
+    strings = [pre[: int(rng.integers(0, 31))] + bytes(rng.integers(97, 100, int(rng.integers(0, 5)),
+                                                                     dtype=np.uint8))
+               for _ in range(600)]
+    chars, offs = pkg.pack_strings(strings)
+    deal = rng.integers(0, 2, len(strings))
+    parts = []
+    for k in (0, 1):
+        members = np.flatnonzero(deal == k).astype(np.uint32)
+        sub, sub_lcp = orc.sort_ids_lcp(chars, offs[members])
+        parts += [members[sub], sub_lcp]
+    ids, lcp, reads = orc.lcp_merge2(chars, offs, *parts)
+    rids, rlcp = orc.sort_ids_lcp(chars, offs)
+    assert np.array_equal(canonical_ids(chars, offs, ids, lcp), canonical_ids(chars, offs, rids, rlcp))
+    assert np.array_equal(lcp[1:], rlcp[1:])
+    full = sum(int(x) + 1 for x in rlcp[1:])  # chars a compare from char 0 reads, at least
+    assert reads < full / 4

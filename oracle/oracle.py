@@ -1,8 +1,11 @@
 """TEST INFRASTRUCTURE, not part of the product: ctypes bindings of the two
-checkers built by oracle/Makefile.
+checkers built by oracle/Makefile, and small restatements in numpy / Python.
 
 * ``build/libpssoracle.so`` -- the plain-C restatement (pss_oracle.c).
 * ``_ref/libps5ref.so``     -- the reference pS5 compiled from its sources.
+* ``split_text`` / ``sorted_output`` -- psstest's text loading and its -o
+  output, pinned to the reference psstest's outputs (tests/golden/text/).
+* ``lcp_merge2`` -- the reference loser tree's LCP rule for two runs.
 
 Only tests/, the smoke check and the CPU-baseline leg of bench.py use this
 module, always as the checker or as the timed reference.

@@ -19,10 +19,17 @@ instance.
              bytes / its summed event time against the measured HBM copy
              bandwidth; roofline_sort does the same for the whole sort with
              the method's algorithmic bytes computed from the LCP array
-  cpu_baseline  the reference pS5 (compiled from the reference sources) on a
-             bounded sample of the same workload, all host threads
+  cpu_baseline  the reference pS5 (compiled from the reference sources) on
+             the same instance, all host threads, best of 3
+  verified   the last timed sort's permutation checked on the host (every id
+             once, neighbouring strings in strcmp order)
+  batched    the 100k-instance batched workload: one batched call (median and
+             p99 over steps) against one call per instance (sampled)
+  serving    a shortened Poisson request stream (--serving-duration seconds at
+             --rate) through the continuous-batching server: p50 / p99 latency
 
---impl reference times the reference pS5 alone on the host cores (rank 0).
+--impl reference times the reference pS5 alone on the host cores (rank 0) on
+the same instance, with the same warm-up and step counts.
 With N GPUs (torchrun) every rank sorts its own instance (weak scaling; no
 collective is needed by the sort).
 """
@@ -45,7 +52,6 @@ sys.path.insert(0, str(ROOT))
 METRIC = "sorted char GB/s"
 N_DEFAULT = 64 * 1024 * 1024
 SEED = 2
-CPU_SAMPLE = 8 * 1024 * 1024
 
 
 def parse():
@@ -60,7 +66,10 @@ def parse():
                         "digits = the 10 MiB random-digit strings, dna = all suffixes of a "
                         "32 MiB repetitive DNA text")
     p.add_argument("--e2e-steps", type=int, default=3)
-    p.add_argument("--cpu-sample", type=int, default=CPU_SAMPLE)
+    p.add_argument("--no-extras", action="store_true",
+                   help="sort mode: leave out the batched and serving records")
+    p.add_argument("--serving-duration", type=float, default=10.0,
+                   help="sort mode: seconds of arrivals of the serving record")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--mode", choices=["sort", "batched", "serving", "autotune", "merge"],
                    default="sort",
@@ -213,74 +222,78 @@ def pinned_alloc(torch):
     return alloc
 
 
-def cpu_baseline(n_sample: int, workload: str = "prefixes") -> dict:
-    """Reference pS5 (parallel_sample_sortBTCUI) on the first n_sample strings
-    of the same generator (the whole input for digits and dna), all host
-    threads, best of 3."""
+def ref_time(chars, offs, nchars: int, reps: int, warmup: int = 0):
+    """The reference pS5 (parallel_sample_sortBTCUI, built from the reference
+    sources into oracle/_ref) on the given arena with every host thread:
+    `warmup` untimed sorts, then `reps` timed ones (each on a fresh copy of
+    the unsorted pointer array, copied outside the timer). Returns (list of
+    seconds, threads), or None when the library is not built."""
     from oracle import oracle as orc
-    import __graft_entry__
-    pkg = __graft_entry__.load_package()
     if not orc.ref_available():
-        return {"value": None, "unit": "GB/s", "cores": os.cpu_count(), "kind": "reference",
-                "sample": "oracle/_ref/libps5ref.so not built"}
-    chars, offs, nchars = make_workload(pkg, workload, n_sample)
-    n_sample = offs.shape[0]
+        return None
     threads = os.cpu_count()
     lib = orc.ref_lib()
     lib.ps5ref_set_threads(threads)
     base = orc.ref_pointer_array(chars, offs)
+    n = base.shape[0]
+    ptrs = np.empty_like(base)
     times = []
-    for _ in range(3):
-        ptrs = base.copy()
+    for i in range(warmup + reps):
+        np.copyto(ptrs, base)
         t0 = time.perf_counter()
-        lib.ps5ref_sort(ptrs.ctypes.data, n_sample)
-        times.append(time.perf_counter() - t0)
+        lib.ps5ref_sort(ptrs.ctypes.data, n)
+        dt = time.perf_counter() - t0
+        if i >= warmup:
+            times.append(dt)
+    return times, threads
+
+
+def cpu_baseline(chars, offs, nchars: int) -> dict:
+    """Reference pS5 on the same input the GPU arm sorts (the whole instance),
+    every host thread, best of 3."""
+    r = ref_time(chars, offs, nchars, reps=3)
+    if r is None:
+        return {"value": None, "unit": "GB/s", "cores": os.cpu_count(), "kind": "reference",
+                "sample": "oracle/_ref/libps5ref.so not built"}
+    times, threads = r
     t = min(times)
+    n = offs.shape[0]
     return {"value": nchars / t / 1e9, "unit": "GB/s", "cores": threads, "kind": "reference",
-            "sample": f"{n_sample} strings of the same generator ({nchars} chars), "
-                      f"pS5-Unroll (parallel_sample_sortBTCUI) best of 3: {t * 1e3:.1f} ms",
-            "strings_per_s": n_sample / t}
+            "sample": f"the whole instance: {n} strings, {nchars} chars; pS5-Unroll "
+                      f"(parallel_sample_sortBTCUI) best of 3: {t * 1e3:.1f} ms",
+            "strings_per_s": n / t}
 
 
 def run_reference(args):
+    """The reference arm: pS5 from the reference sources on the host cores,
+    on the same workload and config as the GPU arm, the same warm-up and step
+    counts, rank 0 only."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     from oracle import oracle as orc
     import __graft_entry__
     pkg = __graft_entry__.load_package()
-    chars, offs, nchars = make_workload(pkg, args.workload, args.cpu_sample)
-    n = offs.shape[0]
     if not orc.ref_available():
         print(json.dumps({"impl": "reference", "unavailable":
                           "oracle/_ref/libps5ref.so (reference pS5 built from its sources) missing"}))
         return
-    threads = os.cpu_count()
-    lib = orc.ref_lib()
-    lib.ps5ref_set_threads(threads)
-    base = orc.ref_pointer_array(chars, offs)
-    for _ in range(args.warmup):
-        ptrs = base.copy()
-        lib.ps5ref_sort(ptrs.ctypes.data, n)
-    times = []
-    for _ in range(args.steps):
-        ptrs = base.copy()
-        t0 = time.perf_counter()
-        lib.ps5ref_sort(ptrs.ctypes.data, n)
-        times.append(time.perf_counter() - t0)
+    chars, offs, nchars = make_workload(pkg, args.workload, args.n)
+    n = offs.shape[0]
+    times, threads = ref_time(chars, offs, nchars, reps=args.steps, warmup=args.warmup)
     t = sum(times) / len(times)
     value = nchars / t / 1e9
-    cfg = workload_config(args.n if args.workload == "prefixes" else n, None, args.workload)
-    cfg.update({"sample_strings": n, "sample_chars": nchars})
     line = {
         "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
-        "data": "synthetic", "config": cfg, "impl": "reference",
+        "data": "synthetic", "config": workload_config(n, nchars, args.workload),
+        "impl": "reference",
+        "strings_per_s": n / t,
         "cpu_baseline": {"value": value, "unit": "GB/s", "cores": threads, "kind": "reference",
-                         "sample": f"{n} strings of the workload generator ({nchars} chars), "
-                                   "pS5-Unroll (parallel_sample_sortBTCUI) from the reference "
-                                   "sources, every host thread"},
+                         "sample": f"the whole instance ({n} strings, {nchars} chars) every "
+                                   "step; pS5-Unroll (parallel_sample_sortBTCUI) from the "
+                                   "reference sources, every host thread"},
         "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -343,10 +356,11 @@ def run_merge(args):
     ctx.close()
 
 
-def run_batched(args):
+def run_batched(args, emit: bool = True) -> dict:
     """The batched workload (100k instances, <= 1 GiB of chars) sorted by one
     batched call, against one pssgpu_sort_device call per instance timed on a
-    random sample of instances and scaled to all instances."""
+    random sample of instances and scaled to all instances. The batched
+    output is checked against the single-instance sorts of the sample."""
     import torch
     import __graft_entry__
     from importlib import import_module
@@ -392,7 +406,14 @@ def run_batched(args):
         ms = timed(batch, args.steps)
         res[name] = {"ms": statistics.median(ms), "ms_all": ms,
                      "launches": ctx.stats()["kernel_launches"]}
-    best = min(res.values(), key=lambda r: r["ms"])
+    best_name = min(res, key=lambda k: res[k]["ms"])
+    best = res[best_name]
+    ctx.set_tree_bits(table if best_name == "tuned" else [0] * 33)
+    clocks = Clocks(0)
+    clocks.start()
+    time.sleep(0.2)
+    ms_best = timed(batch, max(args.steps, 10))
+    clk = clocks.stop()
     batch()  # output of the best configuration for the comparison
     perm_b = dp.cpu().numpy().view(np.uint32)
     lcp_b = dl.cpu().numpy().view(np.uint32)
@@ -418,24 +439,31 @@ def run_batched(args):
                 canonical_ids(h_chars, offs_k, perm_b[b:e], lcp_b[b:e], lens_k))):
             identical = False
     per_instance_ms = single_ms * ninst / len(sample)
+    med = statistics.median(ms_best)
     line = {"mode": "batched", "metric": "batched sort time", "unit": "ms",
             "config": {"workload": "batched-100k", "instances": ninst, "strings": n,
                        "chars": nchars, "sizes": "log-uniform 16..1Mi, scaled to <= 1 GiB",
-                       "lengths": "lognormal(3, 0.5) clipped 1..256", "alphabet": "32..126"},
-            "batched_ms": best["ms"], "batched": res,
-            "char_gb_s": nchars / (best["ms"] / 1e3) / 1e9,
+                       "lengths": "lognormal(3, 0.5) clipped 1..256", "alphabet": "32..126",
+                       "inputs": "resident in HBM (1 GiB of chars > L2)",
+                       "lcp_output": True},
+            "batched_ms": med, "batched_ms_p99": float(np.percentile(ms_best, 99)),
+            "batched_steps": len(ms_best), "tree_bits": best_name, "configs": res,
+            "char_gb_s": nchars / (med / 1e3) / 1e9,
             "per_instance_ms_est": per_instance_ms,
             "per_instance_sample": len(sample),
-            "speedup_vs_per_instance": per_instance_ms / best["ms"],
-            "identical_output_on_sample": identical, "generate_s": gen_s}
-    print(json.dumps(line))
+            "speedup_vs_per_instance": per_instance_ms / med,
+            "identical_output_on_sample": identical, "generate_s": gen_s, "clocks": clk}
+    if emit:
+        print(json.dumps(line))
     ctx.close()
+    return line
 
 
-def run_serving(args):
+def run_serving(args, duration=None, emit: bool = True) -> dict:
     """The serving stream: Poisson arrivals at --rate for --duration seconds,
     sizes log-uniform 1 KB..64 MB, alphabets {4, 10, 26, 95}, lengths
     U[1, 64], through the continuous-batching server under --budget-gb."""
+    duration = args.duration if duration is None else duration
     import torch
     import __graft_entry__
     from importlib import import_module
@@ -445,7 +473,7 @@ def run_serving(args):
     t0 = time.perf_counter()
     pools = serving.make_pools(bytes_per_pool=512 << 20, alloc=alloc)
     t1 = time.perf_counter()
-    reqs = serving.make_stream(pools, rate=args.rate, duration=args.duration)
+    reqs = serving.make_stream(pools, rate=args.rate, duration=duration)
     t2 = time.perf_counter()
     srv = serving.Server(budget=int(args.budget_gb * (1 << 30)), workers=3,
                          max_batch_strings=8 << 20)
@@ -462,13 +490,15 @@ def run_serving(args):
     srv.close()
     line = {"mode": "serving", "metric": "request latency and sustained char GB/s",
             "config": {"workload": "serving-poisson", "rate_per_s": args.rate,
-                       "duration_s": args.duration, "request_bytes": "log-uniform 1 KB..64 MB",
+                       "duration_s": duration, "request_bytes": "log-uniform 1 KB..64 MB",
                        "alphabets": [4, 10, 26, 95], "lengths": "U[1,64]",
                        "hbm_budget_gb": args.budget_gb, "workers": 3,
                        "max_batch_strings": 8 << 20},
             **res, "batches": st["batches"], "slab_gb": st["slab_bytes"] / 2**30,
             "slab_peak_gb": st["slab_peak_bytes"] / 2**30, "clocks": clk}
-    print(json.dumps(line))
+    if emit:
+        print(json.dumps(line))
+    return line
 
 
 def main():
@@ -561,6 +591,15 @@ def main():
     barrier()
     clk = clocks.stop()
 
+    # the last timed sort's output, checked once on the host (outside the
+    # timed region): a permutation of the ids in strcmp order of the strings
+    t_v = time.perf_counter()
+    h_check = d_perm.cpu().numpy().view(np.uint32)
+    verified = bool(pkg.workloads.check_permutation(h_check)) and \
+        pkg.workloads.check_sorted(h_chars, nchars, h_offs, h_check) == -1
+    verify_s = time.perf_counter() - t_v
+    del h_check
+
     # per-kernel-class split (profile mode: classes run one after another on
     # the stream, each between CUDA events), outside the timed region
     ctx.set_profile(True)
@@ -598,7 +637,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(min(args.cpu_sample, n), args.workload)
+        cpu = cpu_baseline(h_chars, h_offs, nchars)
 
     # the same end to end through the text entry point: only the text goes to
     # the device (no offset array) and is split there, as psstest's loader
@@ -662,9 +701,29 @@ def main():
             "gpu_launches": launches,
             "clocks": clk,
             "cpu_baseline": cpu,
+            "verified": verified,
+            "verified_how": "permutation of the last timed sort's ids and strcmp order of "
+                            f"every neighbouring pair, on the host ({verify_s:.1f} s)",
         }
-        print(json.dumps(line))
     ctx.close()
+    del d_chars, d_offs, d_perm, d_lcp
+    torch.cuda.empty_cache()
+    if rank == 0 and world == 1 and args.workload == "prefixes" and not args.no_extras:
+        # the other two patterns of the metric, on the same GPU after the
+        # headline's buffers are freed: the 100k-instance batched sort and a
+        # shortened serving stream (p50 / p99 request latency)
+        del h_chars, h_offs
+        b = run_batched(args, emit=False)
+        line["batched"] = {k: b[k] for k in (
+            "batched_ms", "batched_ms_p99", "batched_steps", "char_gb_s", "per_instance_ms_est",
+            "per_instance_sample", "speedup_vs_per_instance", "identical_output_on_sample",
+            "tree_bits", "config", "clocks")}
+        torch.cuda.empty_cache()
+        sv = run_serving(args, duration=args.serving_duration, emit=False)
+        line["serving"] = {k: sv[k] for k in sv if k not in ("mode", "metric")}
+        line["serving_p99_ms"] = sv.get("p99_ms")
+    if rank == 0:
+        print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
 

@@ -237,13 +237,41 @@ int pssgpu_server_get_stats(pssgpu_server* srv, pssgpu_server_stats* out);
  * do, never writes the characters, and uses the default context of device 0.
  * lcp[0] is left untouched; cache[i] = strings[i][lcp[i]] for i >= 1
  * (verify_lcp_cache, src/tools/stringptr.hpp:977-1033). On failure they
- * abort(). The _status variants return the status code instead. */
+ * abort(). The _status variants return the status code instead.
+ * These entry points read each string from its own pointer (strlen, then a
+ * copy of its bytes), so the strings may live in separate allocations. */
 void pssgpu_sort_strings(unsigned char** strings, size_t n);
 void pssgpu_sort_strings_lcp(unsigned char** strings, uintptr_t* lcp, size_t n);
 void pssgpu_sort_strings_lcp_cache(uint8_t** strings, uintptr_t* lcp,
                                    uint8_t* cache, size_t n);
 int pssgpu_sort_strings_status(unsigned char** strings, uintptr_t* lcp,
                                uint8_t* cache, size_t n);
+
+/* Separate-output variant: the sorted pointers go to output[0, n) and
+ * strings[] is left unchanged. Replaces parallel_sample_sort_out_base
+ * (bingmann-parallel_sample_sort.hpp:1704-1714) behind the reference's
+ * parallel_sample_sortBTCUI_out contestant
+ * (bingmann-parallel_sample_sort.cpp:44-62), whose input array serves as
+ * scratch. output must not overlap strings (output == strings sorts in
+ * place). */
+void pssgpu_sort_strings_out(unsigned char** strings, unsigned char** output, size_t n);
+int pssgpu_sort_strings_out_status(unsigned char** strings, unsigned char** output,
+                                   size_t n);
+
+/* The pointer-array sort for strings that all lie in one caller-owned buffer,
+ * as psstest's string data does (g_string_data / g_string_datasize,
+ * src/psstest.cpp:87-88, which the reference's own contestants declare extern,
+ * src/sinha-copy-burstsort/glue.cpp:33-34). The caller vouches that every
+ * strings[i] and the NUL ending it lie in arena[0, arena_size); a pointer
+ * outside returns PSSGPU_EINVAL. Only the span from the lowest string pointer
+ * to the end of the highest string is read, and it is copied to the device
+ * in one piece, with no per-string host work. output: NULL sorts strings in
+ * place; otherwise as pssgpu_sort_strings_out. lcp and cache (both may be
+ * NULL) as for pssgpu_sort_strings_lcp_cache, indexed by sorted position.
+ * Returns a status code. */
+int pssgpu_sort_strings_arena(const uint8_t* arena, uint64_t arena_size,
+                              unsigned char** strings, unsigned char** output,
+                              uintptr_t* lcp, uint8_t* cache, size_t n);
 
 /* ---- allocation-free sort --------------------------------------------------
  * No counterpart in the reference. Sorts at most PSSGPU_NOALLOC_MAX_STRINGS
@@ -261,8 +289,12 @@ int pssgpu_sort_strings_status(unsigned char** strings, uintptr_t* lcp,
  * calls share it: calls whose GPU work overlaps (other streams, other host
  * threads) race on it, so the caller must serialise them. The first call on
  * a device looks up the array's device address and raises the kernel's
- * shared-memory limit; make that first call before any stream capture.
- * More than PSSGPU_NOALLOC_MAX_STRINGS strings returns PSSGPU_EINVAL. */
+ * shared-memory limit; make that first call before any stream capture. Both
+ * are kept for the life of the process, so calls after a cudaDeviceReset of
+ * that device are not supported.
+ * More than PSSGPU_NOALLOC_MAX_STRINGS strings returns PSSGPU_EINVAL. When a
+ * call fails (an offset outside the arena: PSSGPU_EINVAL), d_perm and d_lcp
+ * hold unspecified values. */
 #define PSSGPU_NOALLOC_MAX_STRINGS 2048
 int pssgpu_sort_device_noalloc(const uint8_t* d_chars, uint64_t nchars,
                                const uint64_t* d_offs, uint64_t n,

@@ -56,6 +56,10 @@ GPU_SIGNATURES = {
     "pssgpu_sort_strings_lcp": (None, [C.c_void_p, C.c_void_p, C.c_size_t]),
     "pssgpu_sort_strings_lcp_cache": (None, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t]),
     "pssgpu_sort_strings_status": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t]),
+    "pssgpu_sort_strings_out": (None, [C.c_void_p, C.c_void_p, C.c_size_t]),
+    "pssgpu_sort_strings_out_status": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t]),
+    "pssgpu_sort_strings_arena": (C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
+                                            C.c_void_p, C.c_void_p, C.c_size_t]),
     "pssgpu_sort_device_noalloc": (C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64,
                                              C.c_void_p, C.c_void_p, C.c_void_p]),
 }
@@ -75,6 +79,9 @@ WORK_SIGNATURES = {
     "pssw_alg_bytes": (None, [C.c_void_p, C.c_uint64, C.c_uint32, C.POINTER(C.c_uint64),
                               C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                               C.POINTER(C.c_uint32)]),
+    "pssw_check_sorted": (C.c_int64, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
+                                      C.c_uint64]),
+    "pssw_check_permutation": (C.c_int, [C.c_void_p, C.c_uint64]),
 }
 
 

@@ -240,3 +240,17 @@ def sort_pointer_array(ptrs, n: int, lcp=None, cache=None) -> int:
     """Call the contestant drop-in on a ctypes ``unsigned char*`` array.
     Returns the status code (the void drop-ins abort on failure instead)."""
     return _native.gpu().pssgpu_sort_strings_status(ptrs, lcp, cache, n)
+
+
+def sort_pointer_array_out(ptrs, output, n: int) -> int:
+    """The separate-output drop-in: sorted pointers into ``output``, ``ptrs``
+    unchanged. Returns the status code."""
+    return _native.gpu().pssgpu_sort_strings_out_status(ptrs, output, n)
+
+
+def sort_pointer_array_arena(arena: int, arena_size: int, ptrs, n: int, output=None, lcp=None,
+                             cache=None) -> int:
+    """The pointer-array sort for strings that all lie in one buffer of
+    ``arena_size`` bytes at address ``arena`` (psstest's string data).
+    ``output`` None sorts in place. Returns the status code."""
+    return _native.gpu().pssgpu_sort_strings_arena(arena, arena_size, ptrs, output, lcp, cache, n)

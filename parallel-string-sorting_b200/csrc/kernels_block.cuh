@@ -86,6 +86,12 @@ __global__ void __launch_bounds__(THREADS, THREADS <= 64 ? 20 : 4) k_block(Work 
     const int buf = sg.meta & META_BUF;
     const uint64_t* ghs = w.hnd[buf];
     uint32_t* err = w.counters + C_ERR;
+    // an offset outside the arena (flagged before this launch) fails the
+    // sort: skip the work on handles that may be corrupt
+    if (threadIdx.x == 0) sm.ng = *(volatile uint32_t*)err & ERR_OFFSET;
+    __syncthreads();
+    if (sm.ng) return;
+    __syncthreads();
     if (sg.meta & META_FINAL) {
         for (uint32_t i = threadIdx.x; i < m; i += THREADS) {
             w.perm[begin + i] = h_id(w, ghs[begin + i]);

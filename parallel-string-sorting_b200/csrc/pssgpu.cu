@@ -14,6 +14,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/pssgpu.h"
@@ -767,57 +768,131 @@ static Ctx* default_ctx(int device, int* rc)
     return ctxs[device];
 }
 
-// Pack a pointer array into (arena, offsets): a dense copy of the span the
-// strings occupy when it is compact (the psstest arena, suffix pointers),
-// else a gather of every string.
-static int sort_pointer_array(unsigned char** strings, uintptr_t* lcp_out, uint8_t* cache,
-                              size_t n)
+// fn(part, lo, hi) over `parts` contiguous slices of [0, n), one host thread
+// per slice.
+template <class F>
+static void host_parts(size_t n, size_t parts, F fn)
+{
+    if (parts <= 1) {
+        fn((size_t)0, (size_t)0, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    th.reserve(parts);
+    for (size_t p = 0; p < parts; ++p)
+        th.emplace_back([&fn, n, parts, p] { fn(p, n * p / parts, n * (p + 1) / parts); });
+    for (auto& t : th) t.join();
+}
+
+// Slices for host_parts: one per 64 Ki items, at most one per hardware thread
+// (capped at 32).
+static size_t host_slices(size_t n)
+{
+    const size_t hw = std::max(1u, std::min(std::thread::hardware_concurrency(), 32u));
+    return std::max<size_t>(1, std::min(hw, n >> 16));
+}
+
+// Pack a pointer array into (arena, offsets), sort it and write the sorted
+// pointers to `out` (== strings: in place, as parallel_sample_sort_base;
+// else a separate output array, as parallel_sample_sort_out_base,
+// bingmann-parallel_sample_sort.hpp:1704-1714, with strings left unchanged).
+// With arena_lo the caller vouches that every string, NUL included, lies in
+// arena_lo[0, arena_size): the span from the lowest string pointer to the end
+// of the highest string is copied as is (psstest's string data, suffix
+// pointers). Without it every string is gathered by strlen / memcpy, so
+// strings in separate allocations are fine and no byte between them is read.
+static int sort_pointer_array(unsigned char** strings, unsigned char** out, uintptr_t* lcp_out,
+                              uint8_t* cache, size_t n, const uint8_t* arena_lo,
+                              uint64_t arena_size)
 {
     if (n > PSSGPU_MAX_STRINGS) return fail(PSSGPU_EINVAL, "too many strings for one call");
-    if (n <= 1) return PSSGPU_OK;
+    if (n == 0) return PSSGPU_OK;
+    if (n == 1) {
+        out[0] = strings[0];
+        return PSSGPU_OK;
+    }
     int rc;
     Ctx* c = default_ctx(0, &rc);
     if (!c) return rc;
     std::lock_guard<std::mutex> lk(c->mu);
-    uintptr_t lo = UINTPTR_MAX, hi = 0;
-    for (size_t i = 0; i < n; ++i) {
-        const uintptr_t p = (uintptr_t)strings[i];
-        lo = std::min(lo, p);
-        hi = std::max(hi, p);
-    }
-    const uint64_t hi_end = hi + strlen((const char*)hi) + 1 - lo;
+    const size_t parts = host_slices(n);
     std::vector<uint64_t> offs(n);
     std::vector<uint8_t> packed;
     const uint8_t* arena;
     uint64_t nchars;
-    if (hi_end <= 8ull * n + (64ull << 20)) {
-        arena = (const uint8_t*)lo;
-        nchars = hi_end;
-        for (size_t i = 0; i < n; ++i) offs[i] = (uintptr_t)strings[i] - lo;
-    } else {
-        uint64_t total = 0;
-        std::vector<uint64_t> len(n);
-        for (size_t i = 0; i < n; ++i) {
-            len[i] = strlen((const char*)strings[i]) + 1;
-            offs[i] = total;
-            total += len[i];
+    if (arena_lo) {
+        const uintptr_t A = (uintptr_t)arena_lo, E = A + arena_size;
+        std::vector<uintptr_t> plo(parts, UINTPTR_MAX), phi(parts, 0);
+        std::vector<char> bad(parts, 0);
+        host_parts(n, parts, [&](size_t p, size_t b, size_t e) {
+            uintptr_t lo = UINTPTR_MAX, hi = 0;
+            for (size_t i = b; i < e; ++i) {
+                const uintptr_t s = (uintptr_t)strings[i];
+                lo = std::min(lo, s);
+                hi = std::max(hi, s);
+            }
+            plo[p] = lo;
+            phi[p] = hi;
+            bad[p] = lo < A || hi >= E;
+        });
+        uintptr_t lo = UINTPTR_MAX, hi = 0;
+        for (size_t p = 0; p < parts; ++p) {
+            if (bad[p]) return fail(PSSGPU_EINVAL, "a string pointer lies outside the arena");
+            lo = std::min(lo, plo[p]);
+            hi = std::max(hi, phi[p]);
         }
-        packed.resize(total);
-        for (size_t i = 0; i < n; ++i) memcpy(packed.data() + offs[i], strings[i], len[i]);
+        const size_t tail = strnlen((const char*)hi, E - hi);
+        if (tail == E - hi) return fail(PSSGPU_EINVAL, "a string is not terminated inside the arena");
+        arena = (const uint8_t*)lo;
+        nchars = hi + tail + 1 - lo;
+        host_parts(n, parts, [&](size_t, size_t b, size_t e) {
+            for (size_t i = b; i < e; ++i) offs[i] = (uintptr_t)strings[i] - lo;
+        });
+    } else {
+        // lengths per slice, slice bases, then offsets and copies
+        std::vector<uint64_t> base(parts + 1, 0);
+        host_parts(n, parts, [&](size_t p, size_t b, size_t e) {
+            uint64_t t = 0;
+            for (size_t i = b; i < e; ++i) {
+                offs[i] = t;
+                t += strlen((const char*)strings[i]) + 1;
+            }
+            base[p + 1] = t;
+        });
+        for (size_t p = 0; p < parts; ++p) base[p + 1] += base[p];
+        nchars = base[parts];
+        packed.resize(nchars);
+        host_parts(n, parts, [&](size_t p, size_t b, size_t e) {
+            for (size_t i = b; i < e; ++i) {
+                const uint64_t o = base[p] + offs[i];
+                const uint64_t len = (i + 1 < e ? offs[i + 1] + base[p] : base[p + 1]) - o;
+                memcpy(packed.data() + o, strings[i], len);
+                offs[i] = o;
+            }
+        });
         arena = packed.data();
-        nchars = total;
     }
     std::vector<uint32_t> perm(n);
     std::vector<uint32_t> lcp32(lcp_out ? n : 0);
     rc = sort_host_locked(c, arena, nchars, offs.data(), n, perm.data(),
                           lcp_out ? lcp32.data() : nullptr);
     if (rc) return rc;
-    std::vector<unsigned char*> orig(strings, strings + n);
-    for (size_t i = 0; i < n; ++i) strings[i] = orig[perm[i]];
-    if (lcp_out)
-        for (size_t i = 1; i < n; ++i) lcp_out[i] = lcp32[i];
-    if (cache && lcp_out)
-        for (size_t i = 1; i < n; ++i) cache[i] = strings[i][lcp_out[i]];
+    std::vector<unsigned char*> orig;
+    unsigned char* const* src = strings;
+    if (out == strings) {
+        orig.resize(n);
+        host_parts(n, parts, [&](size_t, size_t b, size_t e) {
+            memcpy(orig.data() + b, strings + b, (e - b) * sizeof(unsigned char*));
+        });
+        src = orig.data();
+    }
+    host_parts(n, parts, [&](size_t, size_t b, size_t e) {
+        for (size_t i = b; i < e; ++i) out[i] = src[perm[i]];
+        if (lcp_out)
+            for (size_t i = std::max<size_t>(b, 1); i < e; ++i) lcp_out[i] = lcp32[i];
+        if (cache && lcp_out)
+            for (size_t i = std::max<size_t>(b, 1); i < e; ++i) cache[i] = out[i][lcp_out[i]];
+    });
     return PSSGPU_OK;
 }
 
@@ -1318,7 +1393,26 @@ int pssgpu_sort_batch_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t n
 int pssgpu_sort_strings_status(unsigned char** strings, uintptr_t* lcp, uint8_t* cache, size_t n)
 {
     if (n && !strings) return fail(PSSGPU_EINVAL, "null string array");
-    return sort_pointer_array(strings, lcp, cache, n);
+    return sort_pointer_array(strings, strings, lcp, cache, n, nullptr, 0);
+}
+
+int pssgpu_sort_strings_arena(const uint8_t* arena, uint64_t arena_size, unsigned char** strings,
+                              unsigned char** output, uintptr_t* lcp, uint8_t* cache, size_t n)
+{
+    if (n && (!strings || !arena)) return fail(PSSGPU_EINVAL, "null string array or arena");
+    if (output == strings) output = nullptr;
+    if (output && n && output < strings + n && strings < output + n)
+        return fail(PSSGPU_EINVAL, "output overlaps the input array");
+    return sort_pointer_array(strings, output ? output : strings, lcp, cache, n, arena, arena_size);
+}
+
+int pssgpu_sort_strings_out_status(unsigned char** strings, unsigned char** output, size_t n)
+{
+    if (n && (!strings || !output)) return fail(PSSGPU_EINVAL, "null string array");
+    if (output == strings) return sort_pointer_array(strings, strings, nullptr, nullptr, n, nullptr, 0);
+    if (n && output < strings + n && strings < output + n)
+        return fail(PSSGPU_EINVAL, "output overlaps the input array");
+    return sort_pointer_array(strings, output, nullptr, nullptr, n, nullptr, 0);
 }
 
 static void die_on(int rc)
@@ -1342,6 +1436,11 @@ void pssgpu_sort_strings_lcp(unsigned char** strings, uintptr_t* lcp, size_t n)
 void pssgpu_sort_strings_lcp_cache(uint8_t** strings, uintptr_t* lcp, uint8_t* cache, size_t n)
 {
     die_on(pssgpu_sort_strings_status(strings, lcp, cache, n));
+}
+
+void pssgpu_sort_strings_out(unsigned char** strings, unsigned char** output, size_t n)
+{
+    die_on(pssgpu_sort_strings_out_status(strings, output, n));
 }
 
 }  // extern "C"

@@ -1,5 +1,5 @@
-// workgen.cpp -- seeded synthetic workloads and the algorithmic-byte model
-// (libpsswork.so, host only, OpenMP).
+// workgen.cpp -- seeded synthetic workloads, the algorithmic-byte model and
+// output checks of the benchmark (libpsswork.so, host only, OpenMP).
 //
 // Every generator is counter-based (splitmix64 of seed, stream, index), so
 // the output does not depend on the thread count. Arenas are NUL-terminated
@@ -221,6 +221,55 @@ void pssw_alg_bytes(const uint32_t* lcp, uint64_t n, uint32_t T, uint64_t* out_t
     if (out_rounds_bytes) *out_rounds_bytes = rounds_bytes;
     if (out_base_bytes) *out_base_bytes = base_bytes;
     if (out_max_round) *out_max_round = max_round;
+}
+
+// ---- output checks of a sort (measurement side: the benchmark verifies the
+// permutation of a timed sort with these) ----
+// The first position p >= 1 where string perm[p-1] > string perm[p]
+// (unsigned bytewise, as strcmp), or where an id is out of range; -1 when
+// the order holds. chars[nchars - 1] must be NUL.
+int64_t pssw_check_sorted(const uint8_t* chars, uint64_t nchars, const uint64_t* offs,
+                          const uint32_t* perm, uint64_t n)
+{
+    int64_t first = INT64_MAX;
+    if (nchars == 0 || chars[nchars - 1] != 0) return 0;
+#pragma omp parallel for schedule(static) reduction(min : first)
+    for (int64_t p = 0; p < (int64_t)n; ++p) {
+        const uint32_t b = perm[p];
+        if (b >= n || offs[b] >= nchars) {
+            first = std::min(first, p);
+            continue;
+        }
+        if (p == 0) continue;
+        const uint32_t a = perm[p - 1];
+        if (a >= n || offs[a] >= nchars) continue;  // reported at p - 1
+        if (strcmp((const char*)chars + offs[a], (const char*)chars + offs[b]) > 0)
+            first = std::min(first, p);
+    }
+    return first == INT64_MAX ? -1 : first;
+}
+
+// 1 when perm[0, n) holds every id 0..n-1 exactly once.
+int pssw_check_permutation(const uint32_t* perm, uint64_t n)
+{
+    std::vector<uint8_t> seen(n, 0);
+    int ok = 1;
+#pragma omp parallel for schedule(static) reduction(min : ok)
+    for (int64_t p = 0; p < (int64_t)n; ++p) {
+        const uint32_t v = perm[p];
+        if (v >= n) {
+            ok = 0;
+            continue;
+        }
+        // a byte store races only with another occurrence of v, which the
+        // count below reports either way
+        seen[v] = 1;
+    }
+    if (!ok) return 0;
+    uint64_t cnt = 0;
+#pragma omp parallel for schedule(static) reduction(+ : cnt)
+    for (int64_t i = 0; i < (int64_t)n; ++i) cnt += seen[i];
+    return cnt == n ? 1 : 0;
 }
 
 }  // extern "C"

@@ -149,6 +149,21 @@ def alg_bytes(lcp: np.ndarray, T: int = 32) -> dict:
     return {"total": tot.value, "rounds": rb.value, "base": bb.value, "max_round": mr.value}
 
 
+def check_sorted(chars: np.ndarray, nchars: int, offs: np.ndarray, perm: np.ndarray) -> int:
+    """First position whose string sorts before its predecessor (or whose id
+    is out of range); -1 when perm lists the strings in order."""
+    offs = np.ascontiguousarray(offs, dtype=np.uint64)
+    perm = np.ascontiguousarray(perm, dtype=np.uint32)
+    return int(_native.work().pssw_check_sorted(chars.ctypes.data, nchars, offs.ctypes.data,
+                                                perm.ctypes.data, perm.shape[0]))
+
+
+def check_permutation(perm: np.ndarray) -> bool:
+    """True when perm holds every id 0..n-1 exactly once."""
+    perm = np.ascontiguousarray(perm, dtype=np.uint32)
+    return bool(_native.work().pssw_check_permutation(perm.ctypes.data, perm.shape[0]))
+
+
 def string_lengths(chars: np.ndarray, offs: np.ndarray) -> np.ndarray:
     """strlen of every string of the arena."""
     zeros = np.flatnonzero(np.asarray(chars) == 0).astype(np.uint64)

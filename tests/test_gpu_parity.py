@@ -428,17 +428,95 @@ def test_pointer_array_dropins(pkg, orc):
 
 
 def test_suffix_pointer_array_dense_span(pkg, orc):
-    """Overlapping suffix pointers (psstest --suffix) take the dense-span path."""
-    lib = pkg._native.gpu()
+    """Overlapping suffix pointers (psstest --suffix) through the arena entry,
+    which copies the text span once, and through the plain entry, which
+    gathers every suffix."""
     text = pkg.workloads.dna_text(length=20000, seed=15)
     buf = (C.c_ubyte * len(text)).from_buffer_copy(text.tobytes())
     base = C.addressof(buf)
     n = 20001
-    ptrs = (C.c_void_p * n)(*[base + i for i in range(n)])
-    assert pkg.sort_pointer_array(ptrs, n) == 0
-    sa = np.array([p - base for p in ptrs], dtype=np.uint64)
     offs = np.arange(n, dtype=np.uint64)
+    ptrs = (C.c_void_p * n)(*[base + i for i in range(n)])
+    assert pkg.sort_pointer_array_arena(base, 20001, ptrs, n) == 0
+    sa = np.array([p - base for p in ptrs], dtype=np.uint64)
+    assert orc.check_permutation(sa.astype(np.uint32))
     assert orc.check_order(text, offs, sa.astype(np.uint32)) == -1
+    m = 3001  # plain entry: every suffix gathered (quadratic bytes, kept small)
+    ptrs = (C.c_void_p * m)(*[base + 17000 + i for i in range(m)])
+    assert pkg.sort_pointer_array(ptrs, m) == 0
+    got = np.array([p - base - 17000 for p in ptrs], dtype=np.uint32)
+    assert np.array_equal(np.sort(got), np.arange(m, dtype=np.uint32))
+    assert orc.check_order(text[17000:], np.arange(m, dtype=np.uint64), got) == -1
+
+
+def test_pointer_array_separate_allocations(pkg, orc):
+    """Strings in separate host allocations: the plain entry reads each string
+    through its own pointer and nothing between them."""
+    strings = [bytes([97 + (i * 7 + j) % 3 for j in range(i % 13)]) for i in range(5000)]
+    bufs = [C.create_string_buffer(s) for s in strings]
+    n = len(bufs)
+    addr = [C.addressof(b) for b in bufs]
+    ptrs = (C.c_void_p * n)(*addr)
+    assert pkg.sort_pointer_array(ptrs, n) == 0
+    index = {a: i for i, a in enumerate(addr)}
+    got = [strings[index[p]] for p in ptrs]
+    assert sorted(index[p] for p in ptrs) == list(range(n))
+    assert got == sorted(strings)
+
+
+def test_pointer_array_out_and_arena(pkg, orc):
+    """The separate-output entry leaves the input unchanged; the arena entry
+    sorts in place or into an output array, with LCP and cache, and rejects a
+    pointer outside the arena it was given."""
+    chars, offs, nchars = pkg.workloads.random_strings(40000, 0, 14, b"abcd", 16)
+    buf = (C.c_ubyte * len(chars)).from_buffer_copy(chars.tobytes())
+    base = C.addressof(buf)
+    n = len(offs)
+    ptr_t = C.c_void_p * n
+    ids, rlcp = orc.sort_ids_lcp(chars, offs)
+    want = orc.sorted_strings(chars, offs, ids)
+    raw = chars.tobytes()
+
+    def sequence(ptrs):
+        got_offs = np.array([p - base for p in ptrs], dtype=np.uint64)
+        assert np.array_equal(np.sort(got_offs), np.sort(offs))
+        return orc.sorted_strings(chars, got_offs, np.arange(n))
+
+    src = [base + int(o) for o in offs]
+    ptrs, out = ptr_t(*src), ptr_t()
+    assert pkg.sort_pointer_array_out(ptrs, out, n) == 0
+    assert list(ptrs) == src
+    assert sequence(out) == want
+
+    ptrs = ptr_t(*src)
+    lib = pkg._native.gpu()
+    lib.pssgpu_sort_strings_out(ptrs, out, n)
+    assert list(ptrs) == src and sequence(out) == want
+
+    ptrs, out = ptr_t(*src), ptr_t()
+    lcp = (C.c_size_t * n)()
+    lcp[0] = 42
+    cache = (C.c_ubyte * n)()
+    assert pkg.sort_pointer_array_arena(base, nchars, ptrs, n, out, lcp, cache) == 0
+    assert list(ptrs) == src
+    assert sequence(out) == want
+    assert lcp[0] == 42
+    assert np.array_equal(np.array(lcp[1:], dtype=np.uint64), rlcp[1:])
+    for i in range(1, n, 89):
+        assert cache[i] == raw[out[i] - base + lcp[i]]
+
+    ptrs = ptr_t(*src)
+    assert pkg.sort_pointer_array_arena(base, nchars, ptrs, n) == 0
+    assert sequence(ptrs) == want
+
+    # a pointer beyond the declared arena, and a string not terminated inside it
+    ptrs = ptr_t(*src)
+    assert pkg.sort_pointer_array_arena(base, int(offs[-1]), ptrs, n) == 1
+    assert list(ptrs) == src
+    last_len = raw.index(b"\0", int(offs[-1])) - int(offs[-1])
+    rc = pkg.sort_pointer_array_arena(base, int(offs[-1]) + 1, ptrs, n)
+    assert rc == (1 if last_len > 0 else 0)
+    assert pkg.sort_pointer_array_out(ptrs, ptrs, n) == 0  # output == input: in place
 
 
 def test_errors_are_status_codes(pkg, ctx):

@@ -20,8 +20,8 @@ pytestmark = pytest.mark.gpu
 ROOT = Path(__file__).resolve().parent.parent
 PSSTEST = ROOT / "oracle" / "_ref" / "psstest"
 
-CONTESTANTS = ["gpu/sample_sort", "gpu/sample_sort_lcp", "gpu/sample_sort_lcp_cache",
-               "bingmann/parallel_sample_sortBTCUI"]
+GPU_CONTESTANTS = ["gpu/sample_sort", "gpu/sample_sort_lcp", "gpu/sample_sort_lcp_cache",
+                   "gpu/sample_sort_out"]
 
 
 def run_psstest(path, algo, suffix=False):
@@ -65,7 +65,10 @@ def test_psstest_checks_gpu_contestants(inputs, name, suffix):
     assert PSSTEST.exists(), "oracle/_ref/psstest is built by __graft_entry__.build()"
     ref = run_psstest(inputs[name], "bingmann/parallel_sample_sortBTCUI", suffix)
     assert ref["status"] == "ok"
-    for algo in CONTESTANTS[:3]:
+    ref_out = run_psstest(inputs[name], "bingmann/parallel_sample_sortBTCUI_out", suffix)
+    assert ref_out["status"] == "ok"
+    assert (ref_out["dprefix"], ref_out["lcpsum"]) == (ref["dprefix"], ref["lcpsum"])
+    for algo in GPU_CONTESTANTS:
         r = run_psstest(inputs[name], algo, suffix)
         assert r["status"] == "ok", (algo, r)
         assert r["algo"] == algo

@@ -1,6 +1,7 @@
 """GPU tests of the request server (continuous batching under an HBM budget):
-every request's result is the same as sorting it alone, admission waits for
-slab space instead of failing, and impossible requests are refused."""
+every sampled request's result equals the oracle's sort of that request and
+the same request sorted alone, admission waits for slab space instead of
+failing, and impossible requests are refused."""
 import numpy as np
 import pytest
 
@@ -24,7 +25,14 @@ def alone(pkg, ctx, pool, r):
     return ctx.sort_host(chars, offs, lcp=True), chars, offs
 
 
-def test_results_same_alone_and_in_mix(pkg, serving, pools, ctx):
+def oracle_ids(orc, chars, offs):
+    """The oracle's canonical ids and LCP array of one request."""
+    ids, rlcp = orc.sort_ids_lcp(chars, offs)
+    from golden_util import canonical_ids
+    return canonical_ids(chars, offs, ids, rlcp), rlcp
+
+
+def test_results_same_alone_and_in_mix(pkg, orc, serving, pools, ctx):
     reqs = serving.make_stream(pools, rate=4000, duration=0.1, min_bytes=1 << 10,
                                max_bytes=2 << 20, seed=3)
     assert len(reqs) > 200
@@ -41,12 +49,17 @@ def test_results_same_alone_and_in_mix(pkg, serving, pools, ctx):
         r = reqs[k]
         (p1, l1), chars, offs = alone(pkg, ctx, pools[r.alphabet], r)
         assert r.info["status"] == 0
-        assert np.array_equal(r.lcp[1:], l1[1:])
         cw = pkg.workloads.canonical_ids
-        assert np.array_equal(cw(chars, offs, r.perm, r.lcp), cw(chars, offs, p1, l1))
+        want, rlcp = oracle_ids(orc, chars, offs)
+        # in the mix: equal to the oracle
+        assert np.array_equal(r.lcp[1:].astype(np.uint64), rlcp[1:])
+        assert np.array_equal(cw(chars, offs, r.perm, r.lcp), want)
+        # alone: equal to the oracle, hence to the result in the mix
+        assert np.array_equal(l1[1:].astype(np.uint64), rlcp[1:])
+        assert np.array_equal(cw(chars, offs, p1, l1), want)
 
 
-def test_admission_waits_for_space(pkg, serving, pools, ctx):
+def test_admission_waits_for_space(pkg, orc, serving, pools, ctx):
     # a budget whose slab holds only a few requests at a time
     srv = serving.Server(budget=160 << 20, workers=2, max_batch_strings=1 << 16)
     try:
@@ -62,13 +75,14 @@ def test_admission_waits_for_space(pkg, serving, pools, ctx):
     finally:
         srv.close()
     for r in reqs[:20]:
-        (p1, l1), chars, offs = alone(pkg, ctx, pools[r.alphabet], r)
-        ids = pkg.workloads.canonical_ids
+        pool = pools[r.alphabet]
+        chars = pool.chars[r.start:r.start + r.nchars]
+        offs = pool.offs[r.i0:r.i1] - np.uint64(r.start)
         # equal strings may come in another order: compare the sorted bytes
-        raw = chars.tobytes()
-        got = [raw[int(offs[i]):raw.index(b"\0", int(offs[i]))] for i in r.perm]
-        want = [raw[int(offs[i]):raw.index(b"\0", int(offs[i]))] for i in p1]
-        assert got == want
+        # with the oracle's
+        ids = orc.sort_ids(chars, offs)
+        assert orc.check_permutation(r.perm)
+        assert orc.sorted_strings(chars, offs, r.perm) == orc.sorted_strings(chars, offs, ids)
 
 
 def test_refuses_requests_beyond_the_budget(pkg, serving):

@@ -111,3 +111,26 @@ def test_alg_bytes_hand_count(pkg):
     need = [4, 4, 6, 6, 1, 1, 1, 1, 1, 1]
     assert r["rounds"] == 0
     assert r["base"] == sum(12 + x for x in need)
+
+
+def test_bench_output_checks_catch_planted_mistakes(pkg, orc):
+    """The checks bench.py runs on its timed output: a correct sort passes; a
+    swapped pair, a duplicated id and an out-of-range id are caught."""
+    w = pkg.workloads
+    chars, offs, nchars = w.random_strings(5000, 0, 9, b"abc", 31)
+    ids = orc.sort_ids(chars[:nchars], offs)
+    assert w.check_permutation(ids) and w.check_sorted(chars, nchars, offs, ids) == -1
+    # a swap of two different neighbours (the first pair that differs)
+    lcp = orc.lcp_array(chars, offs, ids)
+    lens = w.string_lengths(chars[:nchars + 1], offs)[ids]
+    p = next(i for i in range(1, len(ids)) if not (lcp[i] == lens[i] == lens[i - 1]))
+    bad = ids.copy()
+    bad[p - 1], bad[p] = bad[p], bad[p - 1]
+    assert w.check_permutation(bad) and w.check_sorted(chars, nchars, offs, bad) == p
+    dup = ids.copy()
+    dup[7] = dup[8]
+    assert not w.check_permutation(dup)
+    oob = ids.copy()
+    oob[11] = len(ids)
+    assert not w.check_permutation(oob)
+    assert w.check_sorted(chars, nchars, offs, oob) == 11

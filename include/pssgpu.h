@@ -91,9 +91,17 @@ int pssgpu_ctx_kernel_stats(pssgpu_ctx* ctx, pssgpu_kernel_stats* out, int max);
  * PSSGPU_OPT_INDIRECT_HANDLES: carry bare string ids through the sort and
  * read offsets from the offset array at every gather -- the path a sort takes
  * on its own when an id and an arena offset do not fit one 64-bit handle;
- * for testing that path on small inputs. */
+ * for testing that path on small inputs.
+ * PSSGPU_OPT_SINGLE_LAUNCH (default 1): a single-instance sort whose strings
+ * fit one wave of resident blocks (about 1.2 M strings on a B200) runs as one
+ * cooperative kernel launch, with no host round trip between its steps;
+ * 0 sends every sort through the multi-launch pass loop.
+ * PSSGPU_OPT_WAIT_LIMIT (default 4,194,304): polls of a grid-barrier wait in
+ * that kernel before it gives up and the sort returns PSSGPU_ETIMEOUT. */
 #define PSSGPU_OPT_PROFILE 1
 #define PSSGPU_OPT_INDIRECT_HANDLES 2
+#define PSSGPU_OPT_SINGLE_LAUNCH 3
+#define PSSGPU_OPT_WAIT_LIMIT 4
 int pssgpu_ctx_set_option(pssgpu_ctx* ctx, int option, int64_t value);
 
 /* ---- arena sorts ---------------------------------------------------------

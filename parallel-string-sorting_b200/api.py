@@ -79,6 +79,8 @@ class Context:
 
     OPT_PROFILE = 1
     OPT_INDIRECT_HANDLES = 2
+    OPT_SINGLE_LAUNCH = 3
+    OPT_WAIT_LIMIT = 4
 
     def set_option(self, option: int, value: int) -> None:
         _check(_native.gpu().pssgpu_ctx_set_option(self._h, option, value))

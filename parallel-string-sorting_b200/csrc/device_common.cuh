@@ -14,9 +14,10 @@ namespace pssgpu {
 // Error bits OR-ed into the device error word and mapped to status codes.
 enum : uint32_t {
     ERR_OFFSET = 1u,     // a string offset lies outside the arena
-    ERR_TIMEOUT = 2u,    // a bounded device-side wait gave up (no kernel waits at present)
+    ERR_TIMEOUT = 2u,    // a bounded device-side wait gave up (grid barriers of k_wave)
     ERR_OVERFLOW = 4u,   // a work list exceeded its capacity
     ERR_INTERNAL = 8u,   // an internal invariant failed (index out of range)
+    ERR_UNTERMINATED = 16u,  // the arena's last char is not NUL
 };
 
 struct Seg {

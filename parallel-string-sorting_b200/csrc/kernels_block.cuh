@@ -75,41 +75,19 @@ __device__ __forceinline__ void blk_push(BlockSmem<MAXN>& sm, uint32_t start, ui
     }
 }
 
+// The block sorter proper. On entry the block's strings are in
+// sm.hnd[0, m) (keys in sm.key where a group's keys are valid), their output
+// positions are begin + [0, m), and the initial groups are pushed (sm.ng /
+// sm.nw lists, blk_push); strings in no group are final where they stand.
+// Runs the sample-sort steps on groups of more than 32 strings, the warp
+// windows on the rest, and writes perm[begin, begin + m). buf is the
+// ping-pong buffer the strings came from (stalled warp groups are handed to
+// the deep-group list there, when the Work has one). All threads call.
 template <int MAXN, int THREADS>
-__global__ void __launch_bounds__(THREADS, THREADS <= 64 ? 20 : 4) k_block(Work w, const Seg* list)
+__device__ __forceinline__ void block_sort_groups(const Work& w, BlockSmem<MAXN>& sm,
+                                                  uint32_t begin, uint32_t m, int buf,
+                                                  uint32_t (*wscratch)[32], uint32_t* err)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    BlockSmem<MAXN>& sm = *reinterpret_cast<BlockSmem<MAXN>*>(smem_raw);
-    __shared__ uint32_t wscratch[THREADS / 32][32];
-    const Seg sg = list[blockIdx.x];
-    const uint32_t m = sg.size, begin = sg.begin;
-    const int buf = sg.meta & META_BUF;
-    const uint64_t* ghs = w.hnd[buf];
-    uint32_t* err = w.counters + C_ERR;
-    // an offset outside the arena (flagged before this launch) fails the
-    // sort: skip the work on handles that may be corrupt
-    if (threadIdx.x == 0) sm.ng = *(volatile uint32_t*)err & ERR_OFFSET;
-    __syncthreads();
-    if (sm.ng) return;
-    __syncthreads();
-    if (sg.meta & META_FINAL) {
-        for (uint32_t i = threadIdx.x; i < m; i += THREADS) {
-            w.perm[begin + i] = h_id(w, ghs[begin + i]);
-            if (w.lcp && i) w.lcp[begin + i] = sg.depth;
-        }
-        return;
-    }
-    const bool valid0 = sg.meta & META_VALID;
-    for (uint32_t i = threadIdx.x; i < m; i += THREADS) {
-        sm.hnd[i] = __ldg(ghs + begin + i);
-        if (valid0) sm.key[i] = __ldg(w.keys[buf] + begin + i);
-    }
-    if (threadIdx.x == 0) {
-        sm.ng = 0;
-        sm.nw = 0;
-        blk_push<MAXN, THREADS>(sm, 0, m, sg.depth, valid0, err);
-    }
-    __syncthreads();
     while (true) {
         if (threadIdx.x == 0) {
             if (sm.ng) {
@@ -299,6 +277,44 @@ __global__ void __launch_bounds__(THREADS, THREADS <= 64 ? 20 : 4) k_block(Work 
     });
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < m; i += THREADS) w.perm[begin + i] = h_id(w, sm.hnd[i]);
+}
+
+template <int MAXN, int THREADS>
+__global__ void __launch_bounds__(THREADS, THREADS <= 64 ? 20 : 4) k_block(Work w, const Seg* list)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    BlockSmem<MAXN>& sm = *reinterpret_cast<BlockSmem<MAXN>*>(smem_raw);
+    __shared__ uint32_t wscratch[THREADS / 32][32];
+    const Seg sg = list[blockIdx.x];
+    const uint32_t m = sg.size, begin = sg.begin;
+    const int buf = sg.meta & META_BUF;
+    const uint64_t* ghs = w.hnd[buf];
+    uint32_t* err = w.counters + C_ERR;
+    // an offset outside the arena (flagged before this launch) fails the
+    // sort: skip the work on handles that may be corrupt
+    if (threadIdx.x == 0) sm.ng = *(volatile uint32_t*)err & ERR_OFFSET;
+    __syncthreads();
+    if (sm.ng) return;
+    __syncthreads();
+    if (sg.meta & META_FINAL) {
+        for (uint32_t i = threadIdx.x; i < m; i += THREADS) {
+            w.perm[begin + i] = h_id(w, ghs[begin + i]);
+            if (w.lcp && i) w.lcp[begin + i] = sg.depth;
+        }
+        return;
+    }
+    const bool valid0 = sg.meta & META_VALID;
+    for (uint32_t i = threadIdx.x; i < m; i += THREADS) {
+        sm.hnd[i] = __ldg(ghs + begin + i);
+        if (valid0) sm.key[i] = __ldg(w.keys[buf] + begin + i);
+    }
+    if (threadIdx.x == 0) {
+        sm.ng = 0;
+        sm.nw = 0;
+        blk_push<MAXN, THREADS>(sm, 0, m, sg.depth, valid0, err);
+    }
+    __syncthreads();
+    block_sort_groups<MAXN, THREADS>(w, sm, begin, m, buf, wscratch, err);
 }
 
 #define K_BLOCK_A k_block<SMALL_A, SMALL_A_THREADS>

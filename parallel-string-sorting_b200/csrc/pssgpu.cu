@@ -20,6 +20,7 @@
 #include "../../include/pssgpu.h"
 #include "kernels_big.cuh"
 #include "kernels_block.cuh"
+#include "kernels_wave.cuh"
 #include "prepare.cuh"
 #include "merge.cuh"
 
@@ -43,6 +44,8 @@ static int fail(int code, const std::string& msg)
 
 __global__ void k_init(Work w)
 {
+    if (blockIdx.x == 0 && threadIdx.x == 0 && w.chars[w.nchars - 1] != 0)
+        set_error(w.counters + C_ERR, ERR_UNTERMINATED);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < w.n; i += gridDim.x * blockDim.x) {
         w.hnd[0][i] = h_make(w, i, w.offs[i]);
         if (w.offs[i] >= w.nchars) set_error(w.counters + C_ERR, ERR_OFFSET);
@@ -130,15 +133,16 @@ static uint64_t workspace_bytes(const Sizes& s)
     b += 2 * align256(4ull * MAX_BKT * s.tile_cap);  // tile and chunk counts (chunks <= tiles)
     b += 2 * align256(16 * s.deep_cap);            // deep-group lists
     b += align256(4 * C_COUNT);                    // counters
+    b += align256(sizeof(WaveState));              // single-launch sort state
     return b;
 }
 
 // Kernel classes reported by pssgpu_ctx_kernel_stats.
 enum KClass { K_INIT = 0, K_SAMPLE, K_CLASSIFY, K_BSTART, K_SCATTER, K_CHILDREN, K_TINY,
-              K_SMALLA, K_SMALLB, K_DEEP, K_BOUNDARY, K_NCLASS };
+              K_SMALLA, K_SMALLB, K_DEEP, K_BOUNDARY, K_WAVE, K_NCLASS };
 static const char* const kclass_name[K_NCLASS] = {
     "init", "sample", "classify", "bstart", "scatter", "children", "tiny",
-    "small256", "small1024", "deep", "boundary"};
+    "small256", "small1024", "deep", "boundary", "wave"};
 
 struct KStat {
     uint32_t launches = 0;
@@ -157,6 +161,7 @@ struct Ctx {
     uint64_t ws_bytes = 0;
     Sizes cap{};
     Work base{};
+    WaveState* wave = nullptr;          // right behind the counters (one memset)
     uint32_t* host_counters = nullptr;  // pinned
     // staging for the host entry points
     unsigned char* io = nullptr;
@@ -179,6 +184,11 @@ struct Ctx {
     // carry bare ids and read offsets through offs[] (the path taken when
     // id and offset do not fit one 64-bit handle); settable for testing
     bool indirect_handles = false;
+    // inputs that fit one wave of resident blocks sort in one cooperative
+    // launch (k_wave); off: always the level-synchronous passes
+    bool single_launch = true;
+    // polls of a grid-barrier wait in k_wave before it gives up
+    uint32_t wait_limit = 1u << 22;
     // splitter-tree levels per size class of big segments (0 = default)
     uint8_t tree_bits_by_size[33] = {};
     // device copy of a batch's instance boundaries
@@ -266,14 +276,19 @@ static int ensure_workspace(Ctx* c, uint64_t n)
     for (int i = 0; i < 2; ++i) w.deep[i] = (Seg*)take(16 * s.deep_cap);
     w.deep_cap = (uint32_t)s.deep_cap;
     w.counters = (uint32_t*)take(4 * C_COUNT);
+    c->wave = (WaveState*)take(sizeof(WaveState));
     return PSSGPU_OK;
 }
 
 // Shared-memory limits of the kernels that need more than 48 KB, set once
-// per device (the attribute belongs to the device's context).
+// per device (the attribute belongs to the device's context), and the
+// number of k_wave blocks one wave holds on that device (0: no
+// cooperative launch).
+constexpr int MAXDEV = 64;
+static uint32_t g_wave_blocks[MAXDEV];
+
 static int setup_kernels()
 {
-    constexpr int MAXDEV = 64;
     static bool done[MAXDEV] = {};
     static std::mutex mu;
     int dev = 0;
@@ -281,6 +296,16 @@ static int setup_kernels()
     if (dev < 0 || dev >= MAXDEV) return fail(PSSGPU_ENODEV, "device index out of range");
     std::lock_guard<std::mutex> lk(mu);
     if (done[dev]) return PSSGPU_OK;
+    PSS_CUDA(cudaFuncSetAttribute(k_wave, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sizeof(WaveSmem)));
+    {
+        int coop = 0, sms = 0, per_sm = 0;
+        PSS_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+        PSS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        PSS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_wave, WAVE_THREADS,
+                                                               sizeof(WaveSmem)));
+        g_wave_blocks[dev] = coop ? (uint32_t)(per_sm * sms) : 0u;
+    }
     PSS_CUDA(cudaFuncSetAttribute(K_BLOCK_A, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)sizeof(BlockSmem<SMALL_A>)));
     PSS_CUDA(cudaFuncSetAttribute(K_BLOCK_B, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -293,6 +318,7 @@ static int setup_kernels()
 
 static int map_device_error(uint32_t err)
 {
+    if (err & ERR_UNTERMINATED) return fail(PSSGPU_EINVAL, "arena does not end with NUL");
     if (err & ERR_OFFSET) return fail(PSSGPU_EINVAL, "a string offset lies outside the arena");
     if (err & ERR_TIMEOUT) return fail(PSSGPU_ETIMEOUT, "a bounded device-side wait gave up");
     if (err & ERR_OVERFLOW) return fail(PSSGPU_ECUDA, "an internal work list overflowed");
@@ -320,31 +346,64 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
     for (int k = 0; k < K_NCLASS; ++k) c->kstat[k] = KStat{};
     KTimer kt{c, st};
     const uint64_t out_bytes = lcp ? 8 : 4;  // perm (+ lcp) per string
+    // An input that fits one wave of resident k_wave blocks sorts in one
+    // cooperative launch; what it leaves (buckets over WAVE_SORT_MAX strings,
+    // deep groups) continues in the passes below from the lists of parity 1.
+    const uint32_t wave_cap = g_wave_blocks[c->device];
+    const bool wave = !d_inst && c->single_launch && n >= 2 && wave_cap > 0 &&
+                      (uint64_t)n <= (uint64_t)wave_cap * WAVE_TILE_MAX;
+    int cur = 0;
     PSS_CUDA(cudaEventRecord(c->ev0, st));
-    PSS_CUDA(cudaMemsetAsync(w.counters, 0, 4 * C_COUNT, st));
-    kt.begin(K_INIT);
-    k_init<<<1184, 256, 0, st>>>(w);
-    k_roots<<<d_inst ? 148 : 1, 256, 0, st>>>(w, d_inst, ninst);
-    kt.end(K_INIT);
-    c->kstat[K_INIT].launches += 2;
-    c->kstat[K_INIT].strings += n;
-    c->kstat[K_INIT].alg_bytes += 12ull * n;  // offset read + id write
-    stats.kernel_launches += 2;
+    if (wave) {
+        // the counters and the wave state's header are adjacent: one memset
+        const size_t head = (size_t)((unsigned char*)c->wave - (unsigned char*)w.counters) +
+                            offsetof(WaveState, gcount);
+        PSS_CUDA(cudaMemsetAsync(w.counters, 0, head, st));
+        uint32_t G = std::min<uint32_t>(wave_cap, std::max<uint32_t>(1u, (n + WAVE_WINDOW - 1) / WAVE_WINDOW));
+        G = std::max<uint32_t>(G, (n + WAVE_TILE_MAX - 1) / WAVE_TILE_MAX);
+        // about 128 strings per bucket slot, at most WAVE_MAX_BITS levels
+        const uint32_t lg = bit_length(n) - 1;
+        uint32_t L = std::min<uint32_t>(WAVE_MAX_BITS, lg > 8 ? lg - 7 : 1u);
+        w.cur = 0;
+        WaveState* ws = c->wave;
+        uint32_t limit = c->wait_limit;
+        void* args[] = {&w, &ws, &L, &limit};
+        kt.begin(K_WAVE);
+        PSS_CUDA(cudaLaunchCooperativeKernel((const void*)k_wave, dim3(G), dim3(WAVE_THREADS), args,
+                                             sizeof(WaveSmem), st));
+        kt.end(K_WAVE);
+        c->kstat[K_WAVE].launches += 1;
+        c->kstat[K_WAVE].strings += n;
+        // offset 8 + chars 8 read, key + handle 16 written and read back, output
+        c->kstat[K_WAVE].alg_bytes += (48 + out_bytes) * n;
+        stats.kernel_launches += 1;
+        stats.passes += 1;
+        cur = 1;
+    } else {
+        PSS_CUDA(cudaMemsetAsync(w.counters, 0, 4 * C_COUNT, st));
+        kt.begin(K_INIT);
+        k_init<<<1184, 256, 0, st>>>(w);
+        k_roots<<<d_inst ? 148 : 1, 256, 0, st>>>(w, d_inst, ninst);
+        kt.end(K_INIT);
+        c->kstat[K_INIT].launches += 2;
+        c->kstat[K_INIT].strings += n;
+        c->kstat[K_INIT].alg_bytes += 12ull * n;  // offset read + id write
+        stats.kernel_launches += 2;
+    }
     uint32_t* hc = c->host_counters;
     PSS_CUDA(cudaMemcpyAsync(hc, w.counters, 4 * C_COUNT, cudaMemcpyDeviceToHost, st));
     PSS_CUDA(cudaStreamSynchronize(st));
     kt.collect();
     uint32_t cnt[L_NCLASS], nstr[L_NCLASS];
     for (int k = 0; k < L_NCLASS; ++k) {
-        cnt[k] = hc[k];
-        nstr[k] = k == L_BIG ? 0u : hc[C_NSTR + k];
+        cnt[k] = hc[C_PAR * cur + k];
+        nstr[k] = k == L_BIG ? 0u : hc[C_PAR * cur + C_NSTR + k];
     }
-    uint32_t ntiles = hc[C_NTILES];
-    uint32_t nmulti = hc[C_MULTI];
-    uint32_t ndeep = hc[C_DEEP];
+    uint32_t ntiles = hc[C_PAR * cur + C_NTILES];
+    uint32_t nmulti = hc[C_MULTI + cur];
+    uint32_t ndeep = hc[C_DEEP + cur];
     uint64_t small_segments = 0;
     uint32_t err = hc[C_ERR];
-    int cur = 0;
     auto pending = [&]() {
         return cnt[L_BIG] || cnt[L_TINY] || cnt[L_SMALLA] || cnt[L_SMALLB] || ndeep;
     };
@@ -1117,6 +1176,11 @@ int pssgpu_ctx_set_option(pssgpu_ctx* ctx, int option, int64_t value)
     switch (option) {
     case PSSGPU_OPT_PROFILE: c->profile = value != 0; return PSSGPU_OK;
     case PSSGPU_OPT_INDIRECT_HANDLES: c->indirect_handles = value != 0; return PSSGPU_OK;
+    case PSSGPU_OPT_SINGLE_LAUNCH: c->single_launch = value != 0; return PSSGPU_OK;
+    case PSSGPU_OPT_WAIT_LIMIT:
+        if (value < 1 || value > 0xFFFFFFFFll) return fail(PSSGPU_EINVAL, "wait limit out of range");
+        c->wait_limit = (uint32_t)value;
+        return PSSGPU_OK;
     default: return fail(PSSGPU_EINVAL, "unknown option");
     }
 }
@@ -1333,10 +1397,7 @@ int pssgpu_sort_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nchars,
     std::lock_guard<std::mutex> lk(c->mu);
     PSS_CUDA(cudaSetDevice(c->device));
     cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
-    uint8_t last = 1;
-    PSS_CUDA(cudaMemcpyAsync(&last, d_chars + nchars - 1, 1, cudaMemcpyDeviceToHost, st));
-    PSS_CUDA(cudaStreamSynchronize(st));
-    if (last != 0) return fail(PSSGPU_EINVAL, "arena does not end with NUL");
+    // the arena's last char is checked on the device by the first kernel
     return run_sort(c, d_chars, nchars, d_offs, (uint32_t)n, d_perm, d_lcp, st);
 }
 

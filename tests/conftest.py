@@ -34,3 +34,13 @@ def ctx(pkg):
     c = pkg.Context(0)
     yield c
     c.close()
+
+
+@pytest.fixture(scope="session", params=["single_launch", "pass_loop"])
+def ctx_any(pkg, request):
+    """A context on each sort path: inputs that fit one wave of resident
+    blocks in one cooperative launch, and the multi-launch pass loop."""
+    c = pkg.Context(0)
+    c.set_option(c.OPT_SINGLE_LAUNCH, 1 if request.param == "single_launch" else 0)
+    yield c
+    c.close()

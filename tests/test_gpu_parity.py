@@ -24,10 +24,10 @@ def check_against_oracle(orc, chars, offs, perm, lcp):
 
 
 @pytest.mark.parametrize("path", GOLDEN, ids=[p.stem for p in GOLDEN])
-def test_golden(ctx, path):
+def test_golden(ctx_any, path):
     z = np.load(path)
     chars, offs, gids, glcp = z["chars"], z["offs"], z["ids"], z["lcp"]
-    perm, lcp = ctx.sort_host(chars, offs, lcp=True)
+    perm, lcp = ctx_any.sort_host(chars, offs, lcp=True)
     assert np.array_equal(canonical_ids(chars, offs, perm, lcp), gids)
     assert np.array_equal(lcp[1:].astype(np.uint64), glcp[1:])
 
@@ -43,9 +43,9 @@ def test_golden(ctx, path):
     (300000, 1, 64, bytes(range(32, 127)), 8),
     (1000000, 0, 20, b"ACGT", 9),
 ])
-def test_random_vs_oracle(pkg, orc, ctx, n, lmin, lmax, alpha, seed):
+def test_random_vs_oracle(pkg, orc, ctx_any, n, lmin, lmax, alpha, seed):
     chars, offs, _ = pkg.workloads.random_strings(n, lmin, lmax, alpha, seed)
-    perm, lcp = ctx.sort_host(chars, offs, lcp=True)
+    perm, lcp = ctx_any.sort_host(chars, offs, lcp=True)
     check_against_oracle(orc, chars, offs, perm, lcp)
 
 
@@ -62,13 +62,13 @@ def test_random_vs_oracle(pkg, orc, ctx, n, lmin, lmax, alpha, seed):
     [bytes([97 + i % 3]) * (1 + i % 17) for i in range(4000)],
 ], ids=["empty", "one", "two", "all_empty", "all_equal", "ff_bytes", "prefix_chain",
         "deep_shared_prefix", "split_class_tied", "split_class_runs"])
-def test_edge_cases(pkg, orc, ctx, strings):
+def test_edge_cases(pkg, orc, ctx_any, strings):
     chars, offs = pkg.pack_strings(strings)
     if len(strings) == 0:
-        perm, lcp = ctx.sort_host(np.zeros(1, np.uint8), np.zeros(0, np.uint64), lcp=True)
+        perm, lcp = ctx_any.sort_host(np.zeros(1, np.uint8), np.zeros(0, np.uint64), lcp=True)
         assert perm.shape == (0,)
         return
-    perm, lcp = ctx.sort_host(chars, offs, lcp=True)
+    perm, lcp = ctx_any.sort_host(chars, offs, lcp=True)
     check_against_oracle(orc, chars, offs, perm, lcp)
 
 
@@ -80,7 +80,7 @@ def _rand_tails(n, k, seed):
 @pytest.mark.parametrize("case", ["all_equal_big", "long_prefix_big", "few_differ_early",
                                   "one_differs_first_char", "prefix_outliers",
                                   "outliers_past_one_jump", "many_deep_pairs"])
-def test_common_prefix_jump(pkg, orc, ctx, case):
+def test_common_prefix_jump(pkg, orc, ctx_any, case):
     """Big segments whose samples all share a prefix jump over it inside the
     pass: all strings equal, a long shared prefix (several jumps of at most
     256 chars), a few strings leaving the prefix early, one string differing
@@ -113,7 +113,7 @@ def test_common_prefix_jump(pkg, orc, ctx, case):
     else:
         strings = [b"s" * 40] * 20000 + [b"a"]
     chars, offs = pkg.pack_strings(strings)
-    perm, lcp = ctx.sort_host(chars, offs, lcp=True)
+    perm, lcp = ctx_any.sort_host(chars, offs, lcp=True)
     check_against_oracle(orc, chars, offs, perm, lcp)
 
 
@@ -146,7 +146,7 @@ def _group_strings(case):
 
 @pytest.mark.parametrize("case", ["groups_outliers", "many_groups", "groups_behind_jump",
                                   "groups_indirect", "groups_offsets_shuffled"])
-def test_group_jumps(pkg, orc, ctx, case):
+def test_group_jumps(pkg, orc, ctx_any, case):
     """'=' buckets whose samples share more chunks behind the splitter take a
     jump of their own: members that leave the group's chunks below or above
     (at every position, ending early or with other chars) and members that
@@ -166,16 +166,16 @@ def test_group_jumps(pkg, orc, ctx, case):
         finally:
             c.close()
     else:
-        perm, lcp = ctx.sort_host(chars, offs, lcp=True)
+        perm, lcp = ctx_any.sort_host(chars, offs, lcp=True)
     check_against_oracle(orc, chars, offs, perm, lcp)
 
 
-def test_deep_repeats_suffixes(pkg, orc, ctx):
+def test_deep_repeats_suffixes(pkg, orc, ctx_any):
     # a periodic text: suffix LCPs up to the text length
     text = (b"abcab" * 4000)[:19999] + b"\0"
     chars = np.frombuffer(text, dtype=np.uint8).copy()
     offs = np.arange(len(text), dtype=np.uint64)
-    perm, lcp = ctx.sort_host(chars, offs, lcp=True)
+    perm, lcp = ctx_any.sort_host(chars, offs, lcp=True)
     check_against_oracle(orc, chars, offs, perm, lcp)
 
 
@@ -191,6 +191,65 @@ def test_indirect_handles(pkg, orc, n, alpha, lmax, seed):
         check_against_oracle(orc, chars, offs, perm, lcp)
     finally:
         c.close()
+
+
+@pytest.mark.parametrize("case", ["tied_long_keys", "half_shared_prefix", "big_equal_bucket"])
+def test_single_launch_hands_big_buckets_to_the_passes(pkg, orc, ctx, case):
+    """Buckets of the single-launch sort over 2048 strings that are not all
+    equal continue in the pass loop (a second pass must run); all-equal ones
+    are copied out inside the launch."""
+    rng = np.random.default_rng(47)
+    lower = np.frombuffer(b"abcdefghijklmnopqrstuvwxyz", np.uint8)
+    if case == "tied_long_keys":
+        heads = [bytes(rng.choice(lower, 8)) for _ in range(20)]
+        strings = [heads[i % 20] + bytes(rng.choice(lower[:4], int(rng.integers(1, 12))))
+                   for i in range(100000)]
+    elif case == "half_shared_prefix":
+        pre = bytes(rng.choice(lower, 100))
+        strings = [pre + bytes(rng.choice(lower, int(rng.integers(0, 6)))) for _ in range(150000)]
+        strings += [bytes(rng.choice(lower, int(rng.integers(1, 30)))) for _ in range(150000)]
+    else:
+        strings = [b"x"] * 30000 + [bytes(rng.choice(lower, int(rng.integers(1, 9))))
+                                    for _ in range(30000)]
+    strings = [strings[i] for i in rng.permutation(len(strings))]
+    chars, offs = pkg.pack_strings(strings)
+    perm, lcp = ctx.sort_host(chars, offs, lcp=True)
+    check_against_oracle(orc, chars, offs, perm, lcp)
+    if case != "big_equal_bucket":
+        assert ctx.stats()["passes"] >= 2
+
+
+def test_single_launch_wait_limit(pkg, orc):
+    """A grid-barrier wait of the single-launch sort that runs out of polls
+    ends the sort with PSSGPU_ETIMEOUT (no hang), and the context sorts
+    normally once the limit is raised again."""
+    chars, offs, _ = pkg.workloads.random_strings(300000, 0, 20, b"abcd", 48)
+    c = pkg.Context(0)
+    try:
+        c.set_option(c.OPT_WAIT_LIMIT, 1)
+        with pytest.raises(pkg.SortError) as e:
+            c.sort_host(chars, offs, lcp=False)
+        assert e.value.status == 4  # PSSGPU_ETIMEOUT
+        c.set_option(c.OPT_WAIT_LIMIT, 1 << 22)
+        perm, lcp = c.sort_host(chars, offs, lcp=True)
+        check_against_oracle(orc, chars, offs, perm, lcp)
+    finally:
+        c.close()
+
+
+def test_unterminated_device_arena(pkg, ctx_any):
+    """The device entry checks the arena's last char on the device: an
+    arena that does not end with NUL is PSSGPU_EINVAL on both paths."""
+    import torch
+    chars, offs, nchars = pkg.workloads.random_strings(5000, 1, 9, b"ab", 49)
+    chars = chars.copy()
+    chars[nchars - 1] = 97
+    dc = torch.from_numpy(chars).cuda()
+    do = torch.from_numpy(offs.view(np.int64)).cuda()
+    dp = torch.empty(len(offs), dtype=torch.int32, device="cuda")
+    with pytest.raises(pkg.SortError) as e:
+        ctx_any.sort_device(dc, nchars, do, dp)
+    assert e.value.status == 1 and "NUL" in str(e.value)
 
 
 def test_lcp_optional(pkg, ctx):

@@ -168,7 +168,11 @@ int pssgpu_sort_text_host(pssgpu_ctx* ctx, const uint8_t* text, uint64_t size,
  * merged ids (equal strings keep the order of their runs), d_lcp_out (may be
  * NULL; then d_lcp may be NULL too) its LCP array with d_lcp_out[0] left
  * unchanged. Outputs must not overlap the inputs. All device buffers are on
- * the context's device; the arena rules of pssgpu_sort_device apply. */
+ * the context's device; the arena rules of pssgpu_sort_device apply. Every
+ * id in d_ids must index d_offs (the call cannot check that: it does not
+ * know the length of d_offs); an offset outside the arena returns
+ * PSSGPU_EINVAL, with d_ids_out / d_lcp_out unspecified. With d_lcp the
+ * merge is LCP-aware (compares start at the known common prefix). */
 int pssgpu_merge_lcp_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nchars,
                             const uint64_t* d_offs, const uint64_t* runs, uint32_t nruns,
                             const uint32_t* d_ids, const uint32_t* d_lcp,

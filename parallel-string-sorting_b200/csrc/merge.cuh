@@ -5,23 +5,25 @@
 // LCP-aware K-way merge of src/parallel/eberle-parallel-lcp-merge*.hpp over
 // src/sequential/bingmann-lcp_losertree.hpp).
 //
-// Here the runs merge pairwise, ceil(log2 K) rounds of three launches: the
-// merge-path split of every piece of MERGE_PIECE outputs, the sequential
-// merge of each piece by one thread (equal strings keep the left run
-// first), then every merged position takes its LCP from the input when its
-// predecessor was its predecessor in the same input run, else from
-// comparing the two strings.
+// Here the runs merge pairwise, ceil(log2 K) rounds of two launches: the
+// merge-path split of every piece of MERGE_PIECE outputs, then the merge of
+// each piece by one thread. With the runs' LCP arrays the piece merge is
+// LCP-aware, as the reference's loser tree is
+// (src/sequential/bingmann-lcp_losertree.hpp:61-110, 156-185): each head
+// carries its LCP with the last output, the head with the larger one is the
+// smaller string without reading a char, equal ones compare from that depth
+// only, and every output's LCP falls out of the same step.
 #pragma once
 
 #include "device_common.cuh"
 
 namespace pssgpu {
 
-// Order and LCP of strings a and b (arena offsets oa, ob), 8 chars a step.
-__device__ __forceinline__ int compare_lcp(const uint8_t* chars, uint64_t nchars, uint64_t oa,
-                                           uint64_t ob, uint32_t* lcp)
+// Order and LCP of strings a and b (arena offsets oa, ob) that share at
+// least d chars, 8 chars a step from d.
+__device__ __forceinline__ int compare_from(const uint8_t* chars, uint64_t nchars, uint64_t oa,
+                                            uint64_t ob, uint32_t d, uint32_t* lcp)
 {
-    uint32_t d = 0;
     while (true) {
         const uint64_t ka = load_key(chars, nchars, oa + d), kb = load_key(chars, nchars, ob + d);
         if (ka != kb) {
@@ -36,16 +38,10 @@ __device__ __forceinline__ int compare_lcp(const uint8_t* chars, uint64_t nchars
     }
 }
 
-// run r of the K runs with boundaries runs[0..K] that holds position q: the
-// last r with runs[r] <= q (runs[K] > q)
-__device__ __forceinline__ uint32_t run_of(const uint64_t* runs, uint32_t K, uint64_t q)
+__device__ __forceinline__ int compare_lcp(const uint8_t* chars, uint64_t nchars, uint64_t oa,
+                                           uint64_t ob, uint32_t* lcp)
 {
-    uint32_t lo = 0, hi = K;  // runs[lo] <= q < runs[hi]
-    while (hi - lo > 1) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (runs[mid] <= q) lo = mid; else hi = mid;
-    }
-    return lo;
+    return compare_from(chars, nchars, oa, ob, 0, lcp);
 }
 
 // Merge-path form of a round. A pair is (a0, a1, b1): left run [a0, a1),
@@ -53,7 +49,8 @@ __device__ __forceinline__ uint32_t run_of(const uint64_t* runs, uint32_t K, uin
 // Its output is cut into pieces of MERGE_PIECE positions; task t of the
 // round is piece t - first[pair] of its pair. k_merge_split finds for every
 // piece how many left-run strings precede it (a binary search along the
-// piece's diagonal), k_merge_seq merges each piece sequentially from there.
+// piece's diagonal), k_merge_lcp_seq (or k_merge_seq without LCP arrays)
+// merges each piece sequentially from there.
 constexpr uint32_t MERGE_PIECE = 32;
 
 struct MergePair {
@@ -96,11 +93,12 @@ __global__ void k_merge_split(const uint8_t* __restrict__ chars, uint64_t nchars
     }
 }
 
+// Piece merge without LCP arrays: every pair compares from char 0.
 __global__ void k_merge_seq(const uint8_t* __restrict__ chars, uint64_t nchars,
                             const uint64_t* __restrict__ offs, const MergePair* __restrict__ pairs,
                             const uint64_t* __restrict__ first, uint32_t npair,
                             const uint64_t* __restrict__ split, const uint32_t* __restrict__ ids_in,
-                            uint32_t* __restrict__ ids_out, uint32_t* __restrict__ src)
+                            uint32_t* __restrict__ ids_out)
 {
     const uint64_t ntask = first[npair];
     for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ntask;
@@ -123,35 +121,101 @@ __global__ void k_merge_seq(const uint8_t* __restrict__ chars, uint64_t nchars,
                 take_a = compare_lcp(chars, nchars, __ldg(offs + ids_in[pr.a0 + i]),
                                      __ldg(offs + ids_in[pr.a1 + j]), &l) <= 0;
             }
-            const uint64_t q = take_a ? pr.a0 + i : pr.a1 + j;
-            ids_out[pr.a0 + d] = ids_in[q];
-            src[pr.a0 + d] = (uint32_t)q;
+            ids_out[pr.a0 + d] = take_a ? ids_in[pr.a0 + i] : ids_in[pr.a1 + j];
             if (take_a) ++i; else ++j;
         }
     }
 }
 
-// LCPs of a round's output: runs_out are the merged runs (no LCP at their
-// first position), runs_in the runs merged.
-__global__ void k_merge_lcp(const uint8_t* __restrict__ chars, uint64_t nchars,
-                            const uint64_t* __restrict__ offs, const uint64_t* __restrict__ runs_in,
-                            uint32_t K_in, const uint64_t* __restrict__ runs_out, uint32_t K_out,
-                            const uint32_t* __restrict__ ids_out, const uint32_t* __restrict__ src,
-                            const uint32_t* __restrict__ lcp_in, uint32_t* __restrict__ lcp_out,
-                            uint64_t n)
+// LCP-aware piece merge (the reference's LCP loser-tree rule for two runs).
+// Runs A = ids_in[a0, a1) and B = ids_in[a1, b1) with their LCP arrays in
+// lcp_in (entries at a run's first position are not read). ha / hb are the
+// LCPs of the heads A[i] / B[j] with the last output. A piece that does not
+// start the pair first finds its previous output (the larger of A[i0 - 1]
+// and B[j0 - 1]; equal strings: B's, as A's comes first) and the heads' LCPs
+// with it. lcp_out (may be null) receives the LCP of every output but the
+// pair's first.
+__global__ void k_merge_lcp_seq(const uint8_t* __restrict__ chars, uint64_t nchars,
+                                const uint64_t* __restrict__ offs,
+                                const MergePair* __restrict__ pairs,
+                                const uint64_t* __restrict__ first, uint32_t npair,
+                                const uint64_t* __restrict__ split,
+                                const uint32_t* __restrict__ ids_in,
+                                const uint32_t* __restrict__ lcp_in,
+                                uint32_t* __restrict__ ids_out, uint32_t* __restrict__ lcp_out)
 {
-    for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
-         p += (uint64_t)gridDim.x * blockDim.x) {
-        if (runs_out[run_of(runs_out, K_out, p)] == p) continue;  // first of a merged run
-        const uint32_t s0 = src[p - 1], s1 = src[p];
-        if (s1 == s0 + 1 && runs_in[run_of(runs_in, K_in, s1)] != s1) {
-            lcp_out[p] = lcp_in[s1];  // neighbours in the same input run
-        } else {
-            uint32_t l;
-            compare_lcp(chars, nchars, __ldg(offs + ids_out[p - 1]), __ldg(offs + ids_out[p]), &l);
-            lcp_out[p] = l;
+    const uint64_t ntask = first[npair];
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ntask;
+         t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t p = pair_of(first, npair, t);
+        const MergePair pr = pairs[p];
+        const uint64_t na = pr.a1 - pr.a0, nb = pr.b1 - pr.a1;
+        const uint32_t* A = ids_in + pr.a0;
+        const uint32_t* B = ids_in + pr.a1;
+        const uint32_t* LA = lcp_in + pr.a0;
+        const uint32_t* LB = lcp_in + pr.a1;
+        const uint64_t d0 = (t - first[p]) * MERGE_PIECE;
+        const uint64_t d1 = min(d0 + MERGE_PIECE, na + nb);
+        const uint64_t i0 = split[t];
+        const uint64_t i1 = t + 1 < first[p + 1] ? split[t + 1] : na;
+        const uint64_t j0 = d0 - i0, j1 = d1 - i1;
+        uint64_t i = i0, j = j0;
+        uint32_t ha = 0, hb = 0;
+        if (d0 > 0) {
+            if (i0 == 0) {  // previous output B[j0 - 1]
+                hb = j < nb ? LB[j] : 0u;
+                if (i < na) compare_from(chars, nchars, __ldg(offs + A[i]), __ldg(offs + B[j - 1]), 0, &ha);
+            } else if (j0 == 0) {  // previous output A[i0 - 1]
+                ha = i < na ? LA[i] : 0u;
+                if (j < nb) compare_from(chars, nchars, __ldg(offs + B[j]), __ldg(offs + A[i - 1]), 0, &hb);
+            } else {
+                uint32_t l;
+                const int c = compare_from(chars, nchars, __ldg(offs + A[i - 1]),
+                                           __ldg(offs + B[j - 1]), 0, &l);
+                // LCP(x, z) >= min(LCP(x, y), LCP(y, z)): start from that depth
+                if (c <= 0) {  // previous output B[j0 - 1]
+                    hb = j < nb ? LB[j] : 0u;
+                    if (i < na)
+                        compare_from(chars, nchars, __ldg(offs + A[i]), __ldg(offs + B[j - 1]),
+                                     min(LA[i], l), &ha);
+                } else {       // previous output A[i0 - 1]
+                    ha = i < na ? LA[i] : 0u;
+                    if (j < nb)
+                        compare_from(chars, nchars, __ldg(offs + B[j]), __ldg(offs + A[i - 1]),
+                                     min(LB[j], l), &hb);
+                }
+            }
+        }
+        for (uint64_t d = d0; d < d1; ++d) {
+            bool take_a;
+            if (i >= i1) take_a = false;
+            else if (j >= j1) take_a = true;
+            else if (ha != hb) take_a = ha > hb;
+            else {
+                uint32_t l;
+                take_a = compare_from(chars, nchars, __ldg(offs + A[i]), __ldg(offs + B[j]), ha, &l) <= 0;
+                if (take_a) hb = l; else ha = l;  // the loser's LCP with the new last output
+            }
+            ids_out[pr.a0 + d] = take_a ? A[i] : B[j];
+            if (lcp_out && d > 0) lcp_out[pr.a0 + d] = take_a ? ha : hb;
+            if (take_a) {
+                ++i;
+                ha = i < na ? LA[i] : 0u;  // against its predecessor, the last output
+            } else {
+                ++j;
+                hb = j < nb ? LB[j] : 0u;
+            }
         }
     }
+}
+
+// Every id's offset must lie inside the arena (offsets >= nchars: *err).
+__global__ void k_merge_check(const uint64_t* __restrict__ offs, uint64_t nchars,
+                              const uint32_t* __restrict__ ids, uint64_t n, uint32_t* err)
+{
+    for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n;
+         q += (uint64_t)gridDim.x * blockDim.x)
+        if (__ldg(offs + ids[q]) >= nchars) atomicOr(err, ERR_OFFSET);
 }
 
 }  // namespace pssgpu

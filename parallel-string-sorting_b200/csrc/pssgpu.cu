@@ -1307,8 +1307,8 @@ int pssgpu_merge_lcp_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nc
         PSS_CUDA(cudaStreamSynchronize(st));
         return PSSGPU_OK;
     }
-    // boundaries, pairs and piece counts of every round, uploaded at once:
-    // round i merges the runs of level i into those of level i + 1
+    // pairs and piece counts of every round, uploaded at once: round i
+    // merges the runs of level i into those of level i + 1
     std::vector<std::vector<uint64_t>> level{std::vector<uint64_t>(runs, runs + nruns + 1)};
     while (level.back().size() > 2) {
         const std::vector<uint64_t>& a = level.back();
@@ -1319,13 +1319,9 @@ int pssgpu_merge_lcp_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nc
         level.push_back(std::move(b));
     }
     const size_t rounds = level.size() - 1;
-    std::vector<uint64_t> flat;  // per level: boundaries; per round: pairs, piece starts
-    std::vector<uint64_t> at_runs, at_pairs, at_first, npairs;
+    std::vector<uint64_t> flat;  // per round: pairs, piece starts
+    std::vector<uint64_t> at_pairs, at_first, npairs;
     uint64_t max_tasks = 0;
-    for (size_t i = 0; i <= rounds; ++i) {
-        at_runs.push_back(flat.size());
-        flat.insert(flat.end(), level[i].begin(), level[i].end());
-    }
     for (size_t i = 0; i < rounds; ++i) {
         const std::vector<uint64_t>& a = level[i];
         const uint32_t K = (uint32_t)a.size() - 1, np = (K + 1) / 2;
@@ -1350,36 +1346,43 @@ int pssgpu_merge_lcp_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nc
     }
     const uint64_t b_v = align256(4 * n), b_runs = align256(8 * flat.size());
     const uint64_t b_split = align256(8 * (max_tasks + 1));
-    if ((rc = ensure_buf(&c->mbuf, &c->mbuf_bytes, 5 * b_v + b_runs + b_split))) return rc;
+    if ((rc = ensure_buf(&c->mbuf, &c->mbuf_bytes, 4 * b_v + b_runs + b_split + 256))) return rc;
     uint32_t* tid[2] = {(uint32_t*)c->mbuf, (uint32_t*)(c->mbuf + b_v)};
     uint32_t* tlcp[2] = {(uint32_t*)(c->mbuf + 2 * b_v), (uint32_t*)(c->mbuf + 3 * b_v)};
-    uint32_t* src = (uint32_t*)(c->mbuf + 4 * b_v);
-    uint64_t* d_flat = (uint64_t*)(c->mbuf + 5 * b_v);
-    uint64_t* split = (uint64_t*)(c->mbuf + 5 * b_v + b_runs);
+    uint64_t* d_flat = (uint64_t*)(c->mbuf + 4 * b_v);
+    uint64_t* split = (uint64_t*)(c->mbuf + 4 * b_v + b_runs);
+    uint32_t* d_err = (uint32_t*)(c->mbuf + 4 * b_v + b_runs + b_split);
     PSS_CUDA(cudaMemcpyAsync(d_flat, flat.data(), 8 * flat.size(), cudaMemcpyHostToDevice, st));
+    PSS_CUDA(cudaMemsetAsync(d_err, 0, 4, st));
     const unsigned blocks = (unsigned)std::min<uint64_t>((n + 255) / 256, 148ull * 16);
+    k_merge_check<<<blocks, 256, 0, st>>>(d_offs, nchars, d_ids, n, d_err);
+    // with the runs' LCP arrays every round is LCP-aware and carries the
+    // merged LCP array to the next one (the last round writes d_lcp_out, if any)
+    const bool with_lcp = d_lcp != nullptr;
     const uint32_t* in_ids = d_ids;
     const uint32_t* in_lcp = d_lcp;
     for (size_t i = 0; i < rounds; ++i) {
         const bool lastr = i + 1 == rounds;
         uint32_t* out_ids = lastr ? d_ids_out : tid[i & 1];
         uint32_t* out_lcp = lastr ? d_lcp_out : tlcp[i & 1];
-        const uint32_t K_in = (uint32_t)level[i].size() - 1, K_out = (uint32_t)level[i + 1].size() - 1;
         const MergePair* pairs = reinterpret_cast<const MergePair*>(d_flat + at_pairs[i]);
         const uint64_t* first = d_flat + at_first[i];
         const uint32_t np = (uint32_t)npairs[i];
         k_merge_split<<<blocks, 256, 0, st>>>(d_chars, nchars, d_offs, pairs, first, np, in_ids, split);
-        k_merge_seq<<<blocks, 256, 0, st>>>(d_chars, nchars, d_offs, pairs, first, np, split, in_ids,
-                                            out_ids, src);
-        if (d_lcp_out)
-            k_merge_lcp<<<blocks, 256, 0, st>>>(d_chars, nchars, d_offs, d_flat + at_runs[i], K_in,
-                                                d_flat + at_runs[i + 1], K_out, out_ids, src, in_lcp,
-                                                out_lcp, n);
+        if (with_lcp)
+            k_merge_lcp_seq<<<blocks, 256, 0, st>>>(d_chars, nchars, d_offs, pairs, first, np, split,
+                                                    in_ids, in_lcp, out_ids, out_lcp);
+        else
+            k_merge_seq<<<blocks, 256, 0, st>>>(d_chars, nchars, d_offs, pairs, first, np, split,
+                                                in_ids, out_ids);
         PSS_CUDA(cudaGetLastError());
         in_ids = out_ids;
         in_lcp = out_lcp;
     }
+    uint32_t err = 0;
+    PSS_CUDA(cudaMemcpyAsync(&err, d_err, 4, cudaMemcpyDeviceToHost, st));
     PSS_CUDA(cudaStreamSynchronize(st));
+    if (err) return fail(PSSGPU_EINVAL, "a string offset lies outside the arena");
     return PSSGPU_OK;
 }
 

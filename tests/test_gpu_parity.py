@@ -400,12 +400,14 @@ def _merge_strings(case):
 
 
 @pytest.mark.parametrize("K,case", [(1, "rand"), (2, "rand"), (3, "rand"), (8, "rand"), (33, "rand"),
-                                    (5, "empty_run"), (4, "deep"), (2, "no_lcp")])
+                                    (5, "empty_run"), (4, "deep"), (7, "deep"), (2, "no_lcp"),
+                                    (6, "no_lcp_input")])
 def test_merge_lcp(pkg, orc, ctx, K, case):
     """Sorted runs with their LCP arrays merge into the sorted sequence and
     LCP array of all strings: pairs, odd run counts, many runs, an empty run,
-    runs sharing 250-300 char prefixes with duplicates and empty strings, and
-    the merge without LCP output."""
+    runs sharing 250-300 char prefixes with duplicates and empty strings, the
+    merge without LCP output, and without the runs' LCP arrays (compares from
+    char 0)."""
     import torch
     chars, offs = pkg.pack_strings(_merge_strings("deep" if case == "deep" else "rand"))
     nchars = chars.shape[0]
@@ -413,9 +415,9 @@ def test_merge_lcp(pkg, orc, ctx, K, case):
     dc = torch.from_numpy(np.concatenate([chars, np.zeros(16, np.uint8)])).cuda()
     do = torch.from_numpy(offs.view(np.int64)).cuda()
     di = torch.from_numpy(ids.view(np.int32)).cuda()
-    dl = torch.from_numpy(lcp.view(np.int32)).cuda()
+    dl = torch.from_numpy(lcp.view(np.int32)).cuda() if case != "no_lcp_input" else None
     dio = torch.empty_like(di)
-    dlo = torch.zeros_like(dl) if case != "no_lcp" else None
+    dlo = torch.zeros_like(di) if case not in ("no_lcp", "no_lcp_input") else None
     ctx.merge_lcp_device(dc, nchars, do, runs, di, dl, dio, dlo)
     perm = dio.cpu().numpy().view(np.uint32)
     if dlo is None:
@@ -423,6 +425,22 @@ def test_merge_lcp(pkg, orc, ctx, K, case):
         assert orc.check_order(chars, offs, perm) == -1
     else:
         check_against_oracle(orc, chars, offs, perm, dlo.cpu().numpy().view(np.uint32))
+
+
+def test_merge_rejects_offsets_outside_the_arena(pkg, orc, ctx):
+    import torch
+    chars, offs = pkg.pack_strings([b"b", b"a", b"c", b"a"])
+    nchars = chars.shape[0]
+    offs = offs.copy()
+    offs[2] = nchars + 5
+    dc = torch.from_numpy(np.concatenate([chars, np.zeros(16, np.uint8)])).cuda()
+    do = torch.from_numpy(offs.view(np.int64)).cuda()
+    di = torch.tensor([1, 0, 3, 2], dtype=torch.int32, device="cuda")
+    dl = torch.zeros(4, dtype=torch.int32, device="cuda")
+    with pytest.raises(pkg.SortError) as e:
+        ctx.merge_lcp_device(dc, nchars, do, np.array([0, 2, 4], np.uint64), di, dl,
+                             torch.empty_like(di), torch.zeros_like(dl))
+    assert e.value.status == 1
 
 
 def test_sharded_sort_then_merge(pkg, orc, ctx):

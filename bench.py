@@ -78,6 +78,8 @@ def parse():
                         "through the server; autotune: write the tuning table; merge: "
                         "the device merge of sorted shards (--shards of --n prefixes)")
     p.add_argument("--shards", type=int, default=8, help="merge mode: sorted runs to merge")
+    p.add_argument("--merge-piece", type=int, default=0,
+                   help="merge mode: outputs per thread of a merge round (0: library default)")
     p.add_argument("--duration", type=float, default=60.0, help="serving: seconds of arrivals")
     p.add_argument("--rate", type=float, default=2000.0, help="serving: requests per second")
     p.add_argument("--budget-gb", type=float, default=40.0, help="serving: HBM budget")
@@ -333,6 +335,8 @@ def run_merge(args):
     out = torch.empty_like(ids)
     out_lcp = torch.zeros_like(lcp)
     stream = torch.cuda.current_stream()
+    if args.merge_piece:
+        ctx.set_option(ctx.OPT_MERGE_PIECE, args.merge_piece)
 
     def step():
         ctx.merge_lcp_device(dc, nchars, do, bounds, ids, lcp, out, out_lcp, stream=stream)
@@ -351,7 +355,8 @@ def run_merge(args):
         "unit": "GB/s", "ms_per_step": ms, "steps": args.steps, "warmup": max(args.warmup, 3),
         "higher_is_better": True, "dtype": "u8", "data": "synthetic",
         "config": {"workload": f"prefixes-{n}", "strings": n, "chars": nchars,
-                   "shards": args.shards, "lcp_output": True},
+                   "shards": args.shards, "lcp_output": True,
+                   "merge_piece": args.merge_piece or "default"},
         "strings_per_s": n / (ms / 1e3)}))
     ctx.close()
 

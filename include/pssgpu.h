@@ -97,11 +97,20 @@ int pssgpu_ctx_kernel_stats(pssgpu_ctx* ctx, pssgpu_kernel_stats* out, int max);
  * cooperative kernel launch, with no host round trip between its steps;
  * 0 sends every sort through the multi-launch pass loop.
  * PSSGPU_OPT_WAIT_LIMIT (default 4,194,304): polls of a grid-barrier wait in
- * that kernel before it gives up and the sort returns PSSGPU_ETIMEOUT. */
+ * that kernel before it gives up and the sort returns PSSGPU_ETIMEOUT.
+ * PSSGPU_OPT_MERGE_PIECE (default 32, at most 4096): outputs one GPU thread
+ * merges in each round of pssgpu_merge_lcp_device.
+ * PSSGPU_OPT_SUFFIX_DOUBLING (default 1): when the strings of a sort are all
+ * suffixes of one text (n == nchars, offs[i] == i, no NUL before the last
+ * char: psstest --suffix, src/psstest.cpp:502-518), groups that share 8 or
+ * more chars are finished by prefix doubling on suffix ranks instead of
+ * deeper string passes; the output is the same. 0: sort them as strings. */
 #define PSSGPU_OPT_PROFILE 1
 #define PSSGPU_OPT_INDIRECT_HANDLES 2
 #define PSSGPU_OPT_SINGLE_LAUNCH 3
 #define PSSGPU_OPT_WAIT_LIMIT 4
+#define PSSGPU_OPT_MERGE_PIECE 5
+#define PSSGPU_OPT_SUFFIX_DOUBLING 6
 int pssgpu_ctx_set_option(pssgpu_ctx* ctx, int option, int64_t value);
 
 /* ---- arena sorts ---------------------------------------------------------

@@ -81,6 +81,8 @@ class Context:
     OPT_INDIRECT_HANDLES = 2
     OPT_SINGLE_LAUNCH = 3
     OPT_WAIT_LIMIT = 4
+    OPT_MERGE_PIECE = 5
+    OPT_SUFFIX_DOUBLING = 6
 
     def set_option(self, option: int, value: int) -> None:
         _check(_native.gpu().pssgpu_ctx_set_option(self._h, option, value))

@@ -22,7 +22,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CUDA_SOURCES = ["pssgpu.cu"]
 CUDA_DEPS = ["device_common.cuh", "work.cuh", "block_util.cuh", "kernels_big.cuh",
-             "kernels_small.cuh", "kernels_block.cuh", "kernels_wave.cuh", "server.cuh", "prepare.cuh",
+             "kernels_small.cuh", "kernels_block.cuh", "kernels_wave.cuh", "kernels_suffix.cuh",
+             "server.cuh", "prepare.cuh",
              "merge.cuh",
              "pssgpu.cu"]
 

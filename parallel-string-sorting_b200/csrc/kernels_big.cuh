@@ -646,6 +646,13 @@ __global__ void __launch_bounds__(1024) k_children(Work w)
                         } else {
                             child = Seg{P, c, v, (uint32_t)nbuf | META_FINAL};
                         }
+                    } else if (w.suffix && c <= DBL_MAX) {
+                        // a suffix set: the group is sorted by rank doubling
+                        // after the passes
+                        const uint32_t at = atomicAdd(w.counters + C_DBL, 1u);
+                        if (at < w.dbl_cap) w.dbl[at] = Seg{P, c, dj + 8, (uint32_t)nbuf};
+                        else set_error(w.counters + C_ERR, ERR_OVERFLOW);
+                        inline_done = true;
                     } else {
                         child = Seg{P, c, dj + 8, (uint32_t)nbuf};
                     }

@@ -1,0 +1,250 @@
+// kernels_suffix.cuh -- the suffix-sorting specialisation: prefix doubling
+// on ranks for inputs that are all suffixes of one text.
+//
+// The reference sorts suffixes as strings (UCharSuffixSet,
+// src/tools/stringset.hpp:732-804: string i is text + i up to the text's
+// end), so a group of suffixes sharing a long repeat is walked 8 chars per
+// step. Suffixes allow more: two suffixes x, y that share d chars compare as
+// the suffixes x + d and y + d do. So once the string sort has placed every
+// suffix either at its final position or in an unsorted group whose members
+// share d chars (the group's depth), each group sorts by the rank of suffix
+// x + d -- a final position, or the start of that suffix's own group. Ties
+// form subgroups whose depth is d plus the depth of the tied group, so the
+// depth at least doubles per round (prefix doubling on the ranks the string
+// passes produced): a group of 10 KB repeats needs about 11 rounds instead
+// of 1,280 chunk steps.
+//
+// Arrays (positions p, suffixes x, both in [0, n)): perm[p] = the suffix at p;
+// isa[x] = its rank (final position, or its group's start); gd[par][s] = depth
+// of the group starting at s (read from one parity, written to the other, so
+// a round reads a consistent snapshot); key[p] = the rank used this round;
+// lb[p] (LCP output only) = the depth at which positions p - 1 and p were
+// separated, a lower bound of their LCP, or ~0 when p did not lie inside a
+// doubled group.
+#pragma once
+
+#include "kernels_small.cuh"
+
+namespace pssgpu {
+
+constexpr uint32_t DBL_NONE = 0xFFFFFFFFu;  // lb: no doubling bound
+constexpr uint32_t DBL_MID = 512;           // largest group of the smaller block sort
+
+// Group lists of a round, by size class: 0 at most 32 members (one warp
+// each), 1 at most DBL_MID (a block of 256 threads), 2 at most DBL_MAX (a
+// block of 512 threads); double-buffered by round parity.
+struct DblArrays {
+    uint32_t* isa;
+    uint32_t* gd[2];
+    uint32_t* key;
+    uint32_t* lb;   // null without LCP output
+    Seg* list[3][2];
+    uint32_t cap[3];
+};
+
+__host__ __device__ constexpr int dbl_class(uint32_t size)
+{
+    return size <= (uint32_t)WARP_GROUP_MAX ? 0 : size <= DBL_MID ? 1 : 2;
+}
+
+// The input is a suffix set when offs[i] == i for all i and no NUL lies
+// before the last char (n == nchars is checked by the host): any other
+// input sets *flag.
+__global__ void k_suffix_check(const uint8_t* __restrict__ chars, const uint64_t* __restrict__ offs,
+                               uint64_t n, uint32_t* flag)
+{
+    bool bad = false;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        if (__ldg(offs + i) != i) bad = true;
+        if (i + 1 < n && __ldg(chars + i) == 0) bad = true;
+    }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1u);
+}
+
+// Members of the groups the string passes handed over: their ids into perm
+// (the handles sit in the group's ping-pong buffer).
+__global__ void k_dbl_init(Work w, const Seg* __restrict__ list, uint32_t count)
+{
+    for (uint32_t g = blockIdx.x; g < count; g += gridDim.x) {
+        const Seg s = list[g];
+        const uint64_t* hs = w.hnd[s.meta & META_BUF];
+        for (uint32_t q = threadIdx.x; q < s.size; q += blockDim.x)
+            w.perm[s.begin + q] = h_id(w, hs[s.begin + q]);
+    }
+}
+
+__global__ void k_dbl_isa(const uint32_t* __restrict__ perm, uint32_t n, uint32_t* __restrict__ isa)
+{
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
+        isa[perm[p]] = p;
+}
+
+__device__ __forceinline__ void dbl_push(DblArrays& a, uint32_t* counters, int par, Seg s)
+{
+    const int cls = dbl_class(s.size);
+    const uint32_t at = atomicAdd(counters + C_DBL_CNT + 3 * par + cls, 1u);
+    if (at < a.cap[cls]) a.list[cls][par][at] = s;
+    else set_error(counters + C_ERR, ERR_OVERFLOW);
+}
+
+// Handed-over groups: every member's rank is the group start, the group's
+// depth goes to gd[0]; the groups are sorted into the round lists of parity 0.
+__global__ void k_dbl_rank(const uint32_t* __restrict__ perm, const Seg* __restrict__ list,
+                           uint32_t count, DblArrays a, uint32_t* counters)
+{
+    for (uint32_t g = blockIdx.x; g < count; g += gridDim.x) {
+        const Seg s = list[g];
+        for (uint32_t q = threadIdx.x; q < s.size; q += blockDim.x) a.isa[perm[s.begin + q]] = s.begin;
+        if (threadIdx.x == 0) {
+            a.gd[0][s.begin] = s.depth;
+            dbl_push(a, counters, 0, Seg{s.begin, s.size, s.depth, 0u});
+        }
+    }
+}
+
+// Round step 1: every member's key, the rank of the suffix `depth` chars
+// further (members share depth chars, none of them NUL, so x + depth < n).
+// One warp per group.
+__global__ void k_dbl_keys(const Seg* __restrict__ list, uint32_t count,
+                           const uint32_t* __restrict__ perm, DblArrays a)
+{
+    const uint32_t g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (g >= count) return;
+    const Seg s = list[g];
+    for (uint32_t q = threadIdx.x & 31; q < s.size; q += 32)
+        a.key[s.begin + q] = a.isa[perm[s.begin + q] + s.depth];
+}
+
+// One sorted run [i0, i1) of equal keys K inside group s (positions
+// s.begin + i): a single member is final; more form a subgroup whose
+// members share s.depth + gd(K) chars.
+__device__ __forceinline__ void dbl_run(DblArrays& a, uint32_t* counters, int par, const Seg& s,
+                                        uint32_t i0, uint32_t len, uint32_t K)
+{
+    const uint32_t p = s.begin + i0;
+    if (a.lb && i0 > 0) a.lb[p] = s.depth;  // separated from p - 1 at this depth
+    if (len < 2) return;
+    const uint32_t nd = s.depth + a.gd[par][K];
+    a.gd[par ^ 1][p] = nd;
+    dbl_push(a, counters, par ^ 1, Seg{p, len, nd, 0u});
+}
+
+// Round step 2 for groups of at most 32 members, one warp each: sort by
+// (key, member), write perm and the new ranks, split into runs.
+__global__ void k_dbl_sort_small(const Seg* __restrict__ list, uint32_t count,
+                                 uint32_t* __restrict__ perm, DblArrays a, uint32_t* counters, int par)
+{
+    const uint32_t g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (g >= count) return;
+    const uint32_t lane = threadIdx.x & 31;
+    const Seg s = list[g];
+    const bool real = lane < s.size;
+    const uint32_t x = real ? perm[s.begin + lane] : 0u;
+    uint64_t t = real ? ((uint64_t)a.key[s.begin + lane] << 32) | lane : ~0ull;
+#pragma unroll
+    for (uint32_t kk = 2; kk <= 32; kk <<= 1) {
+#pragma unroll
+        for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
+            const uint64_t o = __shfl_xor_sync(0xffffffffu, t, j);
+            const bool lower = (lane & j) == 0, asc = (lane & kk) == 0;
+            if ((lower == asc) ? (o < t) : (o > t)) t = o;
+        }
+    }
+    const uint32_t K = (uint32_t)(t >> 32);
+    const uint32_t mx = __shfl_sync(0xffffffffu, x, (uint32_t)t & 31u);
+    const uint32_t pk = __shfl_up_sync(0xffffffffu, K, 1);
+    const bool start = real && (lane == 0 || pk != K);
+    const uint32_t S = __ballot_sync(0xffffffffu, start);
+    const uint32_t R = __ballot_sync(0xffffffffu, real);
+    // this lane's run: from the last start at or below it to the next start
+    const uint32_t rs = 31u - __clz(S & (0xFFFFFFFFu >> (31 - lane)));
+    const uint32_t above = lane == 31 ? 0u : (S & (0xFFFFFFFFu << (lane + 1)));
+    const uint32_t re = above ? (uint32_t)(__ffs(above) - 1) : (uint32_t)__popc(R);
+    if (real) {
+        const uint32_t p = s.begin + lane;
+        perm[p] = mx;
+        a.isa[mx] = s.begin + rs;  // final position for a single member
+        if (start) dbl_run(a, counters, par, s, lane, re - rs, K);
+    }
+}
+
+// Round step 2 for groups of 33..MAXM members, one block each: a bitonic
+// sort of (key << 32 | member index) in shared memory (dynamic: MAXM keys,
+// then MAXM member ids).
+template <uint32_t MAXM>
+__global__ void __launch_bounds__(MAXM <= DBL_MID ? 256 : 512) k_dbl_sort_block(
+    const Seg* __restrict__ list, uint32_t* __restrict__ perm, DblArrays a, uint32_t* counters,
+    int par)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint64_t* sk = reinterpret_cast<uint64_t*>(smem_raw);
+    uint32_t* sx = reinterpret_cast<uint32_t*>(smem_raw + 8 * MAXM);
+    const Seg s = list[blockIdx.x];
+    const uint32_t m = s.size;
+    uint32_t S = 64;
+    while (S < m) S <<= 1;
+    for (uint32_t q = threadIdx.x; q < S; q += blockDim.x) {
+        if (q < m) {
+            sx[q] = perm[s.begin + q];
+            sk[q] = ((uint64_t)a.key[s.begin + q] << 32) | q;
+        } else {
+            sk[q] = ~0ull;
+        }
+    }
+    __syncthreads();
+    bitonic_sort_block(sk, S);
+    for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
+        const uint32_t K = (uint32_t)(sk[i] >> 32);
+        const uint32_t x = sx[(uint32_t)sk[i] & (MAXM - 1)];
+        perm[s.begin + i] = x;
+        if (i > 0 && (uint32_t)(sk[i - 1] >> 32) == K) continue;
+        // a run starts here: its length, then every member's rank
+        uint32_t e = i + 1;
+        while (e < m && (uint32_t)(sk[e] >> 32) == K) ++e;
+        for (uint32_t q = i; q < e; ++q) a.isa[sx[(uint32_t)sk[q] & (MAXM - 1)]] = s.begin + i;
+        dbl_run(a, counters, par, s, i, e - i, K);
+    }
+}
+
+// LCPs at the positions the doubling separated (lb[p] set), in text order
+// so that the LCP of suffix x with its predecessor, minus one, bounds that of
+// suffix x + 1 (the Phi-array argument of Kasai et al.): one thread per
+// chunk of DBL_LCP_CHUNK suffixes, compares 8 chars a step from the bound.
+constexpr uint32_t DBL_LCP_CHUNK = 32;
+__global__ void k_dbl_lcp(const uint8_t* __restrict__ chars, uint64_t nchars,
+                          const uint32_t* __restrict__ perm, const uint32_t* __restrict__ isa,
+                          const uint32_t* __restrict__ lb, uint32_t* __restrict__ lcp, uint32_t n)
+{
+    const uint64_t nchunk = ((uint64_t)n + DBL_LCP_CHUNK - 1) / DBL_LCP_CHUNK;
+    for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nchunk;
+         c += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t x0 = (uint32_t)(c * DBL_LCP_CHUNK);
+        const uint32_t x1 = (uint32_t)min((uint64_t)x0 + DBL_LCP_CHUNK, (uint64_t)n);
+        uint32_t prev = 0;  // LCP of suffix x - 1 with its predecessor, when known
+        bool have = false;
+        for (uint32_t x = x0; x < x1; ++x) {
+            const uint32_t p = isa[x];
+            const uint32_t b = p ? lb[p] : DBL_NONE;
+            if (b == DBL_NONE) {
+                have = false;
+                continue;
+            }
+            const uint32_t y = perm[p - 1];
+            uint32_t d = max(b, have && prev ? prev - 1 : 0u);
+            uint64_t ka, kb;
+            while (true) {
+                ka = load_key(chars, nchars, (uint64_t)x + d);
+                kb = load_key(chars, nchars, (uint64_t)y + d);
+                if (ka != kb || key_terminated(ka)) break;
+                d += 8;
+            }
+            const uint32_t l = d + (ka != kb ? lcp_key_type(ka, kb) : lcp_key_depth(ka));
+            lcp[p] = l;
+            prev = l;
+            have = true;
+        }
+    }
+}
+
+}  // namespace pssgpu

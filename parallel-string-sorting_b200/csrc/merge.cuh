@@ -46,12 +46,13 @@ __device__ __forceinline__ int compare_lcp(const uint8_t* chars, uint64_t nchars
 
 // Merge-path form of a round. A pair is (a0, a1, b1): left run [a0, a1),
 // right run [a1, b1) (empty for an unpaired last run), merged into [a0, b1).
-// Its output is cut into pieces of MERGE_PIECE positions; task t of the
-// round is piece t - first[pair] of its pair. k_merge_split finds for every
+// Its output is cut into pieces of `piece` positions (MERGE_PIECE by
+// default); task t of the round is piece t - first[pair] of its pair. k_merge_split finds for every
 // piece how many left-run strings precede it (a binary search along the
 // piece's diagonal), k_merge_lcp_seq (or k_merge_seq without LCP arrays)
 // merges each piece sequentially from there.
 constexpr uint32_t MERGE_PIECE = 32;
+constexpr uint32_t MERGE_PIECE_MAX = 4096;
 
 struct MergePair {
     uint64_t a0, a1, b1;
@@ -70,7 +71,8 @@ __device__ __forceinline__ uint32_t pair_of(const uint64_t* first, uint32_t npai
 __global__ void k_merge_split(const uint8_t* __restrict__ chars, uint64_t nchars,
                               const uint64_t* __restrict__ offs, const MergePair* __restrict__ pairs,
                               const uint64_t* __restrict__ first, uint32_t npair,
-                              const uint32_t* __restrict__ ids_in, uint64_t* __restrict__ split)
+                              const uint32_t* __restrict__ ids_in, uint64_t* __restrict__ split,
+                              uint32_t piece)
 {
     const uint64_t ntask = first[npair];
     for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ntask;
@@ -78,7 +80,7 @@ __global__ void k_merge_split(const uint8_t* __restrict__ chars, uint64_t nchars
         const uint32_t p = pair_of(first, npair, t);
         const MergePair pr = pairs[p];
         const uint64_t na = pr.a1 - pr.a0, nb = pr.b1 - pr.a1;
-        const uint64_t d = (t - first[p]) * MERGE_PIECE;
+        const uint64_t d = (t - first[p]) * piece;
         // left-run strings among the first d outputs: the first i with
         // A[i] > B[d - i - 1] (ties go to the left run)
         uint64_t lo = d > nb ? d - nb : 0, hi = min(d, na);
@@ -98,7 +100,7 @@ __global__ void k_merge_seq(const uint8_t* __restrict__ chars, uint64_t nchars,
                             const uint64_t* __restrict__ offs, const MergePair* __restrict__ pairs,
                             const uint64_t* __restrict__ first, uint32_t npair,
                             const uint64_t* __restrict__ split, const uint32_t* __restrict__ ids_in,
-                            uint32_t* __restrict__ ids_out)
+                            uint32_t* __restrict__ ids_out, uint32_t piece)
 {
     const uint64_t ntask = first[npair];
     for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ntask;
@@ -106,8 +108,8 @@ __global__ void k_merge_seq(const uint8_t* __restrict__ chars, uint64_t nchars,
         const uint32_t p = pair_of(first, npair, t);
         const MergePair pr = pairs[p];
         const uint64_t na = pr.a1 - pr.a0, nb = pr.b1 - pr.a1;
-        const uint64_t d0 = (t - first[p]) * MERGE_PIECE;
-        const uint64_t d1 = min(d0 + MERGE_PIECE, na + nb);
+        const uint64_t d0 = (t - first[p]) * piece;
+        const uint64_t d1 = min(d0 + piece, na + nb);
         const uint64_t i0 = split[t];
         const uint64_t i1 = t + 1 < first[p + 1] ? split[t + 1] : na;
         uint64_t i = i0, j = d0 - i0;
@@ -142,7 +144,8 @@ __global__ void k_merge_lcp_seq(const uint8_t* __restrict__ chars, uint64_t ncha
                                 const uint64_t* __restrict__ split,
                                 const uint32_t* __restrict__ ids_in,
                                 const uint32_t* __restrict__ lcp_in,
-                                uint32_t* __restrict__ ids_out, uint32_t* __restrict__ lcp_out)
+                                uint32_t* __restrict__ ids_out, uint32_t* __restrict__ lcp_out,
+                                uint32_t piece)
 {
     const uint64_t ntask = first[npair];
     for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ntask;
@@ -154,8 +157,8 @@ __global__ void k_merge_lcp_seq(const uint8_t* __restrict__ chars, uint64_t ncha
         const uint32_t* B = ids_in + pr.a1;
         const uint32_t* LA = lcp_in + pr.a0;
         const uint32_t* LB = lcp_in + pr.a1;
-        const uint64_t d0 = (t - first[p]) * MERGE_PIECE;
-        const uint64_t d1 = min(d0 + MERGE_PIECE, na + nb);
+        const uint64_t d0 = (t - first[p]) * piece;
+        const uint64_t d1 = min(d0 + piece, na + nb);
         const uint64_t i0 = split[t];
         const uint64_t i1 = t + 1 < first[p + 1] ? split[t + 1] : na;
         const uint64_t j0 = d0 - i0, j1 = d1 - i1;

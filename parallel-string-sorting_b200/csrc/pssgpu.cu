@@ -21,6 +21,7 @@
 #include "kernels_big.cuh"
 #include "kernels_block.cuh"
 #include "kernels_wave.cuh"
+#include "kernels_suffix.cuh"
 #include "prepare.cuh"
 #include "merge.cuh"
 
@@ -139,10 +140,10 @@ static uint64_t workspace_bytes(const Sizes& s)
 
 // Kernel classes reported by pssgpu_ctx_kernel_stats.
 enum KClass { K_INIT = 0, K_SAMPLE, K_CLASSIFY, K_BSTART, K_SCATTER, K_CHILDREN, K_TINY,
-              K_SMALLA, K_SMALLB, K_DEEP, K_BOUNDARY, K_WAVE, K_NCLASS };
+              K_SMALLA, K_SMALLB, K_DEEP, K_BOUNDARY, K_WAVE, K_DBL, K_NCLASS };
 static const char* const kclass_name[K_NCLASS] = {
     "init", "sample", "classify", "bstart", "scatter", "children", "tiny",
-    "small256", "small1024", "deep", "boundary", "wave"};
+    "small256", "small1024", "deep", "boundary", "wave", "doubling"};
 
 struct KStat {
     uint32_t launches = 0;
@@ -189,6 +190,15 @@ struct Ctx {
     bool single_launch = true;
     // polls of a grid-barrier wait in k_wave before it gives up
     uint32_t wait_limit = 1u << 22;
+    // outputs one thread merges in a round of pssgpu_merge_lcp_device
+    uint32_t merge_piece = MERGE_PIECE;
+    // suffix sets finish their deep groups by rank doubling (off: the string
+    // passes sort them like any strings)
+    bool suffix_doubling = true;
+    // the list of groups the passes hand to rank doubling (allocated on the
+    // first suffix-set sort)
+    unsigned char* sfx = nullptr;
+    uint64_t sfx_bytes = 0;
     // splitter-tree levels per size class of big segments (0 = default)
     uint8_t tree_bits_by_size[33] = {};
     // device copy of a batch's instance boundaries
@@ -298,6 +308,8 @@ static int setup_kernels()
     if (done[dev]) return PSSGPU_OK;
     PSS_CUDA(cudaFuncSetAttribute(k_wave, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)sizeof(WaveSmem)));
+    PSS_CUDA(cudaFuncSetAttribute(k_dbl_sort_block<DBL_MAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(12 * DBL_MAX)));
     {
         int coop = 0, sms = 0, per_sm = 0;
         PSS_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
@@ -323,6 +335,97 @@ static int map_device_error(uint32_t err)
     if (err & ERR_TIMEOUT) return fail(PSSGPU_ETIMEOUT, "a bounded device-side wait gave up");
     if (err & ERR_OVERFLOW) return fail(PSSGPU_ECUDA, "an internal work list overflowed");
     return fail(PSSGPU_ECUDA, "internal device error");
+}
+
+// A device buffer of at least `bytes`, grown (contents dropped) when short.
+static int ensure_buf(unsigned char** buf, uint64_t* have, uint64_t bytes)
+{
+    if (*buf && bytes <= *have) return PSSGPU_OK;
+    if (*buf) {
+        cudaFree(*buf);
+        *buf = nullptr;
+        *have = 0;
+    }
+    PSS_CUDA(cudaMalloc(buf, bytes));
+    *have = bytes;
+    return PSSGPU_OK;
+}
+
+// Rank doubling over the ndbl groups the passes handed over (a suffix set):
+// ranks of every suffix, then rounds that sort each group by the rank of its
+// members' suffixes `depth` chars further, until every group is split into
+// single suffixes; with LCP output, the LCPs at the separated positions.
+// Works in the workspace's key and handle arrays, which the passes no longer
+// need. Caller holds c->mu; *err receives the device error bits.
+static int run_doubling(Ctx* c, Work& w, uint32_t ndbl, cudaStream_t st, pssgpu_stats& stats,
+                        uint32_t* err)
+{
+    const uint32_t n = w.n;
+    const uint64_t capn = c->cap.n;
+    DblArrays a{};
+    a.isa = reinterpret_cast<uint32_t*>(w.keys[0]);
+    a.gd[0] = a.isa + capn;
+    a.gd[1] = reinterpret_cast<uint32_t*>(w.keys[1]);
+    a.key = a.gd[1] + capn;
+    a.lb = w.lcp ? reinterpret_cast<uint32_t*>(w.hnd[0]) : nullptr;
+    const int lcls[3] = {L_TINY, L_SMALLA, L_SMALLB};
+    for (int k = 0; k < 3; ++k) {
+        a.list[k][0] = w.list[lcls[k]][0];
+        a.list[k][1] = w.list[lcls[k]][1];
+        a.cap[k] = w.cap[lcls[k]];
+    }
+    uint32_t* hc = c->host_counters;
+    const unsigned gblocks = std::min<uint32_t>(ndbl, 148u * 16u);
+    PSS_CUDA(cudaMemsetAsync(w.counters + C_DBL_CNT, 0, 4 * 6, st));
+    k_dbl_init<<<gblocks, 256, 0, st>>>(w, w.dbl, ndbl);
+    if (a.lb) PSS_CUDA(cudaMemsetAsync(a.lb, 0xFF, 4ull * n, st));
+    k_dbl_isa<<<1184, 256, 0, st>>>(w.perm, n, a.isa);
+    k_dbl_rank<<<gblocks, 256, 0, st>>>(w.perm, w.dbl, ndbl, a, w.counters);
+    stats.kernel_launches += 3;
+    c->kstat[K_DBL].launches += 3;
+    c->kstat[K_DBL].strings += n;
+    PSS_CUDA(cudaGetLastError());
+    PSS_CUDA(cudaMemcpyAsync(hc, w.counters, 4 * C_COUNT, cudaMemcpyDeviceToHost, st));
+    PSS_CUDA(cudaStreamSynchronize(st));
+    int par = 0;
+    // the depth of every group at least doubles per round after the first
+    // (n <= 2^32 chars): a loop beyond this many rounds is an internal error
+    constexpr int MAX_ROUNDS = 64;
+    for (int round = 0; !hc[C_ERR]; ++round) {
+        uint32_t cnt[3];
+        for (int k = 0; k < 3; ++k) cnt[k] = std::min(hc[C_DBL_CNT + 3 * par + k], a.cap[k]);
+        if (!cnt[0] && !cnt[1] && !cnt[2]) break;
+        if (round >= MAX_ROUNDS) return fail(PSSGPU_ETIMEOUT, "rank doubling round limit exceeded");
+        PSS_CUDA(cudaMemsetAsync(w.counters + C_DBL_CNT + 3 * (par ^ 1), 0, 12, st));
+        for (int k = 0; k < 3; ++k)
+            if (cnt[k]) k_dbl_keys<<<(cnt[k] + 7) / 8, 256, 0, st>>>(a.list[k][par], cnt[k], w.perm, a);
+        if (cnt[0])
+            k_dbl_sort_small<<<(cnt[0] + 7) / 8, 256, 0, st>>>(a.list[0][par], cnt[0], w.perm, a,
+                                                               w.counters, par);
+        if (cnt[1])
+            k_dbl_sort_block<DBL_MID><<<cnt[1], 256, 12 * DBL_MID, st>>>(a.list[1][par], w.perm, a,
+                                                                         w.counters, par);
+        if (cnt[2])
+            k_dbl_sort_block<DBL_MAX><<<cnt[2], 512, 12 * DBL_MAX, st>>>(a.list[2][par], w.perm, a,
+                                                                         w.counters, par);
+        const uint32_t launched = (cnt[0] ? 2 : 0) + (cnt[1] ? 2 : 0) + (cnt[2] ? 2 : 0);
+        stats.kernel_launches += launched;
+        c->kstat[K_DBL].launches += launched;
+        PSS_CUDA(cudaGetLastError());
+        PSS_CUDA(cudaMemcpyAsync(hc, w.counters, 4 * C_COUNT, cudaMemcpyDeviceToHost, st));
+        PSS_CUDA(cudaStreamSynchronize(st));
+        par ^= 1;
+    }
+    *err = hc[C_ERR];
+    if (!*err && a.lb) {
+        const uint64_t nchunk = ((uint64_t)n + DBL_LCP_CHUNK - 1) / DBL_LCP_CHUNK;
+        k_dbl_lcp<<<(unsigned)std::min<uint64_t>((nchunk + 255) / 256, 148ull * 16), 256, 0, st>>>(
+            w.chars, w.nchars, w.perm, a.isa, a.lb, w.lcp, n);
+        stats.kernel_launches += 1;
+        c->kstat[K_DBL].launches += 1;
+        PSS_CUDA(cudaGetLastError());
+    }
+    return PSSGPU_OK;
 }
 
 // Sort n strings already resident on the device. Caller holds c->mu.
@@ -353,6 +456,7 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
     const bool wave = !d_inst && c->single_launch && n >= 2 && wave_cap > 0 &&
                       (uint64_t)n <= (uint64_t)wave_cap * WAVE_TILE_MAX;
     int cur = 0;
+    const bool suffix_try = !wave && !d_inst && c->suffix_doubling && n >= 2 && (uint64_t)n == nchars;
     PSS_CUDA(cudaEventRecord(c->ev0, st));
     if (wave) {
         // the counters and the wave state's header are adjacent: one memset
@@ -384,6 +488,8 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
         kt.begin(K_INIT);
         k_init<<<1184, 256, 0, st>>>(w);
         k_roots<<<d_inst ? 148 : 1, 256, 0, st>>>(w, d_inst, ninst);
+        // every string a suffix of one text (n == nchars is necessary)?
+        if (suffix_try) k_suffix_check<<<1184, 256, 0, st>>>(chars, offs, n, w.counters + C_SFX);
         kt.end(K_INIT);
         c->kstat[K_INIT].launches += 2;
         c->kstat[K_INIT].strings += n;
@@ -404,6 +510,15 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
     uint32_t ndeep = hc[C_DEEP + cur];
     uint64_t small_segments = 0;
     uint32_t err = hc[C_ERR];
+    const bool suffix = suffix_try && !err && hc[C_SFX] == 0;
+    if (suffix) {
+        // groups of at least 2 strings: at most n / 2 of them
+        const uint64_t cap = (uint64_t)n / 2 + 2;
+        if ((rc = ensure_buf(&c->sfx, &c->sfx_bytes, 16 * cap))) return rc;
+        w.suffix = 1;
+        w.dbl = reinterpret_cast<Seg*>(c->sfx);
+        w.dbl_cap = (uint32_t)cap;
+    }
     auto pending = [&]() {
         return cnt[L_BIG] || cnt[L_TINY] || cnt[L_SMALLA] || cnt[L_SMALLB] || ndeep;
     };
@@ -569,6 +684,12 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
         err = hc[C_ERR];
         cur = nxt;
     }
+    if (!err && suffix && hc[C_DBL]) {
+        kt.begin(K_DBL);
+        rc = run_doubling(c, w, std::min(hc[C_DBL], w.dbl_cap), st, stats, &err);
+        kt.end(K_DBL);
+        if (rc) return rc;
+    }
     if (!err && lcp) {
         kt.begin(K_BOUNDARY);
         k_boundary_lcp<<<1184, 256, 0, st>>>(w);
@@ -637,6 +758,7 @@ static void ctx_destroy(Ctx* c)
     if (c->io2) cudaFree(c->io2);
     if (c->prep) cudaFree(c->prep);
     if (c->mbuf) cudaFree(c->mbuf);
+    if (c->sfx) cudaFree(c->sfx);
     if (c->inst_buf) cudaFree(c->inst_buf);
     if (c->host_counters) cudaFreeHost(c->host_counters);
     if (c->ev0) cudaEventDestroy(c->ev0);
@@ -650,20 +772,6 @@ static void ctx_destroy(Ctx* c)
     }
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
-}
-
-// A device buffer of at least `bytes`, grown (contents dropped) when short.
-static int ensure_buf(unsigned char** buf, uint64_t* have, uint64_t bytes)
-{
-    if (*buf && bytes <= *have) return PSSGPU_OK;
-    if (*buf) {
-        cudaFree(*buf);
-        *buf = nullptr;
-        *have = 0;
-    }
-    PSS_CUDA(cudaMalloc(buf, bytes));
-    *have = bytes;
-    return PSSGPU_OK;
 }
 
 static int ensure_io(Ctx* c, uint64_t bytes) { return ensure_buf(&c->io, &c->io_bytes, bytes); }
@@ -1177,6 +1285,11 @@ int pssgpu_ctx_set_option(pssgpu_ctx* ctx, int option, int64_t value)
     case PSSGPU_OPT_PROFILE: c->profile = value != 0; return PSSGPU_OK;
     case PSSGPU_OPT_INDIRECT_HANDLES: c->indirect_handles = value != 0; return PSSGPU_OK;
     case PSSGPU_OPT_SINGLE_LAUNCH: c->single_launch = value != 0; return PSSGPU_OK;
+    case PSSGPU_OPT_SUFFIX_DOUBLING: c->suffix_doubling = value != 0; return PSSGPU_OK;
+    case PSSGPU_OPT_MERGE_PIECE:
+        if (value < 1 || value > (int64_t)MERGE_PIECE_MAX) return fail(PSSGPU_EINVAL, "merge piece out of range");
+        c->merge_piece = (uint32_t)value;
+        return PSSGPU_OK;
     case PSSGPU_OPT_WAIT_LIMIT:
         if (value < 1 || value > 0xFFFFFFFFll) return fail(PSSGPU_EINVAL, "wait limit out of range");
         c->wait_limit = (uint32_t)value;
@@ -1338,7 +1451,7 @@ int pssgpu_merge_lcp_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nc
         for (uint32_t p = 0; p < np; ++p) {
             flat.push_back(t);
             const uint64_t m = flat[at_pairs.back() + 3 * p + 2] - flat[at_pairs.back() + 3 * p];
-            t += (m + MERGE_PIECE - 1) / MERGE_PIECE;
+            t += (m + c->merge_piece - 1) / c->merge_piece;
         }
         flat.push_back(t);
         npairs.push_back(np);
@@ -1368,13 +1481,15 @@ int pssgpu_merge_lcp_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nc
         const MergePair* pairs = reinterpret_cast<const MergePair*>(d_flat + at_pairs[i]);
         const uint64_t* first = d_flat + at_first[i];
         const uint32_t np = (uint32_t)npairs[i];
-        k_merge_split<<<blocks, 256, 0, st>>>(d_chars, nchars, d_offs, pairs, first, np, in_ids, split);
+        const uint32_t pc = c->merge_piece;
+        k_merge_split<<<blocks, 256, 0, st>>>(d_chars, nchars, d_offs, pairs, first, np, in_ids, split,
+                                              pc);
         if (with_lcp)
             k_merge_lcp_seq<<<blocks, 256, 0, st>>>(d_chars, nchars, d_offs, pairs, first, np, split,
-                                                    in_ids, in_lcp, out_ids, out_lcp);
+                                                    in_ids, in_lcp, out_ids, out_lcp, pc);
         else
             k_merge_seq<<<blocks, 256, 0, st>>>(d_chars, nchars, d_offs, pairs, first, np, split,
-                                                in_ids, out_ids);
+                                                in_ids, out_ids, pc);
         PSS_CUDA(cudaGetLastError());
         in_ids = out_ids;
         in_lcp = out_lcp;

@@ -15,6 +15,7 @@ constexpr int SMALL_THREADS = 256;
 constexpr int WARP_GROUP_MAX = 32;  // groups this small are finished by one warp
 constexpr int FINAL_INLINE = 64;    // equal-string buckets this small are copied inline
 constexpr int CHUNK = 32;           // tiles per chunk of the destination scan
+constexpr uint32_t DBL_MAX = 4096;  // largest group a suffix sort hands to rank doubling
 
 // segment list classes
 enum : int { L_BIG = 0, L_TINY = 1, L_SMALLA = 2, L_SMALLB = 3, L_NCLASS = 4 };
@@ -39,7 +40,10 @@ enum : int {
     C_P_LAST = C_P_JCHUNKS,
     C_MULTI = 26,     // + parity: big segments of more than CHUNK tiles in the list
     C_DEEP = 28,      // + parity: length of the deep-group list
-    C_COUNT = 32
+    C_SFX = 30,       // suffix-set check: nonzero when the input is not all suffixes of a text
+    C_DBL = 31,       // groups handed to rank doubling by the passes
+    C_DBL_CNT = 32,   // + 3 * parity + class: rank-doubling round lists
+    C_COUNT = 40
 };
 
 struct Work {
@@ -101,6 +105,12 @@ struct Work {
     // splitter-tree levels for a big segment of 2^k..2^(k+1)-1 strings
     // (0: the default rule), set from a tuning table
     uint8_t tree_bits_by_size[33];
+    // Suffix sets (every string is a suffix of one text: offs[i] = i, no NUL
+    // before the last char): '=' groups of at most DBL_MAX strings below
+    // depth 8 go to the rank-doubling list instead of deeper passes.
+    int suffix;
+    Seg* dbl;
+    uint32_t dbl_cap;
 };
 
 // buckets of a classified big segment: the tree's 2^(L+1) - 1, plus the two

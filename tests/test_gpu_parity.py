@@ -179,6 +179,52 @@ def test_deep_repeats_suffixes(pkg, orc, ctx_any):
     check_against_oracle(orc, chars, offs, perm, lcp)
 
 
+def _suffix_text(case):
+    """A NUL-terminated text and its suffix count."""
+    if case == "periodic":
+        t = (b"abcab" * 8000)[:39999]
+    elif case == "dna_copies":
+        return None
+    elif case == "binary":
+        t = bytes(np.random.default_rng(51).integers(97, 99, 60000, dtype=np.uint8))
+    elif case == "runs_of_a":
+        t = b"a" * 12000 + b"b" + b"a" * 3000
+    else:  # an inner NUL: not a suffix set, sorted as strings
+        t = bytes(np.random.default_rng(52).integers(97, 100, 30000, dtype=np.uint8))
+        t = t[:15000] + b"\0" + t[15001:]
+    return np.frombuffer(t + b"\0", dtype=np.uint8).copy()
+
+
+@pytest.mark.parametrize("case", ["periodic", "dna_copies", "binary", "runs_of_a", "inner_nul"])
+@pytest.mark.parametrize("with_lcp", [True, False])
+def test_suffix_doubling(pkg, orc, case, with_lcp):
+    """Suffix sets through the multi-launch path, where groups sharing 8 or
+    more chars finish by rank doubling: a periodic text (groups of thousands,
+    LCPs up to the text length), a DNA text with copied 1-10 KiB blocks, a
+    binary text, long runs of one char, and a text with a NUL inside (not a
+    suffix set: the string path). Checked against the oracle; the doubling
+    must have run for the suffix sets."""
+    if case == "dna_copies":
+        chars = pkg.workloads.dna_text(length=1 << 20, seed=53)[: (1 << 20) + 1].copy()
+    else:
+        chars = _suffix_text(case)
+    n = chars.shape[0]
+    offs = np.arange(n, dtype=np.uint64)
+    c = pkg.Context(0)
+    try:
+        c.set_option(c.OPT_SINGLE_LAUNCH, 0)
+        perm, lcp = c.sort_host(chars, offs, lcp=with_lcp)
+        used = {k["name"]: k["launches"] for k in c.kernel_stats()}.get("doubling", 0)
+    finally:
+        c.close()
+    assert (used > 0) == (case != "inner_nul")
+    if with_lcp:
+        check_against_oracle(orc, chars, offs, perm, lcp)
+    else:
+        assert orc.check_permutation(perm)
+        assert orc.check_order(chars, offs, perm) == -1
+
+
 @pytest.mark.parametrize("n,alpha,lmax,seed", [(3000, b"ab", 40, 31), (200000, b"abc", 30, 32)])
 def test_indirect_handles(pkg, orc, n, alpha, lmax, seed):
     """The path for inputs whose string id and arena offset do not fit one

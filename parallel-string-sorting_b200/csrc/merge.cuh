@@ -189,6 +189,10 @@ __global__ void k_merge_lcp_seq(const uint8_t* __restrict__ chars, uint64_t ncha
                 }
             }
         }
+        // the heads' ids and arena offsets stay in registers: one offset
+        // load per output, and a compare reads chars only
+        uint32_t ida = i < i1 ? A[i] : 0u, idb = j < j1 ? B[j] : 0u;
+        uint64_t oa = i < i1 ? __ldg(offs + ida) : 0ull, ob = j < j1 ? __ldg(offs + idb) : 0ull;
         for (uint64_t d = d0; d < d1; ++d) {
             bool take_a;
             if (i >= i1) take_a = false;
@@ -196,17 +200,25 @@ __global__ void k_merge_lcp_seq(const uint8_t* __restrict__ chars, uint64_t ncha
             else if (ha != hb) take_a = ha > hb;
             else {
                 uint32_t l;
-                take_a = compare_from(chars, nchars, __ldg(offs + A[i]), __ldg(offs + B[j]), ha, &l) <= 0;
+                take_a = compare_from(chars, nchars, oa, ob, ha, &l) <= 0;
                 if (take_a) hb = l; else ha = l;  // the loser's LCP with the new last output
             }
-            ids_out[pr.a0 + d] = take_a ? A[i] : B[j];
+            ids_out[pr.a0 + d] = take_a ? ida : idb;
             if (lcp_out && d > 0) lcp_out[pr.a0 + d] = take_a ? ha : hb;
             if (take_a) {
                 ++i;
                 ha = i < na ? LA[i] : 0u;  // against its predecessor, the last output
+                if (i < i1) {
+                    ida = A[i];
+                    oa = __ldg(offs + ida);
+                }
             } else {
                 ++j;
                 hb = j < nb ? LB[j] : 0u;
+                if (j < j1) {
+                    idb = B[j];
+                    ob = __ldg(offs + idb);
+                }
             }
         }
     }

@@ -48,7 +48,11 @@ constexpr uint32_t WAVE_TILE_MAX = (uint32_t)WAVE_THREADS * WAVE_PER;
 struct WaveState {
     uint32_t bar;        // grid barrier arrivals
     uint32_t next_task;  // phase-D windows taken
-    uint32_t pad[14];
+    uint32_t pad[4];
+    // with tracing on: the largest SM-clock cycles any block spent in phase
+    // A (incl. block 0's samples), the first barrier wait, B (+ the second
+    // wait), C (+ the third) and D (+ the LCPs)
+    unsigned long long cycles[5];
     uint32_t gcount[WAVE_BKT];   // bucket counts
     uint64_t spl[WAVE_BKT / 2];  // sorted splitters
     uint64_t tree[WAVE_BKT / 2]; // level order, index 1..k
@@ -194,8 +198,16 @@ __device__ __forceinline__ void wave_sort_run(const Work& w, WaveState* ws, Wave
 // w.cur must be 0: the wave's leftovers (big segments, deep groups) go to
 // the lists of parity 1, with their strings in buffer 1.
 __global__ void __launch_bounds__(WAVE_THREADS, 2) k_wave(Work w, WaveState* ws, uint32_t L,
-                                                          uint32_t limit)
+                                                          uint32_t limit, int trace)
 {
+    const long long c0 = clock64();
+    long long cl = c0;
+    auto lap = [&](int k) {  // phase k ended here (tracing only)
+        if (!trace || threadIdx.x) return;
+        const long long t = clock64();
+        atomicMax(ws->cycles + k, (unsigned long long)(t - cl));
+        cl = t;
+    };
     extern __shared__ __align__(16) unsigned char smem_raw[];
     WaveSmem& sm = *reinterpret_cast<WaveSmem*>(smem_raw);
     __shared__ uint32_t wscratch[WAVE_THREADS / 32][32];
@@ -245,7 +257,9 @@ __global__ void __launch_bounds__(WAVE_THREADS, 2) k_wave(Work w, WaveState* ws,
             ws->tree[v] = samp[2 * r + 1];
         }
     }
+    lap(0);
     if (!wave_barrier(ws, 1, err, limit)) return;
+    lap(1);
     // input errors are all flagged in phase A: every block sees the same
     // bits here and leaves together
     if (*(volatile uint32_t*)err & (ERR_OFFSET | ERR_UNTERMINATED)) return;
@@ -281,6 +295,7 @@ __global__ void __launch_bounds__(WAVE_THREADS, 2) k_wave(Work w, WaveState* ws,
         cnt[b] = c ? atomicAdd(&ws->gcount[b], c) : 0u;
     }
     if (!wave_barrier(ws, 2, err, limit)) return;
+    lap(2);
 
     // ---- C: bucket starts, scatter ----------------------------------------
     for (uint32_t b = threadIdx.x; b < B; b += WAVE_THREADS) sm.start[b] = __ldcg(ws->gcount + b);
@@ -301,6 +316,8 @@ __global__ void __launch_bounds__(WAVE_THREADS, 2) k_wave(Work w, WaveState* ws,
         w.hnd[1][dest] = hnd[j];
     }
     if (!wave_barrier(ws, 3, err, limit)) return;
+    lap(3);
+    (void)c0;
 
     // ---- D: buckets over WAVE_WINDOW strings, one block each --------------
     for (uint32_t b = blockIdx.x; b < B; b += G) {
@@ -347,7 +364,10 @@ __global__ void __launch_bounds__(WAVE_THREADS, 2) k_wave(Work w, WaveState* ws,
         }
         __syncthreads();  // task and big_at are rewritten next round
     }
-    if (!w.lcp) return;
+    if (!w.lcp) {
+        lap(4);
+        return;
+    }
 
     // ---- LCPs at the bucket boundaries ---------------------------------------
     if (!wave_barrier(ws, 4, err, limit)) return;
@@ -360,6 +380,7 @@ __global__ void __launch_bounds__(WAVE_THREADS, 2) k_wave(Work w, WaveState* ws,
         const uint64_t lo_this = (b & 1) ? __ldcg(ws->spl + (b >> 1)) : __ldcg(ws->bmin + b);
         w.lcp[P] = lcp_key_type(hi_prev, lo_this);
     }
+    lap(4);
 }
 
 }  // namespace pssgpu

@@ -471,7 +471,8 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
         w.cur = 0;
         WaveState* ws = c->wave;
         uint32_t limit = c->wait_limit;
-        void* args[] = {&w, &ws, &L, &limit};
+        int trace = c->trace ? 1 : 0;
+        void* args[] = {&w, &ws, &L, &limit, &trace};
         kt.begin(K_WAVE);
         PSS_CUDA(cudaLaunchCooperativeKernel((const void*)k_wave, dim3(G), dim3(WAVE_THREADS), args,
                                              sizeof(WaveSmem), st));
@@ -510,6 +511,14 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
     uint32_t ndeep = hc[C_DEEP + cur];
     uint64_t small_segments = 0;
     uint32_t err = hc[C_ERR];
+    if (wave && c->trace) {
+        unsigned long long cyc[5] = {};
+        if (cudaMemcpy(cyc, c->wave->cycles, sizeof(cyc), cudaMemcpyDeviceToHost) == cudaSuccess)
+            std::fprintf(stderr,
+                         "pssgpu single launch: %u strings, SM cycles (max over blocks): keys + samples "
+                         "%llu, first barrier wait %llu, classify %llu, scatter %llu, bucket sorts %llu\n",
+                         n, cyc[0], cyc[1], cyc[2], cyc[3], cyc[4]);
+    }
     const bool suffix = suffix_try && !err && hc[C_SFX] == 0;
     if (suffix) {
         // groups of at least 2 strings: at most n / 2 of them

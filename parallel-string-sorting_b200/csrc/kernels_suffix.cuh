@@ -103,9 +103,42 @@ __global__ void k_dbl_rank(const uint32_t* __restrict__ perm, const Seg* __restr
     }
 }
 
+// Warp-aggregated append to the round lists: every lane of the warp calls;
+// lanes with push set append s (one global reservation per class and warp).
+__device__ __forceinline__ void dbl_push_warp(DblArrays& a, uint32_t* counters, int par, bool push,
+                                              const Seg& s)
+{
+    const uint32_t lane = threadIdx.x & 31;
+    const int cls = push ? dbl_class(s.size) : 3;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const uint32_t m = __ballot_sync(0xffffffffu, cls == c);
+        if (!m) continue;
+        const int leader = __ffs(m) - 1;
+        uint32_t base = 0;
+        if (lane == (uint32_t)leader) base = atomicAdd(counters + C_DBL_CNT + 3 * par + c, (uint32_t)__popc(m));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (cls == c) {
+            const uint32_t at = base + __popc(m & ((1u << lane) - 1u));
+            if (at < a.cap[c]) a.list[c][par][at] = s;
+            else set_error(counters + C_ERR, ERR_OVERFLOW);
+        }
+    }
+}
+
 // Round step 1: every member's key, the rank of the suffix `depth` chars
 // further (members share depth chars, none of them NUL, so x + depth < n).
-// One warp per group.
+// k_dbl_keys_small: one thread per group of at most 32; k_dbl_keys: one warp
+// per larger group.
+__global__ void k_dbl_keys_small(const Seg* __restrict__ list, uint32_t count,
+                                 const uint32_t* __restrict__ perm, DblArrays a)
+{
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= count) return;
+    const Seg s = list[g];
+    for (uint32_t q = 0; q < s.size; ++q) a.key[s.begin + q] = a.isa[perm[s.begin + q] + s.depth];
+}
+
 __global__ void k_dbl_keys(const Seg* __restrict__ list, uint32_t count,
                            const uint32_t* __restrict__ perm, DblArrays a)
 {
@@ -116,57 +149,80 @@ __global__ void k_dbl_keys(const Seg* __restrict__ list, uint32_t count,
         a.key[s.begin + q] = a.isa[perm[s.begin + q] + s.depth];
 }
 
-// One sorted run [i0, i1) of equal keys K inside group s (positions
-// s.begin + i): a single member is final; more form a subgroup whose
-// members share s.depth + gd(K) chars.
-__device__ __forceinline__ void dbl_run(DblArrays& a, uint32_t* counters, int par, const Seg& s,
-                                        uint32_t i0, uint32_t len, uint32_t K)
+// The run of equal keys K that starts at offset i0 of group s and has len
+// members: the LCP bound at its start, and for len >= 2 the subgroup (with
+// its depth recorded for the next round) into *out. Returns whether *out
+// is to be appended.
+__device__ __forceinline__ bool dbl_run(DblArrays& a, int par, const Seg& s, uint32_t i0,
+                                        uint32_t len, uint32_t K, Seg* out)
 {
     const uint32_t p = s.begin + i0;
     if (a.lb && i0 > 0) a.lb[p] = s.depth;  // separated from p - 1 at this depth
-    if (len < 2) return;
+    if (len < 2) return false;
     const uint32_t nd = s.depth + a.gd[par][K];
     a.gd[par ^ 1][p] = nd;
-    dbl_push(a, counters, par ^ 1, Seg{p, len, nd, 0u});
+    *out = Seg{p, len, nd, 0u};
+    return true;
 }
 
-// Round step 2 for groups of at most 32 members, one warp each: sort by
-// (key, member), write perm and the new ranks, split into runs.
+// Round step 2 for groups of at most 32 members: each warp takes
+// DBL_PER_WARP consecutive list entries and packs them into windows of 32
+// lanes; a window sorts by (group, key, lane), writes perm and the new ranks,
+// and splits every group into runs of equal keys.
+constexpr uint32_t DBL_PER_WARP = 16;
 __global__ void k_dbl_sort_small(const Seg* __restrict__ list, uint32_t count,
                                  uint32_t* __restrict__ perm, DblArrays a, uint32_t* counters, int par)
 {
-    const uint32_t g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (g >= count) return;
     const uint32_t lane = threadIdx.x & 31;
-    const Seg s = list[g];
-    const bool real = lane < s.size;
-    const uint32_t x = real ? perm[s.begin + lane] : 0u;
-    uint64_t t = real ? ((uint64_t)a.key[s.begin + lane] << 32) | lane : ~0ull;
-#pragma unroll
-    for (uint32_t kk = 2; kk <= 32; kk <<= 1) {
-#pragma unroll
-        for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
-            const uint64_t o = __shfl_xor_sync(0xffffffffu, t, j);
-            const bool lower = (lane & j) == 0, asc = (lane & kk) == 0;
-            if ((lower == asc) ? (o < t) : (o > t)) t = o;
+    const uint32_t g0 = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * DBL_PER_WARP;
+    if (g0 >= count) return;  // whole warp
+    const uint32_t ng = min(DBL_PER_WARP, count - g0);
+    const Seg* L = list + g0;
+    for_each_window(ng, [&](uint32_t j) { return L[j].size; }, [&](uint32_t j0, uint32_t cnt) {
+        // lane -> (group q of the window, member); gs = the group's first lane
+        uint32_t off = 0, gq = 31, gs = 32;
+        Seg s{};
+        for (uint32_t q = 0; q < cnt; ++q) {
+            const Seg t = L[j0 + q];
+            if (lane >= off && lane < off + t.size) {
+                gq = q;
+                gs = off;
+                s = t;
+            }
+            off += t.size;
         }
-    }
-    const uint32_t K = (uint32_t)(t >> 32);
-    const uint32_t mx = __shfl_sync(0xffffffffu, x, (uint32_t)t & 31u);
-    const uint32_t pk = __shfl_up_sync(0xffffffffu, K, 1);
-    const bool start = real && (lane == 0 || pk != K);
-    const uint32_t S = __ballot_sync(0xffffffffu, start);
-    const uint32_t R = __ballot_sync(0xffffffffu, real);
-    // this lane's run: from the last start at or below it to the next start
-    const uint32_t rs = 31u - __clz(S & (0xFFFFFFFFu >> (31 - lane)));
-    const uint32_t above = lane == 31 ? 0u : (S & (0xFFFFFFFFu << (lane + 1)));
-    const uint32_t re = above ? (uint32_t)(__ffs(above) - 1) : (uint32_t)__popc(R);
-    if (real) {
-        const uint32_t p = s.begin + lane;
-        perm[p] = mx;
-        a.isa[mx] = s.begin + rs;  // final position for a single member
-        if (start) dbl_run(a, counters, par, s, lane, re - rs, K);
-    }
+        const bool real = gs < 32;
+        const uint32_t mem = real ? lane - gs : 0u;
+        const uint32_t x = real ? perm[s.begin + mem] : 0u;
+        uint64_t t = real ? ((uint64_t)gq << 58) | ((uint64_t)a.key[s.begin + mem] << 5) | lane : ~0ull;
+#pragma unroll
+        for (uint32_t kk = 2; kk <= 32; kk <<= 1) {
+#pragma unroll
+            for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
+                const uint64_t o = __shfl_xor_sync(0xffffffffu, t, j);
+                const bool lower = (lane & j) == 0, asc = (lane & kk) == 0;
+                if ((lower == asc) ? (o < t) : (o > t)) t = o;
+            }
+        }
+        // groups keep their lane ranges: sorted by group first
+        const uint32_t K = (uint32_t)(t >> 5);
+        const uint32_t mx = __shfl_sync(0xffffffffu, x, (uint32_t)t & 31u);
+        const uint32_t pk = __shfl_up_sync(0xffffffffu, K, 1);
+        const bool start = real && (lane == gs || pk != K);
+        const uint32_t S = __ballot_sync(0xffffffffu, start);
+        const uint32_t rs = 31u - __clz(S & (0xFFFFFFFFu >> (31 - lane)));
+        const uint32_t above = lane == 31 ? 0u : (S & (0xFFFFFFFFu << (lane + 1)));
+        const uint32_t ge = gs + (real ? s.size : 0u);
+        const uint32_t re = above ? min((uint32_t)(__ffs(above) - 1), ge) : ge;
+        bool push = false;
+        Seg ns{};
+        if (real) {
+            perm[s.begin + mem] = mx;
+            a.isa[mx] = s.begin + (rs - gs);  // final position for a single member
+            if (start) push = dbl_run(a, par, s, rs - gs, re - rs, K, &ns);
+        }
+        dbl_push_warp(a, counters, par ^ 1, push, ns);
+    });
 }
 
 // Round step 2 for groups of 33..MAXM members, one block each: a bitonic
@@ -194,16 +250,23 @@ __global__ void __launch_bounds__(MAXM <= DBL_MID ? 256 : 512) k_dbl_sort_block(
     }
     __syncthreads();
     bitonic_sort_block(sk, S);
-    for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
-        const uint32_t K = (uint32_t)(sk[i] >> 32);
-        const uint32_t x = sx[(uint32_t)sk[i] & (MAXM - 1)];
-        perm[s.begin + i] = x;
-        if (i > 0 && (uint32_t)(sk[i - 1] >> 32) == K) continue;
-        // a run starts here: its length, then every member's rank
-        uint32_t e = i + 1;
-        while (e < m && (uint32_t)(sk[e] >> 32) == K) ++e;
-        for (uint32_t q = i; q < e; ++q) a.isa[sx[(uint32_t)sk[q] & (MAXM - 1)]] = s.begin + i;
-        dbl_run(a, counters, par, s, i, e - i, K);
+    // warp-uniform trip counts, so that appends aggregate per warp
+    for (uint32_t i0 = threadIdx.x & ~31u; i0 < m; i0 += blockDim.x) {
+        const uint32_t i = i0 + (threadIdx.x & 31);
+        bool push = false;
+        Seg ns{};
+        if (i < m) {
+            const uint32_t K = (uint32_t)(sk[i] >> 32);
+            perm[s.begin + i] = sx[(uint32_t)sk[i] & (MAXM - 1)];
+            if (i == 0 || (uint32_t)(sk[i - 1] >> 32) != K) {
+                // a run starts here: its length, then every member's rank
+                uint32_t e = i + 1;
+                while (e < m && (uint32_t)(sk[e] >> 32) == K) ++e;
+                for (uint32_t q = i; q < e; ++q) a.isa[sx[(uint32_t)sk[q] & (MAXM - 1)]] = s.begin + i;
+                push = dbl_run(a, par, s, i, e - i, K, &ns);
+            }
+        }
+        dbl_push_warp(a, counters, par ^ 1, push, ns);
     }
 }
 

@@ -8,18 +8,19 @@
 // 405-676). Here the same steps are phases of one kernel, separated by grid
 // barriers (all blocks are co-resident by the cooperative launch):
 //   A  every block gathers the first 8 chars (get_char_uint64_simple) of its
-//      tile of strings into registers; block 0 also draws 2^(L+1) samples,
-//      sorts them and writes the splitters and the level-order tree
-//      (SampleSortStep::sample, TreeBuilderLevelOrder)
-//   B  classify the tile against the tree (find_bkt), count per bucket in
+//      tile of strings into registers; the first blocks also draw 2^(L+1)
+//      samples in chunks of 512 and sort their chunk
+//   B  every block merges the sorted chunks and builds the splitters and the
+//      level-order tree itself (SampleSortStep::sample,
+//      TreeBuilderLevelOrder), classifies its tile (find_bkt), counts per bucket in
 //      shared memory, reserve the tile's share of every bucket with one
 //      global atomic per non-empty bucket (count, hpp:1414-1435)
 //   C  bucket starts (count_finished), scatter keys and handles in bucket
 //      order (distribute, hpp:1464-1490)
 //   D  a dynamic queue of windows of WAVE_WINDOW positions: the runs of
 //      buckets of at most WAVE_WINDOW strings that start in a window are
-//      finished by the block sorter (block_sort_groups, the SmallsortJob
-//      counterpart); larger buckets are finished alone (up to
+//      finished by the block sorter as one group (block_sort_groups, the
+//      SmallsortJob counterpart); larger buckets are finished alone (up to
 //      WAVE_SORT_MAX strings), copied out when their strings are all equal,
 //      or handed to the level-synchronous passes as a segment
 //      (distribute_finished, hpp:1492-1584). With LCP output a fourth
@@ -42,6 +43,7 @@ constexpr int WAVE_BKT = 2 << WAVE_MAX_BITS;   // 4096 bucket slots
 constexpr int WAVE_WINDOW = 1024;     // positions per window task
 constexpr int WAVE_SORT_MAX = 2048;   // the block sorter of phase D
 constexpr uint32_t WAVE_TILE_MAX = (uint32_t)WAVE_THREADS * WAVE_PER;
+constexpr uint32_t WAVE_SAMPLE_CHUNK = WAVE_THREADS;  // samples one block draws and sorts
 
 // Global state of one wave sort (in the workspace). The header is zeroed by
 // the host before the launch; everything else is written inside.
@@ -55,7 +57,7 @@ struct WaveState {
     unsigned long long cycles[5];
     uint32_t gcount[WAVE_BKT];   // bucket counts
     uint64_t spl[WAVE_BKT / 2];  // sorted splitters
-    uint64_t tree[WAVE_BKT / 2]; // level order, index 1..k
+    uint64_t samp[WAVE_BKT];     // the samples, sorted in chunks of WAVE_SAMPLE_CHUNK
     uint64_t bmin[WAVE_BKT];     // key range of '<' buckets (LCP output only)
     uint64_t bmax[WAVE_BKT];
 };
@@ -63,7 +65,7 @@ struct WaveState {
 // Dynamic shared memory of k_wave: bucket starts, then either the phase A-C
 // view (samples / tree, per-bucket counts) or the block sorter's.
 struct WaveSmemABC {
-    uint64_t tree[WAVE_BKT];     // block 0: up to 2^(L+1) samples; then tree[1..k]
+    uint64_t m[2][WAVE_BKT];     // sample chunks merged back and forth; then the tree
     uint32_t cnt[WAVE_BKT];      // per bucket: count in the tile, then the tile's base
 };
 struct WaveSmem {
@@ -148,7 +150,11 @@ __device__ __forceinline__ void wave_range_block(const Work& w, WaveState* ws, u
 
 // Phase D: sort the strings at positions [P, P + m) of buffer 1, the buckets
 // [b0, b1) (all of at most WAVE_SORT_MAX strings together), with the block
-// sorter. Bucket key ranges are recorded when the LCP array is wanted.
+// sorter. The run is one group at depth 0: its buckets are consecutive key
+// ranges and the keys at depth 0 are cached, so one sample-sort step over
+// the whole run (about 8 strings per bucket) replaces a step per bucket.
+// Bucket key ranges are recorded when the LCP array is wanted (the LCPs at
+// the run's bucket boundaries follow from them).
 __device__ __forceinline__ void wave_sort_run(const Work& w, WaveState* ws, WaveSmem& sm,
                                               uint32_t b0, uint32_t b1, uint32_t (*wscratch)[32],
                                               uint32_t* err)
@@ -163,34 +169,22 @@ __device__ __forceinline__ void wave_sort_run(const Work& w, WaveState* ws, Wave
     if (threadIdx.x == 0) {
         bs.ng = 0;
         bs.nw = 0;
+        if (m > 1) blk_push<WAVE_SORT_MAX, WAVE_THREADS>(bs, 0, m, 0u, true, err);
     }
     __syncthreads();
-    for (uint32_t b = b0 + threadIdx.x; b < b1; b += WAVE_THREADS) {
-        const uint32_t st = sm.start[b], c = sm.start[b + 1] - st;
-        if (c == 0) continue;
-        if (b & 1) {
-            const uint64_t s = __ldcg(ws->spl + (b >> 1));
-            if (key_terminated(s)) {
-                // all equal: final where they stand
-                if (w.lcp)
-                    for (uint32_t q = 1; q < c; ++q) w.lcp[st + q] = lcp_key_depth(s);
-            } else if (c > 1) {
-                blk_push<WAVE_SORT_MAX, WAVE_THREADS>(bs, st - P, c, 8u, false, err);
+    if (w.lcp) {
+        for (uint32_t b = b0 + threadIdx.x; b < b1; b += WAVE_THREADS) {
+            const uint32_t st = sm.start[b], c = sm.start[b + 1] - st;
+            if (c == 0 || (b & 1)) continue;  // '=' buckets: the splitter is their key
+            uint64_t mn = ~0ull, mx = 0;
+            for (uint32_t q = 0; q < c; ++q) {
+                mn = min(mn, bs.key[st - P + q]);
+                mx = max(mx, bs.key[st - P + q]);
             }
-        } else {
-            if (w.lcp) {
-                uint64_t mn = ~0ull, mx = 0;
-                for (uint32_t q = 0; q < c; ++q) {
-                    mn = min(mn, bs.key[st - P + q]);
-                    mx = max(mx, bs.key[st - P + q]);
-                }
-                ws->bmin[b] = mn;
-                ws->bmax[b] = mx;
-            }
-            if (c > 1) blk_push<WAVE_SORT_MAX, WAVE_THREADS>(bs, st - P, c, 0u, true, err);
+            ws->bmin[b] = mn;
+            ws->bmax[b] = mx;
         }
     }
-    __syncthreads();
     block_sort_groups<WAVE_SORT_MAX, WAVE_THREADS>(w, bs, P, m, 1, wscratch, err);
     __syncthreads();
 }
@@ -239,23 +233,21 @@ __global__ void __launch_bounds__(WAVE_THREADS, 2) k_wave(Work w, WaveState* ws,
             key[j] = load_key(w.chars, w.nchars, off);
         }
     }
-    if (blockIdx.x == 0) {
-        uint64_t* samp = sm.u.abc.tree;
-        const uint32_t S = 2u << L;  // oversampling factor 2 (hpp:1388)
-        for (uint32_t i = threadIdx.x; i < S; i += WAVE_THREADS) {
-            const uint64_t h = mix64(0x7761766573616d70ull ^ i);
+    // 2^(L+1) samples (oversampling factor 2, hpp:1388), drawn and sorted in
+    // chunks of WAVE_SAMPLE_CHUNK by the first blocks
+    const uint32_t S = 2u << L;
+    const uint32_t chunk = min(S, WAVE_SAMPLE_CHUNK);
+    for (uint32_t c = blockIdx.x; c < S / chunk; c += G) {
+        uint64_t* samp = sm.u.abc.m[0];
+        if (threadIdx.x < chunk) {
+            const uint64_t h = mix64(0x7761766573616d70ull ^ (c * chunk + threadIdx.x));
             const uint32_t r = (uint32_t)(((h >> 32) * n) >> 32);
-            samp[i] = load_key(w.chars, w.nchars, __ldg(w.offs + r));
+            samp[threadIdx.x] = load_key(w.chars, w.nchars, __ldg(w.offs + r));
         }
         __syncthreads();
-        bitonic_sort_block(samp, S);
-        for (uint32_t j = threadIdx.x; j < k; j += WAVE_THREADS) ws->spl[j] = samp[2 * j + 1];
-        for (uint32_t v = 1 + threadIdx.x; v <= k; v += WAVE_THREADS) {
-            const uint32_t h = 31 - __clz((int)v);
-            const uint32_t p = v - (1u << h);
-            const uint32_t r = ((2 * p + 1) << (L - 1 - h)) - 1;  // in-order rank
-            ws->tree[v] = samp[2 * r + 1];
-        }
+        bitonic_sort_block(samp, chunk);
+        if (threadIdx.x < chunk) ws->samp[c * chunk + threadIdx.x] = samp[threadIdx.x];
+        __syncthreads();
     }
     lap(0);
     if (!wave_barrier(ws, 1, err, limit)) return;
@@ -264,10 +256,49 @@ __global__ void __launch_bounds__(WAVE_THREADS, 2) k_wave(Work w, WaveState* ws,
     // bits here and leaves together
     if (*(volatile uint32_t*)err & (ERR_OFFSET | ERR_UNTERMINATED)) return;
 
-    // ---- B: classify, count, reserve -------------------------------------
-    uint64_t* tree = sm.u.abc.tree;
+    // ---- B: the splitter tree (every block), classify, count, reserve -----
+    // Merge the sorted sample chunks (merge path: each thread makes 8
+    // consecutive outputs of a pair of runs), then the splitters are every
+    // second sample and the tree is their level order.
+    uint64_t* src = sm.u.abc.m[0];
+    uint64_t* dst = sm.u.abc.m[1];
+    for (uint32_t i = threadIdx.x; i < S; i += WAVE_THREADS) src[i] = __ldcg(ws->samp + i);
+    __syncthreads();
+    for (uint32_t R = chunk; R < S; R <<= 1) {
+        for (uint32_t o0 = 8 * threadIdx.x; o0 < S; o0 += 8 * WAVE_THREADS) {
+            const uint64_t* A = src + (o0 / (2 * R)) * (2 * R);
+            const uint64_t* Bv = A + R;
+            const uint32_t d = o0 % (2 * R);
+            // A-run members among the first d outputs (ties: A first)
+            uint32_t lo = d > R ? d - R : 0u, hi = min(d, R);
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (A[mid] <= Bv[d - mid - 1]) lo = mid + 1; else hi = mid;
+            }
+            uint32_t i = lo, j = d - lo;
+            uint64_t* out = dst + (o0 - d) + d;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const bool ta = j >= R || (i < R && A[i] <= Bv[j]);
+                out[q] = ta ? A[i] : Bv[j];
+                if (ta) ++i; else ++j;
+            }
+        }
+        __syncthreads();
+        uint64_t* t = src;
+        src = dst;
+        dst = t;
+    }
+    uint64_t* tree = dst;  // src holds the sorted samples
     uint32_t* cnt = sm.u.abc.cnt;
-    for (uint32_t v = 1 + threadIdx.x; v <= k; v += WAVE_THREADS) tree[v] = __ldcg(ws->tree + v);
+    if (blockIdx.x == 0)
+        for (uint32_t j = threadIdx.x; j < k; j += WAVE_THREADS) ws->spl[j] = src[2 * j + 1];
+    for (uint32_t v = 1 + threadIdx.x; v <= k; v += WAVE_THREADS) {
+        const uint32_t h = 31 - __clz((int)v);
+        const uint32_t p = v - (1u << h);
+        const uint32_t r = ((2 * p + 1) << (L - 1 - h)) - 1;  // in-order rank
+        tree[v] = src[2 * r + 1];
+    }
     for (uint32_t b = threadIdx.x; b < B; b += WAVE_THREADS) cnt[b] = 0;
     __syncthreads();
     uint32_t pk[WAVE_PER];  // (bucket << 16) | rank inside the tile's share

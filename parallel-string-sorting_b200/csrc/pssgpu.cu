@@ -397,11 +397,14 @@ static int run_doubling(Ctx* c, Work& w, uint32_t ndbl, cudaStream_t st, pssgpu_
         if (!cnt[0] && !cnt[1] && !cnt[2]) break;
         if (round >= MAX_ROUNDS) return fail(PSSGPU_ETIMEOUT, "rank doubling round limit exceeded");
         PSS_CUDA(cudaMemsetAsync(w.counters + C_DBL_CNT + 3 * (par ^ 1), 0, 12, st));
-        for (int k = 0; k < 3; ++k)
+        if (cnt[0]) k_dbl_keys_small<<<(cnt[0] + 255) / 256, 256, 0, st>>>(a.list[0][par], cnt[0], w.perm, a);
+        for (int k = 1; k < 3; ++k)
             if (cnt[k]) k_dbl_keys<<<(cnt[k] + 7) / 8, 256, 0, st>>>(a.list[k][par], cnt[k], w.perm, a);
-        if (cnt[0])
-            k_dbl_sort_small<<<(cnt[0] + 7) / 8, 256, 0, st>>>(a.list[0][par], cnt[0], w.perm, a,
-                                                               w.counters, par);
+        if (cnt[0]) {
+            constexpr uint32_t per_block = 8 * DBL_PER_WARP;  // 8 warps
+            k_dbl_sort_small<<<(cnt[0] + per_block - 1) / per_block, 256, 0, st>>>(
+                a.list[0][par], cnt[0], w.perm, a, w.counters, par);
+        }
         if (cnt[1])
             k_dbl_sort_block<DBL_MID><<<cnt[1], 256, 12 * DBL_MID, st>>>(a.list[1][par], w.perm, a,
                                                                          w.counters, par);
@@ -847,6 +850,39 @@ static int text_write(Ctx* c, uint8_t* d_text, uint64_t size, int mode, uint64_t
     return PSSGPU_OK;
 }
 
+// Host text in, host results out (the body of pssgpu_sort_text_host; the
+// suffix-pointer drop-ins use it too). Caller holds c->mu; size > 0.
+static int sort_text_host_locked(Ctx* c, const uint8_t* text, uint64_t size, int mode,
+                                 uint32_t* perm, uint32_t* lcp, uint64_t cap, uint64_t* n_out)
+{
+    PSS_CUDA(cudaSetDevice(c->device));
+    cudaStream_t st = c->stream;
+    const uint64_t b_text = align256(size + PSSGPU_ARENA_PAD);
+    int rc;
+    if ((rc = ensure_io(c, b_text))) return rc;
+    uint8_t* d_text = c->io;
+    PSS_CUDA(cudaMemcpyAsync(d_text, text, size, cudaMemcpyHostToDevice, st));
+    PSS_CUDA(cudaMemsetAsync(d_text + size, 0, b_text - size, st));
+    uint64_t n = 0;
+    if ((rc = text_count(c, d_text, size, mode, &n, st))) return rc;
+    *n_out = n;
+    if (n > cap) return fail(PSSGPU_EINVAL, "result arrays too small");
+    if ((rc = check_args(size, n))) return rc;
+    const uint64_t b_offs = align256(8 * n), b_perm = align256(4 * n);
+    const uint64_t b_lcp = lcp ? align256(4 * n) : 0;
+    if ((rc = ensure_buf(&c->io2, &c->io2_bytes, b_offs + b_perm + b_lcp))) return rc;
+    uint64_t* d_offs = (uint64_t*)c->io2;
+    uint32_t* d_perm = (uint32_t*)(c->io2 + b_offs);
+    uint32_t* d_lcp = lcp ? (uint32_t*)(c->io2 + b_offs + b_perm) : nullptr;
+    if ((rc = text_write(c, d_text, size, mode, d_offs, st))) return rc;
+    if ((rc = run_sort(c, d_text, size, d_offs, (uint32_t)n, d_perm, d_lcp, st))) return rc;
+    PSS_CUDA(cudaMemcpyAsync(perm, d_perm, 4 * n, cudaMemcpyDeviceToHost, st));
+    if (lcp && n > 1)
+        PSS_CUDA(cudaMemcpyAsync(lcp + 1, d_lcp + 1, 4 * (n - 1), cudaMemcpyDeviceToHost, st));
+    PSS_CUDA(cudaStreamSynchronize(st));
+    return PSSGPU_OK;
+}
+
 // Host buffers in, host buffers out. Caller holds c->mu.
 static int sort_host_locked(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_t* offs,
                             uint64_t n, uint32_t* perm, uint32_t* lcp)
@@ -1002,23 +1038,48 @@ static int sort_pointer_array(unsigned char** strings, unsigned char** out, uint
     if (arena_lo) {
         const uintptr_t A = (uintptr_t)arena_lo, E = A + arena_size;
         std::vector<uintptr_t> plo(parts, UINTPTR_MAX), phi(parts, 0);
-        std::vector<char> bad(parts, 0);
+        std::vector<char> bad(parts, 0), seq(parts, 1);
+        const uintptr_t s0 = (uintptr_t)strings[0];
         host_parts(n, parts, [&](size_t p, size_t b, size_t e) {
             uintptr_t lo = UINTPTR_MAX, hi = 0;
+            bool sq = true;  // strings[i] == strings[0] + i: every suffix of one text
             for (size_t i = b; i < e; ++i) {
                 const uintptr_t s = (uintptr_t)strings[i];
                 lo = std::min(lo, s);
                 hi = std::max(hi, s);
+                sq = sq && s == s0 + i;
             }
             plo[p] = lo;
             phi[p] = hi;
             bad[p] = lo < A || hi >= E;
+            seq[p] = sq;
         });
         uintptr_t lo = UINTPTR_MAX, hi = 0;
+        bool suffixes = true;
         for (size_t p = 0; p < parts; ++p) {
             if (bad[p]) return fail(PSSGPU_EINVAL, "a string pointer lies outside the arena");
             lo = std::min(lo, plo[p]);
             hi = std::max(hi, phi[p]);
+            suffixes = suffixes && seq[p];
+        }
+        if (suffixes && ((const uint8_t*)lo)[n - 1] == 0) {
+            // all suffixes of the text lo[0, n) (psstest --suffix): only the
+            // text crosses to the device, which makes the offsets itself, and
+            // the sorted pointers are lo + perm[i]
+            std::vector<uint32_t> perm(n), lcp32(lcp_out ? n : 0);
+            uint64_t nn = 0;
+            rc = sort_text_host_locked(c, (const uint8_t*)lo, n, PSSGPU_TEXT_SUFFIXES, perm.data(),
+                                       lcp_out ? lcp32.data() : nullptr, n, &nn);
+            if (rc) return rc;
+            if (nn != n) return fail(PSSGPU_ECUDA, "suffix count differs");
+            host_parts(n, parts, [&](size_t, size_t b, size_t e) {
+                for (size_t i = b; i < e; ++i) out[i] = (unsigned char*)(lo + perm[i]);
+                if (lcp_out)
+                    for (size_t i = std::max<size_t>(b, 1); i < e; ++i) lcp_out[i] = lcp32[i];
+                if (cache && lcp_out)
+                    for (size_t i = std::max<size_t>(b, 1); i < e; ++i) cache[i] = out[i][lcp_out[i]];
+            });
+            return PSSGPU_OK;
         }
         const size_t tail = strnlen((const char*)hi, E - hi);
         if (tail == E - hi) return fail(PSSGPU_EINVAL, "a string is not terminated inside the arena");
@@ -1372,32 +1433,7 @@ int pssgpu_sort_text_host(pssgpu_ctx* ctx, const uint8_t* text, uint64_t size, i
     if (!text || !perm) return fail(PSSGPU_EINVAL, "null buffer");
     Ctx* c = reinterpret_cast<Ctx*>(ctx);
     std::lock_guard<std::mutex> lk(c->mu);
-    PSS_CUDA(cudaSetDevice(c->device));
-    cudaStream_t st = c->stream;
-    const uint64_t b_text = align256(size + PSSGPU_ARENA_PAD);
-    int rc;
-    if ((rc = ensure_io(c, b_text))) return rc;
-    uint8_t* d_text = c->io;
-    PSS_CUDA(cudaMemcpyAsync(d_text, text, size, cudaMemcpyHostToDevice, st));
-    PSS_CUDA(cudaMemsetAsync(d_text + size, 0, b_text - size, st));
-    uint64_t n = 0;
-    if ((rc = text_count(c, d_text, size, mode, &n, st))) return rc;
-    *n_out = n;
-    if (n > cap) return fail(PSSGPU_EINVAL, "result arrays too small");
-    if ((rc = check_args(size, n))) return rc;
-    const uint64_t b_offs = align256(8 * n), b_perm = align256(4 * n);
-    const uint64_t b_lcp = lcp ? align256(4 * n) : 0;
-    if ((rc = ensure_buf(&c->io2, &c->io2_bytes, b_offs + b_perm + b_lcp))) return rc;
-    uint64_t* d_offs = (uint64_t*)c->io2;
-    uint32_t* d_perm = (uint32_t*)(c->io2 + b_offs);
-    uint32_t* d_lcp = lcp ? (uint32_t*)(c->io2 + b_offs + b_perm) : nullptr;
-    if ((rc = text_write(c, d_text, size, mode, d_offs, st))) return rc;
-    if ((rc = run_sort(c, d_text, size, d_offs, (uint32_t)n, d_perm, d_lcp, st))) return rc;
-    PSS_CUDA(cudaMemcpyAsync(perm, d_perm, 4 * n, cudaMemcpyDeviceToHost, st));
-    if (lcp && n > 1)
-        PSS_CUDA(cudaMemcpyAsync(lcp + 1, d_lcp + 1, 4 * (n - 1), cudaMemcpyDeviceToHost, st));
-    PSS_CUDA(cudaStreamSynchronize(st));
-    return PSSGPU_OK;
+    return sort_text_host_locked(c, text, size, mode, perm, lcp, cap, n_out);
 }
 
 int pssgpu_merge_lcp_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nchars,

@@ -334,7 +334,10 @@ def run_merge(args):
         ids[b:e] += b
     out = torch.empty_like(ids)
     out_lcp = torch.zeros_like(lcp)
-    stream = torch.cuda.current_stream()
+    # a stream of its own (not the legacy default stream, which the library
+    # reads as "the context's stream"): the merges and the events share it
+    stream = torch.cuda.Stream()
+    torch.cuda.synchronize()
     if args.merge_piece:
         ctx.set_option(ctx.OPT_MERGE_PIECE, args.merge_piece)
 
@@ -380,11 +383,13 @@ def run_batched(args, emit: bool = True) -> dict:
     ninst = len(inst) - 1
     ctx = pkg.Context(0)
     table = at.load_table()
-    stream = torch.cuda.current_stream()
+    # the sorts and the events on one stream of their own
+    stream = torch.cuda.Stream()
     dc = torch.from_numpy(h_chars).cuda()
     do = torch.from_numpy(h_offs.view(np.int64)).cuda()
     dp = torch.empty(n, dtype=torch.int32, device="cuda")
     dl = torch.empty(n, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
 
     def timed(fn, reps):
         ms = []
@@ -549,7 +554,10 @@ def main():
     flush = None if args.workload == "prefixes" else torch.empty(256 << 20, dtype=torch.uint8,
                                                                   device="cuda")
     ctx = pkg.Context(local)
-    stream = torch.cuda.current_stream()
+    # the sorts, the L2 flush and the timing events on one stream of their
+    # own (the legacy default stream reads as "the context's stream" in the
+    # library, which would put the sort on another stream than the events)
+    stream = torch.cuda.Stream(device=local)
     d_chars = torch.from_numpy(h_chars).cuda(non_blocking=True)
     d_offs = torch.from_numpy(h_offs.view(np.int64)).cuda(non_blocking=True)
     d_perm = torch.empty(n, dtype=torch.int32, device="cuda")
@@ -585,7 +593,8 @@ def main():
     else:
         tot = 0.0
         for _ in range(args.steps):
-            flush.zero_()
+            with torch.cuda.stream(stream):
+                flush.zero_()
             ev0.record(stream)
             step()
             ev1.record(stream)

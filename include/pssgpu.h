@@ -125,8 +125,10 @@ int pssgpu_ctx_set_option(pssgpu_ctx* ctx, int option, int64_t value);
  *
  * pssgpu_sort_device: device buffers on the context's device. d_chars must
  * be 8-byte aligned and readable for nchars + PSSGPU_ARENA_PAD bytes;
- * `stream` is a cudaStream_t or NULL for the context's stream. The call
- * returns after the sort has completed. */
+ * `stream` is a cudaStream_t or NULL for the context's stream, which orders
+ * with the legacy default stream (work the caller queued there before the
+ * call is done before the sort starts). The call returns after the sort has
+ * completed. */
 int pssgpu_sort_host(pssgpu_ctx* ctx, const uint8_t* chars, uint64_t nchars,
                      const uint64_t* offs, uint64_t n, uint32_t* perm,
                      uint32_t* lcp);

@@ -747,7 +747,9 @@ static int ctx_create(int device, Ctx** out)
     Ctx* c = new Ctx;
     c->trace = std::getenv("PSSGPU_TRACE") != nullptr;
     c->device = device;
-    bool ok = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) == cudaSuccess &&
+    // the context's stream orders with the legacy default stream (a blocking
+    // stream), so a call without a stream sees the caller's earlier work there
+    bool ok = cudaStreamCreateWithFlags(&c->stream, cudaStreamDefault) == cudaSuccess &&
               cudaEventCreate(&c->ev0) == cudaSuccess && cudaEventCreate(&c->ev1) == cudaSuccess &&
               cudaHostAlloc((void**)&c->host_counters, 4 * C_COUNT, cudaHostAllocDefault) ==
                   cudaSuccess;

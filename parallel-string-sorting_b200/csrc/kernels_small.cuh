@@ -232,6 +232,46 @@ __device__ __forceinline__ void for_each_window(uint32_t ngroups, SizeFn sizes, 
     }
 }
 
+// A warp's list entries L[0, ng) (ng <= 32, every entry at most 32 strings)
+// packed greedily into windows of at most 32 strings. The entries are loaded
+// once, one per lane, and read through shuffles. fn(s, gq, gs, real) runs
+// once per window on every lane: s is the lane's entry, gq its index inside
+// the window, gs the entry's first lane, real whether the lane holds a string.
+template <typename Fn>
+__device__ __forceinline__ void warp_seg_windows(const Seg* __restrict__ L, uint32_t ng, Fn fn)
+{
+    const uint32_t lane = threadIdx.x & 31;
+    Seg mine{};
+    if (lane < ng) mine = L[lane];
+    uint32_t j = 0;
+    while (j < ng) {
+        uint32_t used = 0, e = j;
+        while (e < ng) {
+            const uint32_t sz = __shfl_sync(0xffffffffu, mine.size, e);
+            if (used + sz > 32u) break;
+            used += sz;
+            ++e;
+        }
+        if (e == j) ++e;  // no entry is larger than a window; never stall
+        uint32_t off = 0, gs = 32, gq = 31;
+        Seg sg{};
+        for (uint32_t q = j; q < e; ++q) {
+            const uint32_t b = __shfl_sync(0xffffffffu, mine.begin, q);
+            const uint32_t sz = __shfl_sync(0xffffffffu, mine.size, q);
+            const uint32_t d = __shfl_sync(0xffffffffu, mine.depth, q);
+            const uint32_t m = __shfl_sync(0xffffffffu, mine.meta, q);
+            if (lane >= off && lane < off + sz) {
+                sg = Seg{b, sz, d, m};
+                gs = off;
+                gq = q - j;
+            }
+            off += sz;
+        }
+        fn(sg, gq, gs, gs < 32u && lane < 32u);
+        j = e;
+    }
+}
+
 // Segments of at most 32 strings: each warp takes TINY_PER_WARP consecutive
 // list entries and packs them into warp windows.
 constexpr int TINY_WARPS = 8;
@@ -243,19 +283,10 @@ __global__ void __launch_bounds__(32 * TINY_WARPS, 5) k_tiny(Work w, const Seg* 
     const uint32_t g0 = (blockIdx.x * TINY_WARPS + (threadIdx.x >> 5)) * TINY_PER_WARP;
     if (g0 >= count) return;  // whole warp
     const uint32_t ng = min((uint32_t)TINY_PER_WARP, count - g0);
-    const Seg* L = list + g0;
-    for_each_window(ng, [&](uint32_t j) { return L[j].size; }, [&](uint32_t j0, uint32_t cnt) {
-        // lane -> (segment, index inside it)
-        uint32_t off = 0, mygrp = 32, idx = 0;
-        Seg sg{};
-        for (uint32_t q = 0; q < cnt; ++q) {
-            const Seg s = L[j0 + q];
-            if (lane >= off && lane < off + s.size) { sg = s; mygrp = off; idx = lane - off; }
-            off += s.size;
-        }
-        const bool real = mygrp < 32;
+    warp_seg_windows(list + g0, ng, [&](const Seg& sg, uint32_t, uint32_t gs, bool real) {
+        const uint32_t mygrp = real ? gs : 32u;
         const int buf = sg.meta & META_BUF;
-        const uint32_t pos = sg.begin + idx;
+        const uint32_t pos = sg.begin + (lane - gs);
         const uint64_t h = real ? w.hnd[buf][pos] : ~0ull;
         const bool hk = real && (sg.meta & META_VALID);
         const uint64_t k0 = hk ? w.keys[buf][pos] : 0ull;

@@ -63,21 +63,19 @@ __global__ void k_suffix_check(const uint8_t* __restrict__ chars, const uint64_t
 }
 
 // Members of the groups the string passes handed over: their ids into perm
-// (the handles sit in the group's ping-pong buffer).
-__global__ void k_dbl_init(Work w, const Seg* __restrict__ list, uint32_t count)
-{
-    for (uint32_t g = blockIdx.x; g < count; g += gridDim.x) {
-        const Seg s = list[g];
-        const uint64_t* hs = w.hnd[s.meta & META_BUF];
-        for (uint32_t q = threadIdx.x; q < s.size; q += blockDim.x)
-            w.perm[s.begin + q] = h_id(w, hs[s.begin + q]);
-    }
-}
+// (the handles sit in the group's ping-pong buffer), their rank (the group
+// start) into isa, a mark in `taken`; the group's depth into gd[0]. The
+// groups are sorted into the round lists of parity 0 (dbl_push, below).
+__global__ void k_dbl_init(Work w, const Seg* __restrict__ list, uint32_t count, DblArrays a,
+                           uint8_t* __restrict__ taken, uint32_t* counters);
 
-__global__ void k_dbl_isa(const uint32_t* __restrict__ perm, uint32_t n, uint32_t* __restrict__ isa)
+// Every other position (not in a handed-over group) is final: its suffix's
+// rank is the position.
+__global__ void k_dbl_isa(const uint32_t* __restrict__ perm, uint32_t n,
+                          const uint8_t* __restrict__ taken, uint32_t* __restrict__ isa)
 {
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
-        isa[perm[p]] = p;
+        if (!taken[p]) isa[perm[p]] = p;
 }
 
 __device__ __forceinline__ void dbl_push(DblArrays& a, uint32_t* counters, int par, Seg s)
@@ -88,14 +86,18 @@ __device__ __forceinline__ void dbl_push(DblArrays& a, uint32_t* counters, int p
     else set_error(counters + C_ERR, ERR_OVERFLOW);
 }
 
-// Handed-over groups: every member's rank is the group start, the group's
-// depth goes to gd[0]; the groups are sorted into the round lists of parity 0.
-__global__ void k_dbl_rank(const uint32_t* __restrict__ perm, const Seg* __restrict__ list,
-                           uint32_t count, DblArrays a, uint32_t* counters)
+__global__ void k_dbl_init(Work w, const Seg* __restrict__ list, uint32_t count, DblArrays a,
+                           uint8_t* __restrict__ taken, uint32_t* counters)
 {
     for (uint32_t g = blockIdx.x; g < count; g += gridDim.x) {
         const Seg s = list[g];
-        for (uint32_t q = threadIdx.x; q < s.size; q += blockDim.x) a.isa[perm[s.begin + q]] = s.begin;
+        const uint64_t* hs = w.hnd[s.meta & META_BUF];
+        for (uint32_t q = threadIdx.x; q < s.size; q += blockDim.x) {
+            const uint32_t x = h_id(w, hs[s.begin + q]);
+            w.perm[s.begin + q] = x;
+            a.isa[x] = s.begin;
+            taken[s.begin + q] = 1;
+        }
         if (threadIdx.x == 0) {
             a.gd[0][s.begin] = s.depth;
             dbl_push(a, counters, 0, Seg{s.begin, s.size, s.depth, 0u});
@@ -177,21 +179,7 @@ __global__ void k_dbl_sort_small(const Seg* __restrict__ list, uint32_t count,
     const uint32_t g0 = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * DBL_PER_WARP;
     if (g0 >= count) return;  // whole warp
     const uint32_t ng = min(DBL_PER_WARP, count - g0);
-    const Seg* L = list + g0;
-    for_each_window(ng, [&](uint32_t j) { return L[j].size; }, [&](uint32_t j0, uint32_t cnt) {
-        // lane -> (group q of the window, member); gs = the group's first lane
-        uint32_t off = 0, gq = 31, gs = 32;
-        Seg s{};
-        for (uint32_t q = 0; q < cnt; ++q) {
-            const Seg t = L[j0 + q];
-            if (lane >= off && lane < off + t.size) {
-                gq = q;
-                gs = off;
-                s = t;
-            }
-            off += t.size;
-        }
-        const bool real = gs < 32;
+    warp_seg_windows(list + g0, ng, [&](const Seg& s, uint32_t gq, uint32_t gs, bool real) {
         const uint32_t mem = real ? lane - gs : 0u;
         const uint32_t x = real ? perm[s.begin + mem] : 0u;
         uint64_t t = real ? ((uint64_t)gq << 58) | ((uint64_t)a.key[s.begin + mem] << 5) | lane : ~0ull;

@@ -129,6 +129,27 @@ __global__ void k_merge_seq(const uint8_t* __restrict__ chars, uint64_t nchars,
     }
 }
 
+// Sequential reads of a u32 array 16 bytes at a time: a thread that walks
+// its own stretch of ids or LCPs keeps the last aligned 4-word block in
+// registers instead of fetching a sector per word (the threads' streams are
+// too many for the caches to keep their lines). The array must be 16-byte
+// aligned and readable up to the next multiple of 4 words past its end.
+struct SeqRead4 {
+    const uint32_t* base;
+    uint64_t blk = ~0ull;
+    uint4 v{};
+    __device__ __forceinline__ uint32_t get(uint64_t i)
+    {
+        const uint64_t b = i >> 2;
+        if (b != blk) {
+            v = __ldg(reinterpret_cast<const uint4*>(base + (b << 2)));
+            blk = b;
+        }
+        const uint32_t k = (uint32_t)(i & 3);
+        return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w;
+    }
+};
+
 // LCP-aware piece merge (the reference's LCP loser-tree rule for two runs).
 // Runs A = ids_in[a0, a1) and B = ids_in[a1, b1) with their LCP arrays in
 // lcp_in (entries at a run's first position are not read). ha / hb are the
@@ -190,8 +211,10 @@ __global__ void k_merge_lcp_seq(const uint8_t* __restrict__ chars, uint64_t ncha
             }
         }
         // the heads' ids and arena offsets stay in registers: one offset
-        // load per output, and a compare reads chars only
-        uint32_t ida = i < i1 ? A[i] : 0u, idb = j < j1 ? B[j] : 0u;
+        // load per output, and a compare reads chars only; the runs' ids and
+        // LCPs are read 16 bytes at a time
+        SeqRead4 ra{ids_in}, rb{ids_in}, la{lcp_in}, lb{lcp_in};
+        uint32_t ida = i < i1 ? ra.get(pr.a0 + i) : 0u, idb = j < j1 ? rb.get(pr.a1 + j) : 0u;
         uint64_t oa = i < i1 ? __ldg(offs + ida) : 0ull, ob = j < j1 ? __ldg(offs + idb) : 0ull;
         for (uint64_t d = d0; d < d1; ++d) {
             bool take_a;
@@ -207,16 +230,16 @@ __global__ void k_merge_lcp_seq(const uint8_t* __restrict__ chars, uint64_t ncha
             if (lcp_out && d > 0) lcp_out[pr.a0 + d] = take_a ? ha : hb;
             if (take_a) {
                 ++i;
-                ha = i < na ? LA[i] : 0u;  // against its predecessor, the last output
+                ha = i < na ? la.get(pr.a0 + i) : 0u;  // against its predecessor, the last output
                 if (i < i1) {
-                    ida = A[i];
+                    ida = ra.get(pr.a0 + i);
                     oa = __ldg(offs + ida);
                 }
             } else {
                 ++j;
-                hb = j < nb ? LB[j] : 0u;
+                hb = j < nb ? lb.get(pr.a1 + j) : 0u;
                 if (j < j1) {
-                    idb = B[j];
+                    idb = rb.get(pr.a1 + j);
                     ob = __ldg(offs + idb);
                 }
             }

@@ -376,13 +376,16 @@ static int run_doubling(Ctx* c, Work& w, uint32_t ndbl, cudaStream_t st, pssgpu_
     }
     uint32_t* hc = c->host_counters;
     const unsigned gblocks = std::min<uint32_t>(ndbl, 148u * 16u);
+    // marks of the handed-over positions, in the round-key array (free
+    // until the first round)
+    uint8_t* taken = reinterpret_cast<uint8_t*>(a.key);
     PSS_CUDA(cudaMemsetAsync(w.counters + C_DBL_CNT, 0, 4 * 6, st));
-    k_dbl_init<<<gblocks, 256, 0, st>>>(w, w.dbl, ndbl);
+    PSS_CUDA(cudaMemsetAsync(taken, 0, n, st));
+    k_dbl_init<<<gblocks, 256, 0, st>>>(w, w.dbl, ndbl, a, taken, w.counters);
     if (a.lb) PSS_CUDA(cudaMemsetAsync(a.lb, 0xFF, 4ull * n, st));
-    k_dbl_isa<<<1184, 256, 0, st>>>(w.perm, n, a.isa);
-    k_dbl_rank<<<gblocks, 256, 0, st>>>(w.perm, w.dbl, ndbl, a, w.counters);
-    stats.kernel_launches += 3;
-    c->kstat[K_DBL].launches += 3;
+    k_dbl_isa<<<1184, 256, 0, st>>>(w.perm, n, taken, a.isa);
+    stats.kernel_launches += 2;
+    c->kstat[K_DBL].launches += 2;
     c->kstat[K_DBL].strings += n;
     PSS_CUDA(cudaGetLastError());
     PSS_CUDA(cudaMemcpyAsync(hc, w.counters, 4 * C_COUNT, cudaMemcpyDeviceToHost, st));
@@ -1520,10 +1523,19 @@ int pssgpu_merge_lcp_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nc
     const unsigned blocks = (unsigned)std::min<uint64_t>((n + 255) / 256, 148ull * 16);
     k_merge_check<<<blocks, 256, 0, st>>>(d_offs, nchars, d_ids, n, d_err);
     // with the runs' LCP arrays every round is LCP-aware and carries the
-    // merged LCP array to the next one (the last round writes d_lcp_out, if any)
+    // merged LCP array to the next one (the last round writes d_lcp_out, if
+    // any). Its sequential reads take 16 bytes at a time, from the library's
+    // own buffers (aligned, padded): the caller's ids and LCPs are copied in.
     const bool with_lcp = d_lcp != nullptr;
     const uint32_t* in_ids = d_ids;
     const uint32_t* in_lcp = d_lcp;
+    if (with_lcp) {
+        // round 0 writes tid[0], so the copies go to the other buffers
+        PSS_CUDA(cudaMemcpyAsync(tid[1], d_ids, 4 * n, cudaMemcpyDeviceToDevice, st));
+        PSS_CUDA(cudaMemcpyAsync(tlcp[1], d_lcp, 4 * n, cudaMemcpyDeviceToDevice, st));
+        in_ids = tid[1];
+        in_lcp = tlcp[1];
+    }
     for (size_t i = 0; i < rounds; ++i) {
         const bool lastr = i + 1 == rounds;
         uint32_t* out_ids = lastr ? d_ids_out : tid[i & 1];

@@ -86,9 +86,26 @@ __device__ __forceinline__ void dbl_push(DblArrays& a, uint32_t* counters, int p
     else set_error(counters + C_ERR, ERR_OVERFLOW);
 }
 
+// The list appends of a block are staged in shared memory, DBL_INIT_STAGE
+// per class, and reserved with one global atomic per full stage (a global
+// atomic per group serialises on the three list counters).
+constexpr uint32_t DBL_INIT_STAGE = 64;
 __global__ void k_dbl_init(Work w, const Seg* __restrict__ list, uint32_t count, DblArrays a,
                            uint8_t* __restrict__ taken, uint32_t* counters)
 {
+    __shared__ Seg stage[3][DBL_INIT_STAGE];
+    __shared__ uint32_t staged[3];
+    if (threadIdx.x == 0) staged[0] = staged[1] = staged[2] = 0;  // thread 0 alone uses them
+    auto flush = [&](int c) {  // thread 0
+        const uint32_t m = staged[c];
+        if (!m) return;
+        const uint32_t base = atomicAdd(counters + C_DBL_CNT + c, m);  // parity 0
+        for (uint32_t q = 0; q < m; ++q) {
+            if (base + q < a.cap[c]) a.list[c][0][base + q] = stage[c][q];
+            else set_error(counters + C_ERR, ERR_OVERFLOW);
+        }
+        staged[c] = 0;
+    };
     for (uint32_t g = blockIdx.x; g < count; g += gridDim.x) {
         const Seg s = list[g];
         const uint64_t* hs = w.hnd[s.meta & META_BUF];
@@ -100,9 +117,13 @@ __global__ void k_dbl_init(Work w, const Seg* __restrict__ list, uint32_t count,
         }
         if (threadIdx.x == 0) {
             a.gd[0][s.begin] = s.depth;
-            dbl_push(a, counters, 0, Seg{s.begin, s.size, s.depth, 0u});
+            const int c = dbl_class(s.size);
+            stage[c][staged[c]++] = Seg{s.begin, s.size, s.depth, 0u};
+            if (staged[c] == DBL_INIT_STAGE) flush(c);
         }
     }
+    if (threadIdx.x == 0)
+        for (int c = 0; c < 3; ++c) flush(c);
 }
 
 // Warp-aggregated append to the round lists: every lane of the warp calls;

@@ -51,7 +51,7 @@ __device__ __forceinline__ int compare_lcp(const uint8_t* chars, uint64_t nchars
 // piece how many left-run strings precede it (a binary search along the
 // piece's diagonal), k_merge_lcp_seq (or k_merge_seq without LCP arrays)
 // merges each piece sequentially from there.
-constexpr uint32_t MERGE_PIECE = 32;
+constexpr uint32_t MERGE_PIECE = 128;
 constexpr uint32_t MERGE_PIECE_MAX = 4096;
 
 struct MergePair {

@@ -104,6 +104,15 @@ __device__ __forceinline__ void hold_loaded(uint32_t (&v)[N])
                      "+r"(v[i + 5]), "+r"(v[i + 6]), "+r"(v[i + 7])::"memory");
 }
 
+template <int N>
+__device__ __forceinline__ void hold_loaded64(uint64_t (&v)[N])
+{
+    static_assert(N % 4 == 0, "multiple of 4");
+#pragma unroll
+    for (int i = 0; i < N; i += 4)
+        asm volatile("" : "+l"(v[i]), "+l"(v[i + 1]), "+l"(v[i + 2]), "+l"(v[i + 3])::"memory");
+}
+
 // Bitonic stages (kk, j) with j <= 32 for kk in [kk_from, kk_to], on every
 // 64-key chunk of a[0, S) in registers: each warp takes whole chunks, two
 // keys per lane (positions e0 = 64 c + 2 lane and e0 + 1), partners by

@@ -459,11 +459,17 @@ struct ScatterSmem {
 
 // One block per tile: rank every string inside its bucket, stage the tile in
 // bucket order in shared memory, write bucket runs contiguously from the
-// tile's destinations (k_tile_offsets).
-__global__ void __launch_bounds__(TILE_THREADS) k_scatter(Work w, uint32_t nbig)
+// tile's destinations (k_tile_offsets). Global loads are issued a phase
+// ahead of their use: the bucket ids, the destination row and half of the
+// keys together; the other half of the keys before the bucket scan; all
+// handles before the keys are written out. Each thread's slots are packed
+// two to a register while the handles are held.
+__global__ void __launch_bounds__(TILE_THREADS, 2) k_scatter(Work w, uint32_t nbig)
 {
     constexpr int PER = TILE / TILE_THREADS;
+    constexpr int HALF = PER / 2;
     constexpr int NBT = (MAX_BKT + TILE_THREADS - 1) / TILE_THREADS;
+    static_assert(TILE <= 0xFFFF, "slots and ranks take 16 bits");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ScatterSmem& sm = *reinterpret_cast<ScatterSmem*>(smem_raw);
     const uint32_t t = blockIdx.x;
@@ -476,7 +482,8 @@ __global__ void __launch_bounds__(TILE_THREADS) k_scatter(Work w, uint32_t nbig)
     const uint32_t cnt = hi - lo;
     const uint32_t B = seg_buckets(w, s);
     const int buf = sg.meta & META_BUF;
-    // this tile's first destination per bucket, loaded early
+    const uint64_t* ikeys = w.keys[buf];
+    const uint64_t* ihs = w.hnd[buf];
     const uint32_t* dst = w.tcount + (size_t)t * MAX_BKT;
     uint32_t first[NBT];
 #pragma unroll
@@ -484,44 +491,46 @@ __global__ void __launch_bounds__(TILE_THREADS) k_scatter(Work w, uint32_t nbig)
         const uint32_t b = threadIdx.x + i * TILE_THREADS;
         first[i] = b < B ? dst[b] : 0u;
     }
-    for (uint32_t b = threadIdx.x; b < B; b += TILE_THREADS) sm.lcount[b] = 0;
-    __syncthreads();
-    // rank of every string inside its bucket in this tile: (bucket << 16) | rank
     uint32_t pk[PER];
 #pragma unroll
     for (int j = 0; j < PER; ++j) {
         const uint32_t p = lo + threadIdx.x + j * TILE_THREADS;
-        pk[j] = 0xFFFFFFFFu;
-        if (p < hi) {
-            const uint32_t b = __ldg(w.bkt + p);
-            pk[j] = (b << 16) | atomicAdd(&sm.lcount[b], 1u);
-        }
+        pk[j] = p < hi ? (uint32_t)__ldg(w.bkt + p) : 0xFFFFFFFFu;
+    }
+    uint64_t v[PER];
+#pragma unroll
+    for (int j = 0; j < HALF; ++j) {
+        const uint32_t p = lo + threadIdx.x + j * TILE_THREADS;
+        v[j] = p < hi ? __ldg(ikeys + p) : 0ull;
+    }
+    for (uint32_t b = threadIdx.x; b < B; b += TILE_THREADS) sm.lcount[b] = 0;
+    __syncthreads();
+    // rank of every string inside its bucket in this tile: (bucket << 16) | rank
+#pragma unroll
+    for (int j = 0; j < PER; ++j)
+        if (pk[j] != 0xFFFFFFFFu) pk[j] = (pk[j] << 16) | atomicAdd(&sm.lcount[pk[j]], 1u);
+#pragma unroll
+    for (int j = HALF; j < PER; ++j) {
+        const uint32_t p = lo + threadIdx.x + j * TILE_THREADS;
+        v[j] = p < hi ? __ldg(ikeys + p) : 0ull;
     }
     __syncthreads();
     block_scan_array<TILE_THREADS>(sm.lcount, (int)B, sm.tmp);  // counts -> first slots
-    // stage keys in bucket order; pk becomes (bucket << 16) | slot. The
-    // loads of half the thread's elements are issued together (read-only
-    // loads, held in registers) before their shared-memory stores.
-    const uint64_t* ikeys = w.keys[buf];
+    // stage keys in bucket order; slots packed two to a register
+    uint32_t ps[HALF];
 #pragma unroll
-    for (int j = 0; j < PER; ++j) {
-        if (pk[j] == 0xFFFFFFFFu) continue;
-        const uint32_t b = pk[j] >> 16;
-        pk[j] = (b << 16) | (sm.lcount[b] + (pk[j] & 0xFFFFu));
-    }
+    for (int j = 0; j < PER; j += 2) {
+        uint32_t pair = 0xFFFFFFFFu;
 #pragma unroll
-    for (int h = 0; h < PER; h += PER / 2) {
-        uint64_t v[PER / 2];
-#pragma unroll
-        for (int j = 0; j < PER / 2; ++j)
-            v[j] = pk[h + j] != 0xFFFFFFFFu ? __ldg(ikeys + lo + threadIdx.x + (h + j) * TILE_THREADS) : 0ull;
-#pragma unroll
-        for (int j = 0; j < PER / 2; ++j) {
-            if (pk[h + j] == 0xFFFFFFFFu) continue;
-            const uint32_t slot = pk[h + j] & 0xFFFFu;
-            sm.stage[slot] = v[j];
-            sm.sbkt[slot] = (uint16_t)(pk[h + j] >> 16);
+        for (int q = 0; q < 2; ++q) {
+            if (pk[j + q] == 0xFFFFFFFFu) continue;
+            const uint32_t b = pk[j + q] >> 16;
+            const uint32_t slot = sm.lcount[b] + (pk[j + q] & 0xFFFFu);
+            sm.stage[slot] = v[j + q];
+            sm.sbkt[slot] = (uint16_t)b;
+            pair = q ? ((pair & 0xFFFFu) | (slot << 16)) : ((pair & 0xFFFF0000u) | slot);
         }
+        ps[j / 2] = pair;
     }
     __syncthreads();
 #pragma unroll
@@ -529,6 +538,13 @@ __global__ void __launch_bounds__(TILE_THREADS) k_scatter(Work w, uint32_t nbig)
         const uint32_t b = threadIdx.x + i * TILE_THREADS;
         if (b < B) sm.lcount[b] = first[i] - sm.lcount[b];
     }
+    // the handles, in flight while the keys go out
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+        const uint32_t p = lo + threadIdx.x + j * TILE_THREADS;
+        v[j] = p < hi ? __ldg(ihs + p) : 0ull;
+    }
+    hold_loaded64(v);
     __syncthreads();
     // write bucket runs contiguously: keys, then handles
     uint64_t* okeys = w.keys[buf ^ 1];
@@ -541,16 +557,10 @@ __global__ void __launch_bounds__(TILE_THREADS) k_scatter(Work w, uint32_t nbig)
         okeys[dest] = sm.stage[slot];
     }
     __syncthreads();
-    const uint64_t* ihs = w.hnd[buf];
 #pragma unroll
-    for (int h = 0; h < PER; h += PER / 2) {
-        uint64_t v[PER / 2];
-#pragma unroll
-        for (int j = 0; j < PER / 2; ++j)
-            v[j] = pk[h + j] != 0xFFFFFFFFu ? __ldg(ihs + lo + threadIdx.x + (h + j) * TILE_THREADS) : 0ull;
-#pragma unroll
-        for (int j = 0; j < PER / 2; ++j)
-            if (pk[h + j] != 0xFFFFFFFFu) sm.stage[pk[h + j] & 0xFFFFu] = v[j];
+    for (int j = 0; j < PER; ++j) {
+        const uint32_t slot = (ps[j / 2] >> (16 * (j & 1))) & 0xFFFFu;
+        if (slot != 0xFFFFu) sm.stage[slot] = v[j];
     }
     __syncthreads();
     uint64_t* ohs = w.hnd[buf ^ 1];

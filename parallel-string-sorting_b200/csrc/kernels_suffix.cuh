@@ -154,20 +154,24 @@ __device__ __forceinline__ void dbl_push_warp(DblArrays& a, uint32_t* counters, 
 // k_dbl_keys_small: one thread per group of at most 32; k_dbl_keys: one warp
 // per larger group.
 __global__ void k_dbl_keys_small(const Seg* __restrict__ list, uint32_t count,
-                                 const uint32_t* __restrict__ perm, DblArrays a)
+                                 const uint32_t* __restrict__ perm, DblArrays a,
+                                 unsigned long long* members)
 {
     const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= count) return;
-    const Seg s = list[g];
+    const Seg s = g < count ? list[g] : Seg{0u, 0u, 0u, 0u};
+    const uint32_t m = __reduce_add_sync(0xFFFFFFFFu, s.size);
+    if ((threadIdx.x & 31) == 0 && m) atomicAdd(members, (unsigned long long)m);
     for (uint32_t q = 0; q < s.size; ++q) a.key[s.begin + q] = a.isa[perm[s.begin + q] + s.depth];
 }
 
 __global__ void k_dbl_keys(const Seg* __restrict__ list, uint32_t count,
-                           const uint32_t* __restrict__ perm, DblArrays a)
+                           const uint32_t* __restrict__ perm, DblArrays a,
+                           unsigned long long* members)
 {
     const uint32_t g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (g >= count) return;
     const Seg s = list[g];
+    if ((threadIdx.x & 31) == 0) atomicAdd(members, (unsigned long long)s.size);
     for (uint32_t q = threadIdx.x & 31; q < s.size; q += 32)
         a.key[s.begin + q] = a.isa[perm[s.begin + q] + s.depth];
 }

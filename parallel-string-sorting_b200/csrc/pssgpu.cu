@@ -379,7 +379,8 @@ static int run_doubling(Ctx* c, Work& w, uint32_t ndbl, cudaStream_t st, pssgpu_
     // marks of the handed-over positions, in the round-key array (free
     // until the first round)
     uint8_t* taken = reinterpret_cast<uint8_t*>(a.key);
-    PSS_CUDA(cudaMemsetAsync(w.counters + C_DBL_CNT, 0, 4 * 6, st));
+    auto* members = reinterpret_cast<unsigned long long*>(w.counters + C_DBL_MEMB);
+    PSS_CUDA(cudaMemsetAsync(w.counters + C_DBL_CNT, 0, 4 * (C_COUNT - C_DBL_CNT), st));
     PSS_CUDA(cudaMemsetAsync(taken, 0, n, st));
     k_dbl_init<<<gblocks, 256, 0, st>>>(w, w.dbl, ndbl, a, taken, w.counters);
     if (a.lb) PSS_CUDA(cudaMemsetAsync(a.lb, 0xFF, 4ull * n, st));
@@ -400,9 +401,11 @@ static int run_doubling(Ctx* c, Work& w, uint32_t ndbl, cudaStream_t st, pssgpu_
         if (!cnt[0] && !cnt[1] && !cnt[2]) break;
         if (round >= MAX_ROUNDS) return fail(PSSGPU_ETIMEOUT, "rank doubling round limit exceeded");
         PSS_CUDA(cudaMemsetAsync(w.counters + C_DBL_CNT + 3 * (par ^ 1), 0, 12, st));
-        if (cnt[0]) k_dbl_keys_small<<<(cnt[0] + 255) / 256, 256, 0, st>>>(a.list[0][par], cnt[0], w.perm, a);
+        if (cnt[0])
+            k_dbl_keys_small<<<(cnt[0] + 255) / 256, 256, 0, st>>>(a.list[0][par], cnt[0], w.perm, a, members);
         for (int k = 1; k < 3; ++k)
-            if (cnt[k]) k_dbl_keys<<<(cnt[k] + 7) / 8, 256, 0, st>>>(a.list[k][par], cnt[k], w.perm, a);
+            if (cnt[k])
+                k_dbl_keys<<<(cnt[k] + 7) / 8, 256, 0, st>>>(a.list[k][par], cnt[k], w.perm, a, members);
         if (cnt[0]) {
             constexpr uint32_t per_block = 8 * DBL_PER_WARP;  // 8 warps
             k_dbl_sort_small<<<(cnt[0] + per_block - 1) / per_block, 256, 0, st>>>(
@@ -426,6 +429,11 @@ static int run_doubling(Ctx* c, Work& w, uint32_t ndbl, cudaStream_t st, pssgpu_
         par ^= 1;
     }
     *err = hc[C_ERR];
+    // algorithmic bytes: every suffix's first rank (its position read, its
+    // rank written), then per group member and round its id and the rank
+    // `depth` chars further read, its id and new rank written
+    const uint64_t memb = (uint64_t)hc[C_DBL_MEMB] | ((uint64_t)hc[C_DBL_MEMB + 1] << 32);
+    c->kstat[K_DBL].alg_bytes += 8ull * n + 16ull * memb;
     if (!*err && a.lb) {
         const uint64_t nchunk = ((uint64_t)n + DBL_LCP_CHUNK - 1) / DBL_LCP_CHUNK;
         k_dbl_lcp<<<(unsigned)std::min<uint64_t>((nchunk + 255) / 256, 148ull * 16), 256, 0, st>>>(

@@ -43,6 +43,7 @@ enum : int {
     C_SFX = 30,       // suffix-set check: nonzero when the input is not all suffixes of a text
     C_DBL = 31,       // groups handed to rank doubling by the passes
     C_DBL_CNT = 32,   // + 3 * parity + class: rank-doubling round lists
+    C_DBL_MEMB = 38,  // 64-bit (38, 39): members of the rank-doubling groups, summed over rounds
     C_COUNT = 40
 };
 

@@ -63,29 +63,54 @@ __device__ __forceinline__ uint64_t load_key(const uint8_t* __restrict__ chars,
 }
 
 // The raw little-endian 8-char windows at p, p + 8, ... (cnt <= NB of them)
-// into raw[0, cnt): cnt + 1 aligned word loads instead of two per window.
-// Chars at or beyond nchars read as 0; raw[cnt, NB) are left 0. A window
+// into raw[0, cnt); raw[cnt, NB) are left 0 and chars at or beyond nchars
+// read as 0. The words come from 16-byte loads at the 16-byte boundary at or
+// below chars + p (an absolute address, so the arena needs no more than its
+// 8-byte alignment): every vector lies in a 16-byte block that holds a char
+// of the arena or of its padding, and at most ceil((NB + 2) / 2) are read,
+// where byte-wise 8-byte loads would take NB + 1 (a string's loads are one
+// L1 request per lane each, which bounds the common-prefix pass). A window
 // becomes load_key's value through finish_key.
 template <int NB>
 __device__ __forceinline__ void load_raw_chunks(const uint8_t* __restrict__ chars, uint64_t nchars,
                                                 uint64_t p, uint32_t cnt, uint64_t* raw)
 {
-    const uint64_t a = p & ~7ull;
-    const unsigned sh = (unsigned)(p & 7) * 8u;
-    uint64_t wd[NB + 1];
+    constexpr int NV = (NB + 3) / 2;
+    const uintptr_t ab = reinterpret_cast<uintptr_t>(chars + p);
+    const uintptr_t a16 = ab & ~(uintptr_t)15;
+    const unsigned off = (unsigned)(ab - a16);  // 0..15
+    const unsigned sh = (off & 7u) * 8u;
+    const bool upper = off >= 8;                // the first window starts in the upper word
+    const unsigned need = 8u * ((off >> 3) + cnt + 1);  // bytes of words used, from a16
+    const int64_t base = (int64_t)(a16 - reinterpret_cast<uintptr_t>(chars));
+    uint64_t wd[2 * NV];
 #pragma unroll
-    for (int i = 0; i <= NB; ++i) {
-        const uint64_t ai = a + 8ull * i;
-        uint64_t v = 0;
-        if ((uint32_t)i <= cnt && ai < nchars) {
-            v = __ldg(reinterpret_cast<const uint64_t*>(chars + ai));
-            if (ai + 8 > nchars) v &= ~0ull >> (64u - 8u * (unsigned)(nchars - ai));
+    for (int i = 0; i < NV; ++i) {
+        const int64_t r = base + 16 * i;  // arena position of the vector's first byte
+        uint64_t x = 0, y = 0;
+        if ((unsigned)(16 * i) < need && r < (int64_t)nchars) {
+            const ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(a16 + 16 * i));
+            x = v.x;
+            y = v.y;
+            const int64_t left = (int64_t)nchars - r;  // its bytes inside the arena
+            if (left < 16) {
+                if (left <= 8) {
+                    x &= ~0ull >> (64u - 8u * (unsigned)left);
+                    y = 0;
+                } else {
+                    y &= ~0ull >> (64u - 8u * (unsigned)(left - 8));
+                }
+            }
         }
-        wd[i] = v;
+        wd[2 * i] = x;
+        wd[2 * i + 1] = y;
     }
 #pragma unroll
-    for (int i = 0; i < NB; ++i)
-        raw[i] = (uint32_t)i < cnt ? (sh ? ((wd[i] >> sh) | (wd[i + 1] << (64u - sh))) : wd[i]) : 0ull;
+    for (int i = 0; i < NB; ++i) {
+        const uint64_t lo = upper ? wd[i + 1] : wd[i];
+        const uint64_t hi = upper ? wd[i + 2] : wd[i + 1];
+        raw[i] = (uint32_t)i < cnt ? (sh ? ((lo >> sh) | (hi << (64u - sh))) : lo) : 0ull;
+    }
 }
 
 // Big-endian key of a raw window: chars after its first NUL read as NUL.

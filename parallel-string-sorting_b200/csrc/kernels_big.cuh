@@ -98,7 +98,11 @@ __global__ void __launch_bounds__(1024) k_sample(Work w)
     }
     const uint32_t L = tree_bits_for(w, sg.size);
     const uint32_t k = (1u << L) - 1;
-    const uint32_t S = 2u << L;  // oversampling factor 2 (hpp:1388)
+    // one sample per bucket slot: 2^L sorted samples, the splitters are all
+    // but the first. pS5 oversamples by 2 (hpp:1388); here half the
+    // samples halve the bitonic sort, which is most of this kernel's work,
+    // while '<' buckets still hold about 8 strings on average
+    const uint32_t S = 1u << L;
     const int buf = sg.meta & META_BUF;
     const bool valid = sg.meta & META_VALID;
     // handles (and cached keys) of the samples, then the keys of stale ones:
@@ -194,15 +198,15 @@ __global__ void __launch_bounds__(1024) k_sample(Work w)
             atomicAdd(w.counters + C_P_JCHUNKS, sg.size * J);
         }
     }
-    // splitters: every second sample; level-order tree over them
+    // splitters: every sample but the first; level-order tree over them
     uint64_t* spl = w.spl + (size_t)s * 1024;
     uint64_t* tree = w.tree + (size_t)s * 1024;
-    for (uint32_t j = threadIdx.x; j < k; j += blockDim.x) spl[j] = samp[2 * j + 1];
+    for (uint32_t j = threadIdx.x; j < k; j += blockDim.x) spl[j] = samp[j + 1];
     for (uint32_t v = 1 + threadIdx.x; v <= k; v += blockDim.x) {
         const uint32_t h = 31 - __clz((int)v);
         const uint32_t p = v - (1u << h);
         const uint32_t r = ((2 * p + 1) << (L - 1 - h)) - 1;  // in-order rank
-        tree[v] = samp[2 * r + 1];
+        tree[v] = samp[r + 1];
     }
     if (threadIdx.x == 0) w.tree_bits[s] = (uint8_t)L;
 }

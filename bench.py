@@ -217,6 +217,23 @@ def replica_value(ranks: Ranks, chars: int, ms: float) -> tuple:
     return total / (ms_max / 1e3) / 1e9, ms_max, total
 
 
+def offset_wire_bytes(offs) -> int:
+    """Bytes of an offset array that cross PCIe in pssgpu_sort_host: 1- or
+    2-byte gaps for 2^20 or more offsets that never decrease with every gap
+    below 65536 (the library rebuilds them on the device), else 8 each."""
+    n = len(offs)
+    if n < (1 << 20):
+        return 8 * n
+    o = offs.view(np.int64)
+    top = 0
+    for i in range(0, n - 1, 1 << 24):
+        d = np.diff(o[i:min(i + (1 << 24) + 1, n)])
+        if d.size and d.min() < 0:
+            return 8 * n
+        top = max(top, int(d.max()) if d.size else 0)
+    return n if top < 256 else 2 * n if top < 65536 else 8 * n
+
+
 def pinned_alloc(torch):
     def alloc(nbytes, dtype):
         t = torch.empty(int(nbytes), dtype=torch.uint8, pin_memory=True)
@@ -696,7 +713,8 @@ def main():
             "data": "synthetic", "config": workload_config(n, nchars, args.workload),
             "strings_per_s": world * n / (ms_max / 1e3),
             "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": nchars + 8 * n,
-                    "d2h_bytes_per_step": 4 * n, "ms_per_step": e2e_s * 1e3},
+                    "d2h_bytes_per_step": 4 * n, "ms_per_step": e2e_s * 1e3,
+                    "h2d_wire_bytes_per_step": nchars + offset_wire_bytes(h_offs)},
             "e2e_text": e2e_text,
             "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak,

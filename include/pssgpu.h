@@ -122,6 +122,11 @@ int pssgpu_ctx_set_option(pssgpu_ctx* ctx, int option, int64_t value);
  * pssgpu_sort_host: host buffers; the call copies the arena and offsets to
  * the device, sorts, and copies perm/lcp back. Replaces the body of a
  * psstest contestant run (src/psstest.cpp:387-403) for an arena input.
+ * Offsets of 2^20 or more strings that never decrease, with every gap below
+ * 65536 (strings laid out in order), cross PCIe as 1- or 2-byte gaps,
+ * computed by host threads while the arena is copied, and are rebuilt on the
+ * device; other offset arrays are copied as they are. The result is the same
+ * either way. Pinned host buffers let the copies overlap the host work.
  *
  * pssgpu_sort_device: device buffers on the context's device. d_chars must
  * be 8-byte aligned and readable for nchars + PSSGPU_ARENA_PAD bytes;

@@ -115,4 +115,82 @@ __global__ void k_text_suffixes(uint64_t* __restrict__ offs, uint64_t size)
         offs[i] = i;
 }
 
+// Offsets rebuilt from gaps. A host offset array that never decreases
+// crosses PCIe as its gaps g[0] = 0, g[i] = offs[i] - offs[i-1] in 1 or 2
+// bytes each; offs[i] = offs[0] + g[0] + ... + g[i]. Per chunk of
+// GAP_CHUNK gaps (GAP_THREADS threads, GAP_PER contiguous gaps each): the
+// chunk sum (k_gap_sum), the scan of the chunk sums (k_text_scan), then the
+// offsets of the chunk (k_gap_offsets). The gap buffer is zero-padded to a
+// whole number of chunks.
+constexpr int GAP_THREADS = 256;
+constexpr int GAP_PER = 32;
+constexpr uint32_t GAP_CHUNK = GAP_THREADS * GAP_PER;
+
+template <class T>
+__device__ __forceinline__ void load_gaps(const T* __restrict__ g, uint32_t (&v)[GAP_PER])
+{
+    static_assert(sizeof(T) * GAP_PER % 16 == 0, "whole 16-byte vectors");
+    constexpr int NV = (int)(sizeof(T) * GAP_PER / 16);
+    const uint4* p = reinterpret_cast<const uint4*>(g);
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+        const uint4 x = __ldg(p + q);
+        const uint32_t w[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (sizeof(T) == 1) {
+#pragma unroll
+                for (int b = 0; b < 4; ++b) v[16 * q + 4 * k + b] = (w[k] >> (8 * b)) & 0xFFu;
+            } else {
+                v[8 * q + 2 * k] = w[k] & 0xFFFFu;
+                v[8 * q + 2 * k + 1] = w[k] >> 16;
+            }
+        }
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(GAP_THREADS) k_gap_sum(const T* __restrict__ gaps, uint32_t* __restrict__ cnt)
+{
+    __shared__ uint32_t tmp[32];
+    uint32_t v[GAP_PER];
+    load_gaps<T>(gaps + (size_t)blockIdx.x * GAP_CHUNK + (size_t)threadIdx.x * GAP_PER, v);
+    uint32_t s = 0;
+#pragma unroll
+    for (int j = 0; j < GAP_PER; ++j) s += v[j];
+    uint32_t total;
+    block_excl_sum<GAP_THREADS>(s, tmp, &total);
+    if (threadIdx.x == 0) cnt[blockIdx.x] = total;
+}
+
+template <class T>
+__global__ void __launch_bounds__(GAP_THREADS) k_gap_offsets(const T* __restrict__ gaps, uint64_t n, uint64_t first,
+                                                             const uint64_t* __restrict__ base,
+                                                             uint64_t* __restrict__ offs)
+{
+    __shared__ uint32_t tmp[32];
+    const uint64_t i0 = (uint64_t)blockIdx.x * GAP_CHUNK + (uint64_t)threadIdx.x * GAP_PER;
+    uint32_t v[GAP_PER];
+    load_gaps<T>(gaps + i0, v);
+    uint32_t s = 0;
+#pragma unroll
+    for (int j = 0; j < GAP_PER; ++j) s += v[j];
+    uint64_t run = first + base[blockIdx.x] + block_excl_sum<GAP_THREADS>(s, tmp, nullptr);
+    if (i0 + GAP_PER <= n) {
+        ulonglong2* o = reinterpret_cast<ulonglong2*>(offs + i0);
+#pragma unroll
+        for (int j = 0; j < GAP_PER; j += 2) {
+            const uint64_t a = run + v[j];
+            run = a + v[j + 1];
+            o[j / 2] = make_ulonglong2(a, run);
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < GAP_PER; ++j) {
+            run += v[j];
+            if (i0 + j < n) offs[i0 + j] = run;
+        }
+    }
+}
+
 }  // namespace pssgpu

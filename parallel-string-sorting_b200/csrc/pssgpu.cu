@@ -167,6 +167,8 @@ struct Ctx {
     // staging for the host entry points
     unsigned char* io = nullptr;
     uint64_t io_bytes = 0;
+    unsigned char* gap_host = nullptr;  // pinned: offset gaps on their way to the device
+    uint64_t gap_host_bytes = 0;
     // text entry point: offsets, perm and lcp beside the text in io;
     // chunk counts and bases of the line split
     unsigned char* io2 = nullptr;
@@ -789,6 +791,7 @@ static void ctx_destroy(Ctx* c)
     if (c->sfx) cudaFree(c->sfx);
     if (c->inst_buf) cudaFree(c->inst_buf);
     if (c->host_counters) cudaFreeHost(c->host_counters);
+    if (c->gap_host) cudaFreeHost(c->gap_host);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     for (int k = 0; k < 2 * K_NCLASS; ++k)
@@ -896,6 +899,119 @@ static int sort_text_host_locked(Ctx* c, const uint8_t* text, uint64_t size, int
     return PSSGPU_OK;
 }
 
+// fn(part, lo, hi) over `parts` contiguous slices of [0, n), one host thread
+// per slice.
+template <class F>
+static void host_parts(size_t n, size_t parts, F fn)
+{
+    if (parts <= 1) {
+        fn((size_t)0, (size_t)0, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    th.reserve(parts);
+    for (size_t p = 0; p < parts; ++p)
+        th.emplace_back([&fn, n, parts, p] { fn(p, n * p / parts, n * (p + 1) / parts); });
+    for (auto& t : th) t.join();
+}
+
+// Slices for host_parts: one per 64 Ki items, at most one per hardware thread
+// (capped at 32).
+static size_t host_slices(size_t n)
+{
+    const size_t hw = std::max(1u, std::min(std::thread::hardware_concurrency(), 32u));
+    return std::max<size_t>(1, std::min(hw, n >> 16));
+}
+
+// Offset arrays of at least this many strings may cross PCIe as gaps.
+constexpr uint64_t GAP_MIN_N = 1u << 20;
+
+// Copy n host offsets to d_offs on stream st. When the offsets never
+// decrease (strings laid out in order, as psstest's loader and the packing
+// of pointer arrays leave them) and every gap is below 65536, host threads
+// write the gaps in 1 or 2 bytes each to a pinned buffer while the copies
+// already queued on st run, 1-2 bytes instead of 8 cross PCIe, and
+// k_gap_sum / k_text_scan / k_gap_offsets rebuild the offsets in HBM.
+// scratch (device, 256-byte aligned, free until the sort writes it) takes
+// the gaps and the chunk sums; when it is too small, or n < GAP_MIN_N, or
+// the offsets do not qualify, the offsets are copied as they are.
+static int upload_offsets(Ctx* c, const uint64_t* offs, uint64_t n, uint64_t* d_offs,
+                          unsigned char* scratch, uint64_t scratch_bytes, cudaStream_t st)
+{
+    const uint64_t nchunk = (n + GAP_CHUNK - 1) / GAP_CHUNK;
+    const uint64_t padded = nchunk * GAP_CHUNK;
+    auto need = [&](uint64_t w) {
+        return align256(w * padded) + align256(4 * nchunk) + 8 * (nchunk + 1);
+    };
+    if (n < GAP_MIN_N || need(2) > scratch_bytes) {
+        PSS_CUDA(cudaMemcpyAsync(d_offs, offs, 8 * n, cudaMemcpyHostToDevice, st));
+        return PSSGPU_OK;
+    }
+    if (!c->gap_host || c->gap_host_bytes < 2 * n) {
+        if (c->gap_host) cudaFreeHost(c->gap_host);
+        c->gap_host = nullptr;
+        c->gap_host_bytes = 0;
+        if (cudaHostAlloc((void**)&c->gap_host, 2 * n, cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            c->gap_host = nullptr;
+            PSS_CUDA(cudaMemcpyAsync(d_offs, offs, 8 * n, cudaMemcpyHostToDevice, st));
+            return PSSGPU_OK;
+        }
+        c->gap_host_bytes = 2 * n;
+    }
+    const size_t parts = host_slices(n);
+    std::vector<uint8_t> ok(parts, 1);
+    std::vector<uint64_t> mx(parts, 0);
+    uint8_t* g8 = c->gap_host;
+    host_parts(n, parts, [&](size_t p, size_t b, size_t e) {
+        uint64_t prev = offs[b ? b - 1 : 0], m = 0;
+        bool up = true;
+        for (size_t i = b; i < e; ++i) {
+            const uint64_t o = offs[i];
+            up &= o >= prev;
+            m = std::max(m, o - prev);
+            g8[i] = (uint8_t)(o - prev);
+            prev = o;
+        }
+        ok[p] = up;
+        mx[p] = m;
+    });
+    uint64_t m = 0;
+    for (size_t p = 0; p < parts; ++p) {
+        if (!ok[p]) m = ~0ull;
+        m = std::max(m, mx[p]);
+    }
+    if (m >= 65536) {
+        PSS_CUDA(cudaMemcpyAsync(d_offs, offs, 8 * n, cudaMemcpyHostToDevice, st));
+        return PSSGPU_OK;
+    }
+    const uint64_t w = m < 256 ? 1 : 2;
+    if (w == 2) {
+        uint16_t* g16 = reinterpret_cast<uint16_t*>(c->gap_host);
+        host_parts(n, parts, [&](size_t, size_t b, size_t e) {
+            for (size_t i = b; i < e; ++i) g16[i] = (uint16_t)(i ? offs[i] - offs[i - 1] : 0);
+        });
+    }
+    unsigned char* d_gaps = scratch;
+    uint32_t* d_cnt = reinterpret_cast<uint32_t*>(scratch + align256(w * padded));
+    uint64_t* d_base = reinterpret_cast<uint64_t*>(scratch + align256(w * padded) + align256(4 * nchunk));
+    PSS_CUDA(cudaMemcpyAsync(d_gaps, c->gap_host, w * n, cudaMemcpyHostToDevice, st));
+    PSS_CUDA(cudaMemsetAsync(d_gaps + w * n, 0, w * (padded - n), st));
+    const unsigned nb = (unsigned)nchunk;
+    if (w == 1) {
+        k_gap_sum<uint8_t><<<nb, GAP_THREADS, 0, st>>>(d_gaps, d_cnt);
+        k_text_scan<<<1, 1024, 0, st>>>(d_cnt, nb, d_base, d_base + nchunk);
+        k_gap_offsets<uint8_t><<<nb, GAP_THREADS, 0, st>>>(d_gaps, n, offs[0], d_base, d_offs);
+    } else {
+        const uint16_t* g = reinterpret_cast<const uint16_t*>(d_gaps);
+        k_gap_sum<uint16_t><<<nb, GAP_THREADS, 0, st>>>(g, d_cnt);
+        k_text_scan<<<1, 1024, 0, st>>>(d_cnt, nb, d_base, d_base + nchunk);
+        k_gap_offsets<uint16_t><<<nb, GAP_THREADS, 0, st>>>(g, n, offs[0], d_base, d_offs);
+    }
+    PSS_CUDA(cudaGetLastError());
+    return PSSGPU_OK;
+}
+
 // Host buffers in, host buffers out. Caller holds c->mu.
 static int sort_host_locked(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_t* offs,
                             uint64_t n, uint32_t* perm, uint32_t* lcp)
@@ -917,7 +1033,7 @@ static int sort_host_locked(Ctx* c, const uint8_t* chars, uint64_t nchars, const
     cudaStream_t st = c->stream;
     PSS_CUDA(cudaMemcpyAsync(d_chars, chars, nchars, cudaMemcpyHostToDevice, st));
     PSS_CUDA(cudaMemsetAsync(d_chars + nchars, 0, b_chars - nchars, st));
-    PSS_CUDA(cudaMemcpyAsync(d_offs, offs, 8 * n, cudaMemcpyHostToDevice, st));
+    if ((rc = upload_offsets(c, offs, n, d_offs, (unsigned char*)d_perm, b_perm, st))) return rc;
     if ((rc = run_sort(c, d_chars, nchars, d_offs, (uint32_t)n, d_perm, d_lcp, st))) return rc;
     PSS_CUDA(cudaMemcpyAsync(perm, d_perm, 4 * n, cudaMemcpyDeviceToHost, st));
     if (lcp && n > 1)
@@ -969,7 +1085,7 @@ static int sort_batch_host_locked(Ctx* c, const uint8_t* chars, uint64_t nchars,
     uint32_t* d_lcp = lcp ? (uint32_t*)(c->io + b_chars + b_offs + b_perm) : nullptr;
     PSS_CUDA(cudaMemcpyAsync(d_chars, chars, nchars, cudaMemcpyHostToDevice, st));
     PSS_CUDA(cudaMemsetAsync(d_chars + nchars, 0, b_chars - nchars, st));
-    PSS_CUDA(cudaMemcpyAsync(d_offs, offs, 8 * n, cudaMemcpyHostToDevice, st));
+    if ((rc = upload_offsets(c, offs, n, d_offs, (unsigned char*)d_perm, b_perm, st))) return rc;
     if ((rc = run_sort(c, d_chars, nchars, d_offs, (uint32_t)n, d_perm, d_lcp, st, c->inst_buf,
                        ninst)))
         return rc;
@@ -994,30 +1110,6 @@ static Ctx* default_ctx(int device, int* rc)
     }
     *rc = PSSGPU_OK;
     return ctxs[device];
-}
-
-// fn(part, lo, hi) over `parts` contiguous slices of [0, n), one host thread
-// per slice.
-template <class F>
-static void host_parts(size_t n, size_t parts, F fn)
-{
-    if (parts <= 1) {
-        fn((size_t)0, (size_t)0, n);
-        return;
-    }
-    std::vector<std::thread> th;
-    th.reserve(parts);
-    for (size_t p = 0; p < parts; ++p)
-        th.emplace_back([&fn, n, parts, p] { fn(p, n * p / parts, n * (p + 1) / parts); });
-    for (auto& t : th) t.join();
-}
-
-// Slices for host_parts: one per 64 Ki items, at most one per hardware thread
-// (capped at 32).
-static size_t host_slices(size_t n)
-{
-    const size_t hw = std::max(1u, std::min(std::thread::hardware_concurrency(), 32u));
-    return std::max<size_t>(1, std::min(hw, n >> 16));
 }
 
 // Pack a pointer array into (arena, offsets), sort it and write the sorted

@@ -335,6 +335,43 @@ def test_prefix_small_vs_oracle(pkg, orc, ctx):
     check_against_oracle(orc, chars[:nchars], offs, perm, lcp)
 
 
+def _arena_from_lengths(lens, alpha, seed):
+    rng = np.random.default_rng(seed)
+    lens = np.asarray(lens, np.uint64)
+    offs = np.zeros(len(lens), np.uint64)
+    offs[1:] = np.cumsum(lens[:-1] + 1)
+    total = int(offs[-1] + lens[-1]) + 1
+    chars = rng.choice(np.frombuffer(alpha, np.uint8), total).astype(np.uint8)
+    chars[(offs + lens).astype(np.int64)] = 0
+    return chars, offs
+
+
+@pytest.mark.parametrize("case", ["gaps8", "gaps16", "decreasing", "gap_over_16_bits"])
+def test_host_offsets_as_gaps(pkg, orc, ctx, case):
+    # host offset arrays of 1 Mi or more strings that never decrease cross
+    # PCIe as 1- or 2-byte gaps and are rebuilt on the device; the others are
+    # copied as they are. Every form must sort exactly as the oracle does.
+    n = 1_100_000
+    rng = np.random.default_rng(71)
+    lens = rng.integers(0, 12, n)
+    if case == "gaps16":
+        lens[::997] = rng.integers(300, 700, len(lens[::997]))
+    if case == "gap_over_16_bits":
+        lens[n // 2] = 70_000
+    chars, offs = _arena_from_lengths(lens, b"abcd", 72)
+    if case == "decreasing":
+        offs = offs[rng.permutation(n)]
+    perm, lcp = ctx.sort_host(chars, offs, lcp=True)
+    check_against_oracle(orc, chars, offs, perm, lcp)
+    # the same strings through the device entry point (offsets copied as they are)
+    import torch
+    dp = torch.empty(n, dtype=torch.int32, device="cuda")
+    ctx.sort_device(torch.from_numpy(chars).cuda(), len(chars),
+                    torch.from_numpy(offs.view(np.int64)).cuda(), dp)
+    assert np.array_equal(canonical_ids(chars, offs, dp.cpu().numpy().view(np.uint32), lcp),
+                          canonical_ids(chars, offs, perm, lcp))
+
+
 def test_device_api(pkg, orc, ctx):
     import torch
     chars, offs, nchars = pkg.workloads.random_strings(50000, 0, 16, b"abcd", 13)

@@ -175,4 +175,87 @@ __device__ __forceinline__ void bitonic_sort_block(uint64_t* a, uint32_t S)
     }
 }
 
+// Ascending bitonic sort of a[0, S) (S a power of two, at least 64) by the
+// whole block, where a[m, S) holds padding larger than every key (m >= 1).
+// Every compare-exchange puts the smaller key at the lower position, and each
+// merge of 2^k keys starts by comparing every position with its mirror in the
+// merged block (the network without descending halves), so the padding never
+// moves: pairs that reach into it are skipped, and so are the 64-key chunks
+// that hold only padding. A group of m keys just above a power of two costs
+// little more than the power of two below it. Synchronises before returning.
+__device__ __forceinline__ void bitonic_sort_block_padded(uint64_t* a, uint32_t S, uint32_t m)
+{
+    const uint32_t lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const uint32_t nch = (m + 63) / 64;  // chunks holding keys
+    // register stages of one chunk: merges of 2..min(64, kk_to) keys in full
+    // (tail = false), or the steps of partner distance 32..1 (tail = true)
+    auto chunks = [&](uint32_t kk_to, bool tail) {
+        for (uint32_t c = threadIdx.x >> 5; c < nch; c += nw) {
+            const uint32_t e0 = c * 64 + 2 * lane;
+            uint64_t x0 = a[e0], x1 = a[e0 + 1];
+            auto step = [&](uint32_t j) {  // partner distance j, ascending
+                if (j == 1) {
+                    const uint64_t lo = min(x0, x1), hi = max(x0, x1);
+                    x0 = lo;
+                    x1 = hi;
+                } else {
+                    const uint64_t y0 = __shfl_xor_sync(0xffffffffu, x0, j >> 1);
+                    const uint64_t y1 = __shfl_xor_sync(0xffffffffu, x1, j >> 1);
+                    const bool keep_min = (lane & (j >> 1)) == 0;
+                    x0 = keep_min ? min(x0, y0) : max(x0, y0);
+                    x1 = keep_min ? min(x1, y1) : max(x1, y1);
+                }
+            };
+            if (tail) {
+#pragma unroll
+                for (uint32_t j = 32; j > 0; j >>= 1) step(j);
+            } else {
+                for (uint32_t kk = 2; kk <= min(64u, kk_to); kk <<= 1) {
+                    if (kk == 2) {
+                        step(1);
+                        continue;
+                    }
+                    // mirror step: position e pairs with e ^ (kk - 1)
+                    const uint32_t mm = (kk >> 1) - 1;
+                    const uint64_t y0 = __shfl_xor_sync(0xffffffffu, x1, mm);
+                    const uint64_t y1 = __shfl_xor_sync(0xffffffffu, x0, mm);
+                    const bool lower = (lane & (kk >> 2)) == 0;
+                    x0 = lower ? min(x0, y0) : max(x0, y0);
+                    x1 = lower ? min(x1, y1) : max(x1, y1);
+                    for (uint32_t j = kk >> 2; j > 0; j >>= 1) step(j);
+                }
+            }
+            a[e0] = x0;
+            a[e0 + 1] = x1;
+        }
+    };
+    auto cas = [&](uint32_t x0, uint32_t x1) {
+        if (x1 >= m) return;  // padding stays where it is
+        const uint64_t x = a[x0], y = a[x1];
+        if (x > y) {
+            a[x0] = y;
+            a[x1] = x;
+        }
+    };
+    chunks(S, false);
+    __syncthreads();
+    for (uint32_t kk = 128; kk <= S; kk <<= 1) {
+        const uint32_t half = kk >> 1;
+        for (uint32_t i = threadIdx.x; i < S / 2; i += blockDim.x) {
+            const uint32_t blk = i / half, off = i - blk * half;
+            cas(blk * kk + off, blk * kk + kk - 1 - off);
+        }
+        __syncthreads();
+        for (uint32_t j = kk >> 2; j >= 64; j >>= 1) {
+            for (uint32_t i = threadIdx.x; i < S / 2; i += blockDim.x) {
+                const uint32_t x0 = 2 * i - (i & (j - 1));
+                cas(x0, x0 + j);
+            }
+            __syncthreads();
+        }
+        chunks(0, true);
+        __syncthreads();
+    }
+}
+
 }  // namespace pssgpu

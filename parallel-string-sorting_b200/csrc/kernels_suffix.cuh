@@ -240,7 +240,8 @@ __global__ void k_dbl_sort_small(const Seg* __restrict__ list, uint32_t count,
 
 // Round step 2 for groups of 33..MAXM members, one block each: a bitonic
 // sort of (key << 32 | member index) in shared memory (dynamic: MAXM keys,
-// then MAXM member ids).
+// then MAXM member ids), padded to a power of two with keys that the network
+// never moves (bitonic_sort_block_padded).
 template <uint32_t MAXM>
 __global__ void __launch_bounds__(MAXM <= DBL_MID ? 256 : 512) k_dbl_sort_block(
     const Seg* __restrict__ list, uint32_t* __restrict__ perm, DblArrays a, uint32_t* counters,
@@ -262,7 +263,7 @@ __global__ void __launch_bounds__(MAXM <= DBL_MID ? 256 : 512) k_dbl_sort_block(
         }
     }
     __syncthreads();
-    bitonic_sort_block(sk, S);
+    bitonic_sort_block_padded(sk, S, m);
     // warp-uniform trip counts, so that appends aggregate per warp
     for (uint32_t i0 = threadIdx.x & ~31u; i0 < m; i0 += blockDim.x) {
         const uint32_t i = i0 + (threadIdx.x & 31);

@@ -28,7 +28,11 @@
 namespace pssgpu {
 
 constexpr uint32_t DBL_NONE = 0xFFFFFFFFu;  // lb: no doubling bound
-constexpr uint32_t DBL_MID = 512;           // largest group of the smaller block sort
+// largest group of the smaller block sort (256 threads, 12 KB of shared
+// memory); groups just above 512, common when a text's 8-char prefixes each
+// head about 512 suffixes, sort here rather than in 512-thread blocks of
+// 48 KB
+constexpr uint32_t DBL_MID = 1024;
 
 // Group lists of a round, by size class: 0 at most 32 members (one warp
 // each), 1 at most DBL_MID (a block of 256 threads), 2 at most DBL_MAX (a

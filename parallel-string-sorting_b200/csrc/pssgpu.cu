@@ -426,8 +426,8 @@ static int run_doubling(Ctx* c, Work& w, uint32_t ndbl, cudaStream_t st, pssgpu_
         PSS_CUDA(cudaMemcpyAsync(hc, w.counters, 4 * C_COUNT, cudaMemcpyDeviceToHost, st));
         PSS_CUDA(cudaStreamSynchronize(st));
         if (c->trace)
-            std::fprintf(stderr, "pssgpu doubling round %d: groups %u / %u / %u (<=32 / <=512 / <=4096)\n",
-                         round, cnt[0], cnt[1], cnt[2]);
+            std::fprintf(stderr, "pssgpu doubling round %d: groups %u / %u / %u (<=32 / <=%u / <=%u)\n",
+                         round, cnt[0], cnt[1], cnt[2], DBL_MID, DBL_MAX);
         par ^= 1;
     }
     *err = hc[C_ERR];

@@ -346,18 +346,27 @@ def _arena_from_lengths(lens, alpha, seed):
     return chars, offs
 
 
-@pytest.mark.parametrize("case", ["gaps8", "gaps16", "decreasing", "gap_over_16_bits"])
+@pytest.mark.parametrize("case", ["gaps8", "gaps16", "decreasing", "gap_over_16_bits",
+                                  "gap_255", "gap_256", "gap_65535", "threshold"])
 def test_host_offsets_as_gaps(pkg, orc, ctx, case):
     # host offset arrays of 1 Mi or more strings that never decrease cross
     # PCIe as 1- or 2-byte gaps and are rebuilt on the device; the others are
     # copied as they are. Every form must sort exactly as the oracle does.
-    n = 1_100_000
+    # A gap is a string's length + 1: 255 is the widest 1-byte gap, 65535 the
+    # widest 2-byte one; "threshold" has exactly 2^20 strings.
+    n = (1 << 20) if case == "threshold" else 1_100_000
     rng = np.random.default_rng(71)
     lens = rng.integers(0, 12, n)
     if case == "gaps16":
         lens[::997] = rng.integers(300, 700, len(lens[::997]))
     if case == "gap_over_16_bits":
         lens[n // 2] = 70_000
+    if case == "gap_255":
+        lens[n // 3] = 254
+    if case == "gap_256":
+        lens[n // 3] = 255
+    if case == "gap_65535":
+        lens[n - 2] = 65_534
     chars, offs = _arena_from_lengths(lens, b"abcd", 72)
     if case == "decreasing":
         offs = offs[rng.permutation(n)]

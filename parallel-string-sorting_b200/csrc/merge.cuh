@@ -68,30 +68,48 @@ __device__ __forceinline__ uint32_t pair_of(const uint64_t* first, uint32_t npai
     return lo;
 }
 
+// Splits in two launches: coarse = 1 searches every MERGE_SPLIT_COARSE-th
+// piece of a pair over the whole diagonal; coarse = 0 searches the other
+// pieces between the two coarse splits around them. The merge path is a
+// monotone staircase, so for a diagonal d between coarse diagonals D0 < D1
+// with splits i0, i1: i0 <= i(d) <= i1 and d - D1 + i1 <= i(d) <= d - D0 + i0,
+// a window of at most MERGE_SPLIT_COARSE * piece positions.
+constexpr uint32_t MERGE_SPLIT_COARSE = 32;
+
 __global__ void k_merge_split(const uint8_t* __restrict__ chars, uint64_t nchars,
                               const uint64_t* __restrict__ offs, const MergePair* __restrict__ pairs,
                               const uint64_t* __restrict__ first, uint32_t npair,
                               const uint32_t* __restrict__ ids_in, uint64_t* __restrict__ split,
-                              uint32_t piece)
+                              uint32_t piece, int coarse)
 {
     const uint64_t ntask = first[npair];
     for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ntask;
          t += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t p = pair_of(first, npair, t);
+        const uint64_t k = t - first[p];
+        if ((k % MERGE_SPLIT_COARSE == 0) != (coarse != 0)) continue;
         const MergePair pr = pairs[p];
         const uint64_t na = pr.a1 - pr.a0, nb = pr.b1 - pr.a1;
-        const uint64_t d = (t - first[p]) * piece;
+        const uint64_t d = k * piece;
         // left-run strings among the first d outputs: the first i with
         // A[i] > B[d - i - 1] (ties go to the left run)
-        uint64_t lo = d > nb ? d - nb : 0, hi = min(d, na);
+        int64_t lo = d > nb ? (int64_t)(d - nb) : 0, hi = (int64_t)min(d, na);
+        if (!coarse) {
+            const uint64_t k0 = k - k % MERGE_SPLIT_COARSE, k1 = k0 + MERGE_SPLIT_COARSE;
+            const uint64_t D0 = k0 * piece, i0 = split[first[p] + k0];
+            const bool last = first[p] + k1 >= first[p + 1];
+            const uint64_t D1 = last ? na + nb : k1 * piece, i1 = last ? na : split[first[p] + k1];
+            lo = max(lo, max((int64_t)i0, (int64_t)d - (int64_t)D1 + (int64_t)i1));
+            hi = min(hi, min((int64_t)i1, (int64_t)(d - D0 + i0)));
+        }
         while (lo < hi) {
-            const uint64_t mid = (lo + hi) >> 1;
+            const int64_t mid = (lo + hi) >> 1;
             uint32_t l;
             const int c = compare_lcp(chars, nchars, __ldg(offs + ids_in[pr.a0 + mid]),
                                       __ldg(offs + ids_in[pr.a1 + d - mid - 1]), &l);
             if (c <= 0) lo = mid + 1; else hi = mid;
         }
-        split[t] = lo;
+        split[t] = (uint64_t)lo;
     }
 }
 

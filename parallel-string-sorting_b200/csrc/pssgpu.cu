@@ -1644,8 +1644,9 @@ int pssgpu_merge_lcp_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nc
         const uint64_t* first = d_flat + at_first[i];
         const uint32_t np = (uint32_t)npairs[i];
         const uint32_t pc = c->merge_piece;
-        k_merge_split<<<blocks, 256, 0, st>>>(d_chars, nchars, d_offs, pairs, first, np, in_ids, split,
-                                              pc);
+        for (int coarse = 1; coarse >= 0; --coarse)
+            k_merge_split<<<blocks, 256, 0, st>>>(d_chars, nchars, d_offs, pairs, first, np, in_ids,
+                                                  split, pc, coarse);
         if (with_lcp)
             k_merge_lcp_seq<<<blocks, 256, 0, st>>>(d_chars, nchars, d_offs, pairs, first, np, split,
                                                     in_ids, in_lcp, out_ids, out_lcp, pc);

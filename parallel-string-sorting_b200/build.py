@@ -46,7 +46,8 @@ def build_cuda(force: bool = False) -> Path:
     if force or _stale(out, deps):
         LIB.mkdir(exist_ok=True)
         _run([NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
-              "-shared", "-o", str(out), *[str(CSRC / s) for s in CUDA_SOURCES]])
+              "-Xcompiler", "-fopenmp", "-shared", "-o", str(out),
+              *[str(CSRC / s) for s in CUDA_SOURCES], "-lgomp"])
     return out
 
 

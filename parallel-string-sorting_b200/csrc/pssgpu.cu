@@ -169,6 +169,9 @@ struct Ctx {
     uint64_t io_bytes = 0;
     unsigned char* gap_host = nullptr;  // pinned: offset gaps on their way to the device
     uint64_t gap_host_bytes = 0;
+    // pinned: the pointer-array entry points' offsets, permutation and LCPs
+    unsigned char* ptr_host = nullptr;
+    uint64_t ptr_host_bytes = 0;
     // text entry point: offsets, perm and lcp beside the text in io;
     // chunk counts and bases of the line split
     unsigned char* io2 = nullptr;
@@ -792,6 +795,7 @@ static void ctx_destroy(Ctx* c)
     if (c->inst_buf) cudaFree(c->inst_buf);
     if (c->host_counters) cudaFreeHost(c->host_counters);
     if (c->gap_host) cudaFreeHost(c->gap_host);
+    if (c->ptr_host) cudaFreeHost(c->ptr_host);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     for (int k = 0; k < 2 * K_NCLASS; ++k)
@@ -900,7 +904,8 @@ static int sort_text_host_locked(Ctx* c, const uint8_t* text, uint64_t size, int
 }
 
 // fn(part, lo, hi) over `parts` contiguous slices of [0, n), one host thread
-// per slice.
+// per slice, from OpenMP's pool (its threads outlive the call, so a call
+// costs no thread start-up).
 template <class F>
 static void host_parts(size_t n, size_t parts, F fn)
 {
@@ -908,11 +913,9 @@ static void host_parts(size_t n, size_t parts, F fn)
         fn((size_t)0, (size_t)0, n);
         return;
     }
-    std::vector<std::thread> th;
-    th.reserve(parts);
-    for (size_t p = 0; p < parts; ++p)
-        th.emplace_back([&fn, n, parts, p] { fn(p, n * p / parts, n * (p + 1) / parts); });
-    for (auto& t : th) t.join();
+#pragma omp parallel for num_threads((int)parts) schedule(static, 1)
+    for (long long p = 0; p < (long long)parts; ++p)
+        fn((size_t)p, n * (size_t)p / parts, n * ((size_t)p + 1) / parts);
 }
 
 // Slices for host_parts: one per 64 Ki items, at most one per hardware thread
@@ -1136,7 +1139,19 @@ static int sort_pointer_array(unsigned char** strings, unsigned char** out, uint
     if (!c) return rc;
     std::lock_guard<std::mutex> lk(c->mu);
     const size_t parts = host_slices(n);
-    std::vector<uint64_t> offs(n);
+    // offsets, permutation and LCPs in the context's pinned buffer (copies at
+    // full PCIe speed, no page faults per call)
+    const uint64_t need = 8ull * n + 4ull * n + (lcp_out ? 4ull * n : 0ull);
+    if (!c->ptr_host || c->ptr_host_bytes < need) {
+        if (c->ptr_host) cudaFreeHost(c->ptr_host);
+        c->ptr_host = nullptr;
+        c->ptr_host_bytes = 0;
+        PSS_CUDA(cudaHostAlloc((void**)&c->ptr_host, need, cudaHostAllocDefault));
+        c->ptr_host_bytes = need;
+    }
+    uint64_t* const offs = reinterpret_cast<uint64_t*>(c->ptr_host);
+    uint32_t* const perm = reinterpret_cast<uint32_t*>(c->ptr_host + 8ull * n);
+    uint32_t* const lcp32 = lcp_out ? perm + n : nullptr;
     std::vector<uint8_t> packed;
     const uint8_t* arena;
     uint64_t nchars;
@@ -1171,10 +1186,9 @@ static int sort_pointer_array(unsigned char** strings, unsigned char** out, uint
             // all suffixes of the text lo[0, n) (psstest --suffix): only the
             // text crosses to the device, which makes the offsets itself, and
             // the sorted pointers are lo + perm[i]
-            std::vector<uint32_t> perm(n), lcp32(lcp_out ? n : 0);
             uint64_t nn = 0;
-            rc = sort_text_host_locked(c, (const uint8_t*)lo, n, PSSGPU_TEXT_SUFFIXES, perm.data(),
-                                       lcp_out ? lcp32.data() : nullptr, n, &nn);
+            rc = sort_text_host_locked(c, (const uint8_t*)lo, n, PSSGPU_TEXT_SUFFIXES, perm, lcp32, n,
+                                       &nn);
             if (rc) return rc;
             if (nn != n) return fail(PSSGPU_ECUDA, "suffix count differs");
             host_parts(n, parts, [&](size_t, size_t b, size_t e) {
@@ -1217,14 +1231,14 @@ static int sort_pointer_array(unsigned char** strings, unsigned char** out, uint
         });
         arena = packed.data();
     }
-    std::vector<uint32_t> perm(n);
-    std::vector<uint32_t> lcp32(lcp_out ? n : 0);
-    rc = sort_host_locked(c, arena, nchars, offs.data(), n, perm.data(),
-                          lcp_out ? lcp32.data() : nullptr);
+    rc = sort_host_locked(c, arena, nchars, offs, n, perm, lcp32);
     if (rc) return rc;
+    // sorted pointers: in the caller's buffer string id's pointer is
+    // arena + offs[id]; gathered strings need the original array (a copy
+    // of it when the output overwrites it)
     std::vector<unsigned char*> orig;
     unsigned char* const* src = strings;
-    if (out == strings) {
+    if (!arena_lo && out == strings) {
         orig.resize(n);
         host_parts(n, parts, [&](size_t, size_t b, size_t e) {
             memcpy(orig.data() + b, strings + b, (e - b) * sizeof(unsigned char*));
@@ -1232,7 +1246,10 @@ static int sort_pointer_array(unsigned char** strings, unsigned char** out, uint
         src = orig.data();
     }
     host_parts(n, parts, [&](size_t, size_t b, size_t e) {
-        for (size_t i = b; i < e; ++i) out[i] = src[perm[i]];
+        if (arena_lo)
+            for (size_t i = b; i < e; ++i) out[i] = const_cast<unsigned char*>(arena) + offs[perm[i]];
+        else
+            for (size_t i = b; i < e; ++i) out[i] = src[perm[i]];
         if (lcp_out)
             for (size_t i = std::max<size_t>(b, 1); i < e; ++i) lcp_out[i] = lcp32[i];
         if (cache && lcp_out)

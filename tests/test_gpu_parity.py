@@ -688,6 +688,29 @@ def test_pointer_array_out_and_arena(pkg, orc):
     assert pkg.sort_pointer_array_out(ptrs, ptrs, n) == 0  # output == input: in place
 
 
+@pytest.mark.parametrize("n", [1_100_000, 1_300_000])
+def test_pointer_array_arena_large(pkg, orc, n):
+    """The arena entry above 2^20 strings (offsets cross PCIe as gaps; the
+    context's pinned buffers are reused by the second size and grown), in
+    place and with LCP output, twice in a row, against the oracle."""
+    chars, offs, nchars = pkg.workloads.random_strings(n, 0, 20, b"abc", 31 + n)
+    buf = (C.c_ubyte * len(chars)).from_buffer_copy(chars.tobytes())
+    base = C.addressof(buf)
+    ids, rlcp = orc.sort_ids_lcp(chars, offs)
+    want = np.array([int(offs[i]) for i in ids], dtype=np.uint64)
+    src = (C.c_void_p * n)(*[base + int(o) for o in offs])
+    for _ in range(2):
+        ptrs = (C.c_void_p * n)()
+        C.memmove(ptrs, src, C.sizeof(src))
+        lcp = (C.c_size_t * n)()
+        assert pkg.sort_pointer_array_arena(base, nchars, ptrs, n, None, lcp) == 0
+        got = np.frombuffer(ptrs, dtype=np.uint64) - np.uint64(base)
+        # equal strings may come in any order: order and multiset of offsets
+        assert np.array_equal(np.array(lcp[1:], dtype=np.uint64), rlcp[1:])
+        assert orc.check_order(chars, got, np.arange(n, dtype=np.uint32)) == -1
+        assert np.array_equal(np.sort(got), np.sort(want))
+
+
 def test_errors_are_status_codes(pkg, ctx):
     chars = np.frombuffer(b"abc", dtype=np.uint8).copy()  # no terminating NUL
     with pytest.raises(pkg.SortError) as e:

@@ -34,10 +34,19 @@ constexpr uint32_t DBL_NONE = 0xFFFFFFFFu;  // lb: no doubling bound
 // 48 KB
 constexpr uint32_t DBL_MID = 1024;
 
+// Round 0 sorts every handed-over group by the DBL_ROUND0_CHARS chars that
+// follow its shared prefix, read from the text (a text of this size stays in
+// L2), instead of by ranks: no rank has to be written before it and none
+// read in it, and its ties form groups DBL_ROUND0_CHARS deeper. The key and
+// a member index of up to 16 bits fill one 64-bit sort word.
+constexpr uint32_t DBL_ROUND0_CHARS = 6;
+
 // Group lists of a round, by size class: 0 at most 32 members (one warp
 // each), 1 at most DBL_MID (a block of 256 threads), 2 at most DBL_MAX (a
 // block of 512 threads); double-buffered by round parity.
 struct DblArrays {
+    const uint8_t* text;  // the text the suffixes belong to (round 0 reads it)
+    uint64_t ntext;
     uint32_t* isa;
     uint32_t* gd[2];
     uint32_t* key;
@@ -67,11 +76,13 @@ __global__ void k_suffix_check(const uint8_t* __restrict__ chars, const uint64_t
 }
 
 // Members of the groups the string passes handed over: their ids into perm
-// (the handles sit in the group's ping-pong buffer), their rank (the group
-// start) into isa, a mark in `taken`; the group's depth into gd[0]. The
-// groups are sorted into the round lists of parity 0 (dbl_push, below).
+// (the handles sit in the group's ping-pong buffer) and a mark in `taken`;
+// the group's depth into gd[0]. Their ranks come from round 0, which sorts
+// by text chars. The groups are sorted into the round lists of parity 0
+// (dbl_push, below) and their members counted.
 __global__ void k_dbl_init(Work w, const Seg* __restrict__ list, uint32_t count, DblArrays a,
-                           uint8_t* __restrict__ taken, uint32_t* counters);
+                           uint8_t* __restrict__ taken, uint32_t* counters,
+                           unsigned long long* members);
 
 // Every other position (not in a handed-over group) is final: its suffix's
 // rank is the position.
@@ -95,7 +106,8 @@ __device__ __forceinline__ void dbl_push(DblArrays& a, uint32_t* counters, int p
 // atomic per group serialises on the three list counters).
 constexpr uint32_t DBL_INIT_STAGE = 64;
 __global__ void k_dbl_init(Work w, const Seg* __restrict__ list, uint32_t count, DblArrays a,
-                           uint8_t* __restrict__ taken, uint32_t* counters)
+                           uint8_t* __restrict__ taken, uint32_t* counters,
+                           unsigned long long* members)
 {
     __shared__ Seg stage[3][DBL_INIT_STAGE];
     __shared__ uint32_t staged[3];
@@ -114,13 +126,12 @@ __global__ void k_dbl_init(Work w, const Seg* __restrict__ list, uint32_t count,
         const Seg s = list[g];
         const uint64_t* hs = w.hnd[s.meta & META_BUF];
         for (uint32_t q = threadIdx.x; q < s.size; q += blockDim.x) {
-            const uint32_t x = h_id(w, hs[s.begin + q]);
-            w.perm[s.begin + q] = x;
-            a.isa[x] = s.begin;
+            w.perm[s.begin + q] = h_id(w, hs[s.begin + q]);
             taken[s.begin + q] = 1;
         }
         if (threadIdx.x == 0) {
             a.gd[0][s.begin] = s.depth;
+            atomicAdd(members, (unsigned long long)s.size);
             const int c = dbl_class(s.size);
             stage[c][staged[c]++] = Seg{s.begin, s.size, s.depth, 0u};
             if (staged[c] == DBL_INIT_STAGE) flush(c);
@@ -182,18 +193,26 @@ __global__ void k_dbl_keys(const Seg* __restrict__ list, uint32_t count,
 
 // The run of equal keys K that starts at offset i0 of group s and has len
 // members: the LCP bound at its start, and for len >= 2 the subgroup (with
-// its depth recorded for the next round) into *out. Returns whether *out
-// is to be appended.
+// its depth recorded for the next round) into *out. The subgroup lies
+// `step` chars deeper (round 0's text chars), or, with step 0, as deep as
+// the group ranked K. Returns whether *out is to be appended.
 __device__ __forceinline__ bool dbl_run(DblArrays& a, int par, const Seg& s, uint32_t i0,
-                                        uint32_t len, uint32_t K, Seg* out)
+                                        uint32_t len, uint32_t K, Seg* out, uint32_t step)
 {
     const uint32_t p = s.begin + i0;
     if (a.lb && i0 > 0) a.lb[p] = s.depth;  // separated from p - 1 at this depth
     if (len < 2) return false;
-    const uint32_t nd = s.depth + a.gd[par][K];
+    const uint32_t nd = s.depth + (step ? step : a.gd[par][K]);
     a.gd[par ^ 1][p] = nd;
     *out = Seg{p, len, nd, 0u};
     return true;
+}
+
+// Round 0's key of suffix x in a group of depth d: the DBL_ROUND0_CHARS chars
+// at x + d, big-endian (load_key's NUL convention).
+__device__ __forceinline__ uint64_t dbl_round0_key(const DblArrays& a, uint32_t x, uint32_t d)
+{
+    return load_key(a.text, a.ntext, (uint64_t)x + d) >> (64 - 8 * DBL_ROUND0_CHARS);
 }
 
 // Round step 2 for groups of at most 32 members: each warp takes
@@ -202,7 +221,8 @@ __device__ __forceinline__ bool dbl_run(DblArrays& a, int par, const Seg& s, uin
 // and splits every group into runs of equal keys.
 constexpr uint32_t DBL_PER_WARP = 16;
 __global__ void k_dbl_sort_small(const Seg* __restrict__ list, uint32_t count,
-                                 uint32_t* __restrict__ perm, DblArrays a, uint32_t* counters, int par)
+                                 uint32_t* __restrict__ perm, DblArrays a, uint32_t* counters, int par,
+                                 int round0)
 {
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t g0 = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * DBL_PER_WARP;
@@ -211,7 +231,8 @@ __global__ void k_dbl_sort_small(const Seg* __restrict__ list, uint32_t count,
     warp_seg_windows(list + g0, ng, [&](const Seg& s, uint32_t gq, uint32_t gs, bool real) {
         const uint32_t mem = real ? lane - gs : 0u;
         const uint32_t x = real ? perm[s.begin + mem] : 0u;
-        uint64_t t = real ? ((uint64_t)gq << 58) | ((uint64_t)a.key[s.begin + mem] << 5) | lane : ~0ull;
+        const uint64_t key = !real ? 0ull : round0 ? dbl_round0_key(a, x, s.depth) : a.key[s.begin + mem];
+        uint64_t t = real ? ((uint64_t)gq << 58) | (key << 5) | lane : ~0ull;
 #pragma unroll
         for (uint32_t kk = 2; kk <= 32; kk <<= 1) {
 #pragma unroll
@@ -222,9 +243,9 @@ __global__ void k_dbl_sort_small(const Seg* __restrict__ list, uint32_t count,
             }
         }
         // groups keep their lane ranges: sorted by group first
-        const uint32_t K = (uint32_t)(t >> 5);
+        const uint64_t K = (t >> 5) & ((1ull << 53) - 1);  // the key (group bits dropped)
         const uint32_t mx = __shfl_sync(0xffffffffu, x, (uint32_t)t & 31u);
-        const uint32_t pk = __shfl_up_sync(0xffffffffu, K, 1);
+        const uint64_t pk = __shfl_up_sync(0xffffffffu, K, 1);
         const bool start = real && (lane == gs || pk != K);
         const uint32_t S = __ballot_sync(0xffffffffu, start);
         const uint32_t rs = 31u - __clz(S & (0xFFFFFFFFu >> (31 - lane)));
@@ -236,7 +257,8 @@ __global__ void k_dbl_sort_small(const Seg* __restrict__ list, uint32_t count,
         if (real) {
             perm[s.begin + mem] = mx;
             a.isa[mx] = s.begin + (rs - gs);  // final position for a single member
-            if (start) push = dbl_run(a, par, s, rs - gs, re - rs, K, &ns);
+            if (start)
+                push = dbl_run(a, par, s, rs - gs, re - rs, (uint32_t)K, &ns, round0 ? DBL_ROUND0_CHARS : 0u);
         }
         dbl_push_warp(a, counters, par ^ 1, push, ns);
     });
@@ -249,8 +271,9 @@ __global__ void k_dbl_sort_small(const Seg* __restrict__ list, uint32_t count,
 template <uint32_t MAXM>
 __global__ void __launch_bounds__(MAXM <= DBL_MID ? 256 : 512) k_dbl_sort_block(
     const Seg* __restrict__ list, uint32_t* __restrict__ perm, DblArrays a, uint32_t* counters,
-    int par)
+    int par, int round0)
 {
+    static_assert(MAXM <= (1u << (64 - 8 * DBL_ROUND0_CHARS)), "member index beside round 0's key");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint64_t* sk = reinterpret_cast<uint64_t*>(smem_raw);
     uint32_t* sx = reinterpret_cast<uint32_t*>(smem_raw + 8 * MAXM);
@@ -260,8 +283,10 @@ __global__ void __launch_bounds__(MAXM <= DBL_MID ? 256 : 512) k_dbl_sort_block(
     while (S < m) S <<= 1;
     for (uint32_t q = threadIdx.x; q < S; q += blockDim.x) {
         if (q < m) {
-            sx[q] = perm[s.begin + q];
-            sk[q] = ((uint64_t)a.key[s.begin + q] << 32) | q;
+            const uint32_t x = perm[s.begin + q];
+            sx[q] = x;
+            sk[q] = round0 ? (dbl_round0_key(a, x, s.depth) << (64 - 8 * DBL_ROUND0_CHARS)) | q
+                           : ((uint64_t)a.key[s.begin + q] << 32) | q;
         } else {
             sk[q] = ~0ull;
         }
@@ -274,14 +299,15 @@ __global__ void __launch_bounds__(MAXM <= DBL_MID ? 256 : 512) k_dbl_sort_block(
         bool push = false;
         Seg ns{};
         if (i < m) {
-            const uint32_t K = (uint32_t)(sk[i] >> 32);
+            const uint32_t ksh = round0 ? 64 - 8 * DBL_ROUND0_CHARS : 32;
+            const uint64_t K = sk[i] >> ksh;
             perm[s.begin + i] = sx[(uint32_t)sk[i] & (MAXM - 1)];
-            if (i == 0 || (uint32_t)(sk[i - 1] >> 32) != K) {
+            if (i == 0 || (sk[i - 1] >> ksh) != K) {
                 // a run starts here: its length, then every member's rank
                 uint32_t e = i + 1;
-                while (e < m && (uint32_t)(sk[e] >> 32) == K) ++e;
+                while (e < m && (sk[e] >> ksh) == K) ++e;
                 for (uint32_t q = i; q < e; ++q) a.isa[sx[(uint32_t)sk[q] & (MAXM - 1)]] = s.begin + i;
-                push = dbl_run(a, par, s, i, e - i, K, &ns);
+                push = dbl_run(a, par, s, i, e - i, (uint32_t)K, &ns, round0 ? DBL_ROUND0_CHARS : 0u);
             }
         }
         dbl_push_warp(a, counters, par ^ 1, push, ns);

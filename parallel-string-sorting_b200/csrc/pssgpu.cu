@@ -368,6 +368,8 @@ static int run_doubling(Ctx* c, Work& w, uint32_t ndbl, cudaStream_t st, pssgpu_
     const uint32_t n = w.n;
     const uint64_t capn = c->cap.n;
     DblArrays a{};
+    a.text = w.chars;
+    a.ntext = w.nchars;
     a.isa = reinterpret_cast<uint32_t*>(w.keys[0]);
     a.gd[0] = a.isa + capn;
     a.gd[1] = reinterpret_cast<uint32_t*>(w.keys[1]);
@@ -387,7 +389,7 @@ static int run_doubling(Ctx* c, Work& w, uint32_t ndbl, cudaStream_t st, pssgpu_
     auto* members = reinterpret_cast<unsigned long long*>(w.counters + C_DBL_MEMB);
     PSS_CUDA(cudaMemsetAsync(w.counters + C_DBL_CNT, 0, 4 * (C_COUNT - C_DBL_CNT), st));
     PSS_CUDA(cudaMemsetAsync(taken, 0, n, st));
-    k_dbl_init<<<gblocks, 256, 0, st>>>(w, w.dbl, ndbl, a, taken, w.counters);
+    k_dbl_init<<<gblocks, 256, 0, st>>>(w, w.dbl, ndbl, a, taken, w.counters, members);
     if (a.lb) PSS_CUDA(cudaMemsetAsync(a.lb, 0xFF, 4ull * n, st));
     k_dbl_isa<<<1184, 256, 0, st>>>(w.perm, n, taken, a.isa);
     stats.kernel_launches += 2;
@@ -406,23 +408,30 @@ static int run_doubling(Ctx* c, Work& w, uint32_t ndbl, cudaStream_t st, pssgpu_
         if (!cnt[0] && !cnt[1] && !cnt[2]) break;
         if (round >= MAX_ROUNDS) return fail(PSSGPU_ETIMEOUT, "rank doubling round limit exceeded");
         PSS_CUDA(cudaMemsetAsync(w.counters + C_DBL_CNT + 3 * (par ^ 1), 0, 12, st));
-        if (cnt[0])
-            k_dbl_keys_small<<<(cnt[0] + 255) / 256, 256, 0, st>>>(a.list[0][par], cnt[0], w.perm, a, members);
-        for (int k = 1; k < 3; ++k)
-            if (cnt[k])
-                k_dbl_keys<<<(cnt[k] + 7) / 8, 256, 0, st>>>(a.list[k][par], cnt[k], w.perm, a, members);
+        // round 0 sorts by text chars (dbl_round0_key); later rounds by the
+        // ranks of one snapshot, read first
+        const int round0 = round == 0;
+        if (!round0) {
+            if (cnt[0])
+                k_dbl_keys_small<<<(cnt[0] + 255) / 256, 256, 0, st>>>(a.list[0][par], cnt[0], w.perm, a,
+                                                                       members);
+            for (int k = 1; k < 3; ++k)
+                if (cnt[k])
+                    k_dbl_keys<<<(cnt[k] + 7) / 8, 256, 0, st>>>(a.list[k][par], cnt[k], w.perm, a, members);
+        }
         if (cnt[0]) {
             constexpr uint32_t per_block = 8 * DBL_PER_WARP;  // 8 warps
             k_dbl_sort_small<<<(cnt[0] + per_block - 1) / per_block, 256, 0, st>>>(
-                a.list[0][par], cnt[0], w.perm, a, w.counters, par);
+                a.list[0][par], cnt[0], w.perm, a, w.counters, par, round0);
         }
         if (cnt[1])
             k_dbl_sort_block<DBL_MID><<<cnt[1], 256, 12 * DBL_MID, st>>>(a.list[1][par], w.perm, a,
-                                                                         w.counters, par);
+                                                                         w.counters, par, round0);
         if (cnt[2])
             k_dbl_sort_block<DBL_MAX><<<cnt[2], 512, 12 * DBL_MAX, st>>>(a.list[2][par], w.perm, a,
-                                                                         w.counters, par);
-        const uint32_t launched = (cnt[0] ? 2 : 0) + (cnt[1] ? 2 : 0) + (cnt[2] ? 2 : 0);
+                                                                         w.counters, par, round0);
+        const uint32_t per_class = round0 ? 1 : 2;  // (keys and) sort
+        const uint32_t launched = (cnt[0] ? per_class : 0) + (cnt[1] ? per_class : 0) + (cnt[2] ? per_class : 0);
         stats.kernel_launches += launched;
         c->kstat[K_DBL].launches += launched;
         PSS_CUDA(cudaGetLastError());

@@ -2,18 +2,23 @@
 (csrc/kernels_suffix.cuh), checked against sorting the suffixes outright.
 
 The model follows the kernels' rules step by step: groups of equal 8-char
-prefixes are handed over at depth 8; every suffix's rank is its final
-position or its group's start; a round reads the ranks and group depths of
-one snapshot, sorts each group by the rank of its members' suffixes `depth`
-chars further, gives singletons their position and runs of equal ranks a
-subgroup of depth `depth + depth of the tied group`; positions separated in
-a round record that depth, and the LCPs there come from the larger of that
-depth and the previous suffix's LCP minus one. Small texts, pure Python: the
+prefixes are handed over at depth 8; round 0 sorts each group by the 6 text
+chars that follow its shared prefix, giving runs of equal chars a subgroup 6
+chars deeper; every suffix's rank is then its final position or its group's
+start; each later round reads the ranks and group depths of one snapshot,
+sorts each group by the rank of its members' suffixes `depth` chars further,
+gives singletons their position and runs of equal ranks a subgroup of depth
+`depth + depth of the tied group`; positions separated in a round record
+that depth, and the LCPs there come from the larger of that depth and the
+previous suffix's LCP minus one. Small texts, pure Python: the
 method, not the kernels, is under test here (the kernels are checked against
 the oracle by the GPU tests).
 """
 import numpy as np
 import pytest
+
+
+ROUND0_CHARS = 6  # DBL_ROUND0_CHARS of the kernels
 
 
 def doubling_model(text: bytes, split_above: int = 0):
@@ -64,8 +69,12 @@ def doubling_model(text: bytes, split_above: int = 0):
     lb = [None] * n
     par, rounds = 0, 0
     while groups:
+        round0 = rounds == 0
         rounds += 1
-        keys = {q: isa[sa[q] + d] for b, m, d in groups for q in range(b, b + m)}  # snapshot
+        if round0:  # the text chars behind the shared prefix
+            keys = {q: s(sa[q])[d:d + ROUND0_CHARS] for b, m, d in groups for q in range(b, b + m)}
+        else:       # ranks of one snapshot
+            keys = {q: isa[sa[q] + d] for b, m, d in groups for q in range(b, b + m)}
         nxt = []
         gd[par ^ 1] = {}
         for b, m, d in groups:
@@ -84,7 +93,7 @@ def doubling_model(text: bytes, split_above: int = 0):
                 for q in range(i, e):
                     isa[order[q][1]] = b + i
                 if e - i >= 2:
-                    nd = d + gd[par][K]
+                    nd = d + (ROUND0_CHARS if round0 else gd[par][K])
                     gd[par ^ 1][b + i] = nd
                     nxt.append((b + i, e - i, nd))
                 i = e

@@ -255,8 +255,11 @@ __global__ void k_dbl_sort_small(const Seg* __restrict__ list, uint32_t count,
         bool push = false;
         Seg ns{};
         if (real) {
-            perm[s.begin + mem] = mx;
-            a.isa[mx] = s.begin + (rs - gs);  // final position for a single member
+            // unchanged values are not written back: a member that kept its
+            // place keeps its perm entry, and after round 0 (which writes
+            // every rank) a run at its group's start keeps the group's rank
+            if (mx != x) perm[s.begin + mem] = mx;
+            if (round0 || rs != gs) a.isa[mx] = s.begin + (rs - gs);  // final position for a single member
             if (start)
                 push = dbl_run(a, par, s, rs - gs, re - rs, (uint32_t)K, &ns, round0 ? DBL_ROUND0_CHARS : 0u);
         }
@@ -301,12 +304,15 @@ __global__ void __launch_bounds__(MAXM <= DBL_MID ? 256 : 512) k_dbl_sort_block(
         if (i < m) {
             const uint32_t ksh = round0 ? 64 - 8 * DBL_ROUND0_CHARS : 32;
             const uint64_t K = sk[i] >> ksh;
-            perm[s.begin + i] = sx[(uint32_t)sk[i] & (MAXM - 1)];
+            const uint32_t src = (uint32_t)sk[i] & (MAXM - 1);
+            if (src != i) perm[s.begin + i] = sx[src];  // unchanged entries are not rewritten
             if (i == 0 || (sk[i - 1] >> ksh) != K) {
                 // a run starts here: its length, then every member's rank
+                // (after round 0 a run at the group's start keeps its rank)
                 uint32_t e = i + 1;
                 while (e < m && (sk[e] >> ksh) == K) ++e;
-                for (uint32_t q = i; q < e; ++q) a.isa[sx[(uint32_t)sk[q] & (MAXM - 1)]] = s.begin + i;
+                if (round0 || i)
+                    for (uint32_t q = i; q < e; ++q) a.isa[sx[(uint32_t)sk[q] & (MAXM - 1)]] = s.begin + i;
                 push = dbl_run(a, par, s, i, e - i, (uint32_t)K, &ns, round0 ? DBL_ROUND0_CHARS : 0u);
             }
         }

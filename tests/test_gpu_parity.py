@@ -189,21 +189,27 @@ def _suffix_text(case):
         t = bytes(np.random.default_rng(51).integers(97, 99, 60000, dtype=np.uint8))
     elif case == "runs_of_a":
         t = b"a" * 12000 + b"b" + b"a" * 3000
+    elif case == "high_bytes":
+        # chars 1..255 (round 0's text-char keys compare them unsigned), with
+        # repeats of 10 KB and 1 KB so that groups reach the doubling
+        r = bytes(np.random.default_rng(54).integers(1, 256, 20000, dtype=np.uint8))
+        t = r + r[5000:15000] + r[:1000] * 3 + r
     else:  # an inner NUL: not a suffix set, sorted as strings
         t = bytes(np.random.default_rng(52).integers(97, 100, 30000, dtype=np.uint8))
         t = t[:15000] + b"\0" + t[15001:]
     return np.frombuffer(t + b"\0", dtype=np.uint8).copy()
 
 
-@pytest.mark.parametrize("case", ["periodic", "dna_copies", "binary", "runs_of_a", "inner_nul"])
+@pytest.mark.parametrize("case", ["periodic", "dna_copies", "binary", "runs_of_a", "high_bytes",
+                                  "inner_nul"])
 @pytest.mark.parametrize("with_lcp", [True, False])
 def test_suffix_doubling(pkg, orc, case, with_lcp):
     """Suffix sets through the multi-launch path, where groups sharing 8 or
     more chars finish by rank doubling: a periodic text (groups of thousands,
     LCPs up to the text length), a DNA text with copied 1-10 KiB blocks, a
-    binary text, long runs of one char, and a text with a NUL inside (not a
-    suffix set: the string path). Checked against the oracle; the doubling
-    must have run for the suffix sets."""
+    binary text, long runs of one char, chars 1..255 with repeats, and a text
+    with a NUL inside (not a suffix set: the string path). Checked against
+    the oracle; the doubling must have run for the suffix sets."""
     if case == "dna_copies":
         chars = pkg.workloads.dna_text(length=1 << 20, seed=53)[: (1 << 20) + 1].copy()
     else:

@@ -176,7 +176,18 @@ __global__ void k_dbl_keys_small(const Seg* __restrict__ list, uint32_t count,
     const Seg s = g < count ? list[g] : Seg{0u, 0u, 0u, 0u};
     const uint32_t m = __reduce_add_sync(0xFFFFFFFFu, s.size);
     if ((threadIdx.x & 31) == 0 && m) atomicAdd(members, (unsigned long long)m);
-    for (uint32_t q = 0; q < s.size; ++q) a.key[s.begin + q] = a.isa[perm[s.begin + q] + s.depth];
+    // four members at a time: their ids, then their ranks, all in flight
+    // together (stores to key would otherwise order every next load)
+    for (uint32_t q = 0; q < s.size; q += 4) {
+        uint32_t x[4], r[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) x[j] = q + j < s.size ? __ldg(perm + s.begin + q + j) : 0u;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) r[j] = q + j < s.size ? a.isa[x[j] + s.depth] : 0u;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (q + j < s.size) a.key[s.begin + q + j] = r[j];
+    }
 }
 
 __global__ void k_dbl_keys(const Seg* __restrict__ list, uint32_t count,

@@ -90,8 +90,9 @@ int pssgpu_ctx_kernel_stats(pssgpu_ctx* ctx, pssgpu_kernel_stats* out, int max);
 /* Context options. PSSGPU_OPT_PROFILE: as pssgpu_ctx_set_profile.
  * PSSGPU_OPT_INDIRECT_HANDLES: carry bare string ids through the sort and
  * read offsets from the offset array at every gather -- the path a sort takes
- * on its own when an id and an arena offset do not fit one 64-bit handle;
- * for testing that path on small inputs.
+ * on its own when an id and an arena offset do not fit one 64-bit handle,
+ * and a merge when the arena exceeds 4 GiB; for testing those paths on small
+ * inputs.
  * PSSGPU_OPT_SINGLE_LAUNCH (default 1): a single-instance sort whose strings
  * fit one wave of resident blocks (about 1.2 M strings on a B200) runs as one
  * cooperative kernel launch, with no host round trip between its steps;

@@ -68,6 +68,62 @@ __device__ __forceinline__ uint32_t pair_of(const uint64_t* first, uint32_t npai
     return lo;
 }
 
+// How a round reads its runs. MergeByIds: the entries are string ids and
+// a string's arena offset is gathered through offs at each use.
+// MergeByHandles: the entries are handles (id << hbits | offset), made once
+// by k_merge_pack, so the offset comes with the entry a round reads in order
+// and no round gathers offsets.
+struct MergeByIds {
+    using T = uint32_t;
+    const uint64_t* offs;
+    __device__ __forceinline__ uint64_t off(uint32_t v) const { return __ldg(offs + v); }
+};
+struct MergeByHandles {
+    using T = uint64_t;
+    uint64_t hmask;
+    __device__ __forceinline__ uint64_t off(uint64_t v) const { return v & hmask; }
+};
+
+// Sequential reads of an array 16 bytes at a time: a thread that walks its
+// own stretch of entries or LCPs keeps the last aligned 16-byte block in
+// registers instead of fetching a sector per entry (the threads' streams are
+// too many for the caches to keep their lines). The array must be 16-byte
+// aligned and readable up to the next 16-byte boundary past its end.
+template <class T>
+struct SeqRead;
+template <>
+struct SeqRead<uint32_t> {
+    const uint32_t* base;
+    uint64_t blk = ~0ull;
+    uint4 v{};
+    __device__ __forceinline__ uint32_t get(uint64_t i)
+    {
+        const uint64_t b = i >> 2;
+        if (b != blk) {
+            v = __ldg(reinterpret_cast<const uint4*>(base + (b << 2)));
+            blk = b;
+        }
+        const uint32_t k = (uint32_t)(i & 3);
+        return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w;
+    }
+};
+template <>
+struct SeqRead<uint64_t> {
+    const uint64_t* base;
+    uint64_t blk = ~0ull;
+    ulonglong2 v{};
+    __device__ __forceinline__ uint64_t get(uint64_t i)
+    {
+        const uint64_t b = i >> 1;
+        if (b != blk) {
+            v = __ldg(reinterpret_cast<const ulonglong2*>(base + (b << 1)));
+            blk = b;
+        }
+        return (i & 1) ? v.y : v.x;
+    }
+};
+using SeqRead4 = SeqRead<uint32_t>;
+
 // Splits in two launches: coarse = 1 searches every MERGE_SPLIT_COARSE-th
 // piece of a pair over the whole diagonal; coarse = 0 searches the other
 // pieces between the two coarse splits around them. The merge path is a
@@ -76,10 +132,11 @@ __device__ __forceinline__ uint32_t pair_of(const uint64_t* first, uint32_t npai
 // a window of at most MERGE_SPLIT_COARSE * piece positions.
 constexpr uint32_t MERGE_SPLIT_COARSE = 32;
 
-__global__ void k_merge_split(const uint8_t* __restrict__ chars, uint64_t nchars,
-                              const uint64_t* __restrict__ offs, const MergePair* __restrict__ pairs,
+template <class V>
+__global__ void k_merge_split(const uint8_t* __restrict__ chars, uint64_t nchars, V view,
+                              const MergePair* __restrict__ pairs,
                               const uint64_t* __restrict__ first, uint32_t npair,
-                              const uint32_t* __restrict__ ids_in, uint64_t* __restrict__ split,
+                              const typename V::T* __restrict__ in, uint64_t* __restrict__ split,
                               uint32_t piece, int coarse)
 {
     const uint64_t ntask = first[npair];
@@ -105,8 +162,8 @@ __global__ void k_merge_split(const uint8_t* __restrict__ chars, uint64_t nchars
         while (lo < hi) {
             const int64_t mid = (lo + hi) >> 1;
             uint32_t l;
-            const int c = compare_lcp(chars, nchars, __ldg(offs + ids_in[pr.a0 + mid]),
-                                      __ldg(offs + ids_in[pr.a1 + d - mid - 1]), &l);
+            const int c = compare_lcp(chars, nchars, view.off(in[pr.a0 + mid]),
+                                      view.off(in[pr.a1 + d - mid - 1]), &l);
             if (c <= 0) lo = mid + 1; else hi = mid;
         }
         split[t] = (uint64_t)lo;
@@ -114,11 +171,12 @@ __global__ void k_merge_split(const uint8_t* __restrict__ chars, uint64_t nchars
 }
 
 // Piece merge without LCP arrays: every pair compares from char 0.
-__global__ void k_merge_seq(const uint8_t* __restrict__ chars, uint64_t nchars,
-                            const uint64_t* __restrict__ offs, const MergePair* __restrict__ pairs,
+template <class V>
+__global__ void k_merge_seq(const uint8_t* __restrict__ chars, uint64_t nchars, V view,
+                            const MergePair* __restrict__ pairs,
                             const uint64_t* __restrict__ first, uint32_t npair,
-                            const uint64_t* __restrict__ split, const uint32_t* __restrict__ ids_in,
-                            uint32_t* __restrict__ ids_out, uint32_t piece)
+                            const uint64_t* __restrict__ split, const typename V::T* __restrict__ in,
+                            typename V::T* __restrict__ out, uint32_t piece)
 {
     const uint64_t ntask = first[npair];
     for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ntask;
@@ -138,62 +196,42 @@ __global__ void k_merge_seq(const uint8_t* __restrict__ chars, uint64_t nchars,
             else if (j >= j1) take_a = true;
             else {
                 uint32_t l;
-                take_a = compare_lcp(chars, nchars, __ldg(offs + ids_in[pr.a0 + i]),
-                                     __ldg(offs + ids_in[pr.a1 + j]), &l) <= 0;
+                take_a = compare_lcp(chars, nchars, view.off(in[pr.a0 + i]), view.off(in[pr.a1 + j]),
+                                     &l) <= 0;
             }
-            ids_out[pr.a0 + d] = take_a ? ids_in[pr.a0 + i] : ids_in[pr.a1 + j];
+            out[pr.a0 + d] = take_a ? in[pr.a0 + i] : in[pr.a1 + j];
             if (take_a) ++i; else ++j;
         }
     }
 }
 
-// Sequential reads of a u32 array 16 bytes at a time: a thread that walks
-// its own stretch of ids or LCPs keeps the last aligned 4-word block in
-// registers instead of fetching a sector per word (the threads' streams are
-// too many for the caches to keep their lines). The array must be 16-byte
-// aligned and readable up to the next multiple of 4 words past its end.
-struct SeqRead4 {
-    const uint32_t* base;
-    uint64_t blk = ~0ull;
-    uint4 v{};
-    __device__ __forceinline__ uint32_t get(uint64_t i)
-    {
-        const uint64_t b = i >> 2;
-        if (b != blk) {
-            v = __ldg(reinterpret_cast<const uint4*>(base + (b << 2)));
-            blk = b;
-        }
-        const uint32_t k = (uint32_t)(i & 3);
-        return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w;
-    }
-};
-
 // LCP-aware piece merge (the reference's LCP loser-tree rule for two runs).
-// Runs A = ids_in[a0, a1) and B = ids_in[a1, b1) with their LCP arrays in
-// lcp_in (entries at a run's first position are not read). ha / hb are the
-// LCPs of the heads A[i] / B[j] with the last output. A piece that does not
-// start the pair first finds its previous output (the larger of A[i0 - 1]
-// and B[j0 - 1]; equal strings: B's, as A's comes first) and the heads' LCPs
+// Runs A = in[a0, a1) and B = in[a1, b1) with their LCP arrays in lcp_in
+// (entries at a run's first position are not read). ha / hb are the LCPs of
+// the heads A[i] / B[j] with the last output. A piece that does not start
+// the pair first finds its previous output (the larger of A[i0 - 1] and
+// B[j0 - 1]; equal strings: B's, as A's comes first) and the heads' LCPs
 // with it. lcp_out (may be null) receives the LCP of every output but the
 // pair's first.
-__global__ void k_merge_lcp_seq(const uint8_t* __restrict__ chars, uint64_t nchars,
-                                const uint64_t* __restrict__ offs,
+template <class V>
+__global__ void __launch_bounds__(256, 4) k_merge_lcp_seq(const uint8_t* __restrict__ chars, uint64_t nchars, V view,
                                 const MergePair* __restrict__ pairs,
                                 const uint64_t* __restrict__ first, uint32_t npair,
                                 const uint64_t* __restrict__ split,
-                                const uint32_t* __restrict__ ids_in,
+                                const typename V::T* __restrict__ in,
                                 const uint32_t* __restrict__ lcp_in,
-                                uint32_t* __restrict__ ids_out, uint32_t* __restrict__ lcp_out,
+                                typename V::T* __restrict__ out, uint32_t* __restrict__ lcp_out,
                                 uint32_t piece)
 {
+    using T = typename V::T;
     const uint64_t ntask = first[npair];
     for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ntask;
          t += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t p = pair_of(first, npair, t);
         const MergePair pr = pairs[p];
         const uint64_t na = pr.a1 - pr.a0, nb = pr.b1 - pr.a1;
-        const uint32_t* A = ids_in + pr.a0;
-        const uint32_t* B = ids_in + pr.a1;
+        const T* A = in + pr.a0;
+        const T* B = in + pr.a1;
         const uint32_t* LA = lcp_in + pr.a0;
         const uint32_t* LB = lcp_in + pr.a1;
         const uint64_t d0 = (t - first[p]) * piece;
@@ -206,34 +244,32 @@ __global__ void k_merge_lcp_seq(const uint8_t* __restrict__ chars, uint64_t ncha
         if (d0 > 0) {
             if (i0 == 0) {  // previous output B[j0 - 1]
                 hb = j < nb ? LB[j] : 0u;
-                if (i < na) compare_from(chars, nchars, __ldg(offs + A[i]), __ldg(offs + B[j - 1]), 0, &ha);
+                if (i < na) compare_from(chars, nchars, view.off(A[i]), view.off(B[j - 1]), 0, &ha);
             } else if (j0 == 0) {  // previous output A[i0 - 1]
                 ha = i < na ? LA[i] : 0u;
-                if (j < nb) compare_from(chars, nchars, __ldg(offs + B[j]), __ldg(offs + A[i - 1]), 0, &hb);
+                if (j < nb) compare_from(chars, nchars, view.off(B[j]), view.off(A[i - 1]), 0, &hb);
             } else {
                 uint32_t l;
-                const int c = compare_from(chars, nchars, __ldg(offs + A[i - 1]),
-                                           __ldg(offs + B[j - 1]), 0, &l);
+                const int c = compare_from(chars, nchars, view.off(A[i - 1]), view.off(B[j - 1]), 0, &l);
                 // LCP(x, z) >= min(LCP(x, y), LCP(y, z)): start from that depth
                 if (c <= 0) {  // previous output B[j0 - 1]
                     hb = j < nb ? LB[j] : 0u;
                     if (i < na)
-                        compare_from(chars, nchars, __ldg(offs + A[i]), __ldg(offs + B[j - 1]),
-                                     min(LA[i], l), &ha);
+                        compare_from(chars, nchars, view.off(A[i]), view.off(B[j - 1]), min(LA[i], l), &ha);
                 } else {       // previous output A[i0 - 1]
                     ha = i < na ? LA[i] : 0u;
                     if (j < nb)
-                        compare_from(chars, nchars, __ldg(offs + B[j]), __ldg(offs + A[i - 1]),
-                                     min(LB[j], l), &hb);
+                        compare_from(chars, nchars, view.off(B[j]), view.off(A[i - 1]), min(LB[j], l), &hb);
                 }
             }
         }
-        // the heads' ids and arena offsets stay in registers: one offset
-        // load per output, and a compare reads chars only; the runs' ids and
-        // LCPs are read 16 bytes at a time
-        SeqRead4 ra{ids_in}, rb{ids_in}, la{lcp_in}, lb{lcp_in};
-        uint32_t ida = i < i1 ? ra.get(pr.a0 + i) : 0u, idb = j < j1 ? rb.get(pr.a1 + j) : 0u;
-        uint64_t oa = i < i1 ? __ldg(offs + ida) : 0ull, ob = j < j1 ? __ldg(offs + idb) : 0ull;
+        // the heads' entries and arena offsets stay in registers: a compare
+        // reads chars only; the runs' entries and LCPs are read 16 bytes at
+        // a time
+        SeqRead<T> ra{in}, rb{in};
+        SeqRead4 la{lcp_in}, lb{lcp_in};
+        T va = i < i1 ? ra.get(pr.a0 + i) : T(0), vb = j < j1 ? rb.get(pr.a1 + j) : T(0);
+        uint64_t oa = i < i1 ? view.off(va) : 0ull, ob = j < j1 ? view.off(vb) : 0ull;
         for (uint64_t d = d0; d < d1; ++d) {
             bool take_a;
             if (i >= i1) take_a = false;
@@ -244,25 +280,49 @@ __global__ void k_merge_lcp_seq(const uint8_t* __restrict__ chars, uint64_t ncha
                 take_a = compare_from(chars, nchars, oa, ob, ha, &l) <= 0;
                 if (take_a) hb = l; else ha = l;  // the loser's LCP with the new last output
             }
-            ids_out[pr.a0 + d] = take_a ? ida : idb;
+            out[pr.a0 + d] = take_a ? va : vb;
             if (lcp_out && d > 0) lcp_out[pr.a0 + d] = take_a ? ha : hb;
             if (take_a) {
                 ++i;
                 ha = i < na ? la.get(pr.a0 + i) : 0u;  // against its predecessor, the last output
                 if (i < i1) {
-                    ida = ra.get(pr.a0 + i);
-                    oa = __ldg(offs + ida);
+                    va = ra.get(pr.a0 + i);
+                    oa = view.off(va);
                 }
             } else {
                 ++j;
                 hb = j < nb ? lb.get(pr.a1 + j) : 0u;
                 if (j < j1) {
-                    idb = rb.get(pr.a1 + j);
-                    ob = __ldg(offs + idb);
+                    vb = rb.get(pr.a1 + j);
+                    ob = view.off(vb);
                 }
             }
         }
     }
+}
+
+// Handles of the runs' strings (32-bit id << hbits | arena offset, offsets
+// below 2^hbits <= 2^32), with the arena check of k_merge_check.
+__global__ void k_merge_pack(const uint64_t* __restrict__ offs, uint64_t nchars,
+                             const uint32_t* __restrict__ ids, uint64_t n, uint32_t hbits,
+                             uint64_t* __restrict__ out, uint32_t* err)
+{
+    for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n;
+         q += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t id = ids[q];
+        const uint64_t o = __ldg(offs + id);
+        if (o >= nchars) atomicOr(err, ERR_OFFSET);
+        out[q] = ((uint64_t)id << hbits) | (o < nchars ? o : 0ull);
+    }
+}
+
+// The ids of merged handles.
+__global__ void k_merge_unpack(const uint64_t* __restrict__ h, uint64_t n, uint32_t hbits,
+                               uint32_t* __restrict__ ids)
+{
+    for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n;
+         q += (uint64_t)gridDim.x * blockDim.x)
+        ids[q] = (uint32_t)(h[q] >> hbits);
 }
 
 // Every id's offset must lie inside the arena (offsets >= nchars: *err).

@@ -1636,53 +1636,86 @@ int pssgpu_merge_lcp_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nc
         npairs.push_back(np);
         max_tasks = std::max(max_tasks, t);
     }
-    const uint64_t b_v = align256(4 * n), b_runs = align256(8 * flat.size());
-    const uint64_t b_split = align256(8 * (max_tasks + 1));
-    if ((rc = ensure_buf(&c->mbuf, &c->mbuf_bytes, 4 * b_v + b_runs + b_split + 256))) return rc;
-    uint32_t* tid[2] = {(uint32_t*)c->mbuf, (uint32_t*)(c->mbuf + b_v)};
-    uint32_t* tlcp[2] = {(uint32_t*)(c->mbuf + 2 * b_v), (uint32_t*)(c->mbuf + 3 * b_v)};
-    uint64_t* d_flat = (uint64_t*)(c->mbuf + 4 * b_v);
-    uint64_t* split = (uint64_t*)(c->mbuf + 4 * b_v + b_runs);
-    uint32_t* d_err = (uint32_t*)(c->mbuf + 4 * b_v + b_runs + b_split);
+    // runs as handles (32-bit id << hbits | offset) when the offsets fit 32
+    // bits: made once, then every round reads offsets in order with the
+    // entries instead of gathering them; else as ids
+    const uint32_t hbits = std::max<uint32_t>(1, bit_length(nchars - 1));
+    const bool packed = hbits <= 32 && !c->indirect_handles;
+    const uint64_t b_v = align256(4 * n + 16), b_h = align256(8 * n + 16);
+    const uint64_t b_runs = align256(8 * flat.size()), b_split = align256(8 * (max_tasks + 1));
+    if ((rc = ensure_buf(&c->mbuf, &c->mbuf_bytes, 2 * b_h + 2 * b_v + b_runs + b_split + 256))) return rc;
+    unsigned char* tv[2] = {c->mbuf, c->mbuf + b_h};  // ids or handles, by round parity
+    uint32_t* tlcp[2] = {(uint32_t*)(c->mbuf + 2 * b_h), (uint32_t*)(c->mbuf + 2 * b_h + b_v)};
+    uint64_t* d_flat = (uint64_t*)(c->mbuf + 2 * b_h + 2 * b_v);
+    uint64_t* split = (uint64_t*)(c->mbuf + 2 * b_h + 2 * b_v + b_runs);
+    uint32_t* d_err = (uint32_t*)(c->mbuf + 2 * b_h + 2 * b_v + b_runs + b_split);
     PSS_CUDA(cudaMemcpyAsync(d_flat, flat.data(), 8 * flat.size(), cudaMemcpyHostToDevice, st));
     PSS_CUDA(cudaMemsetAsync(d_err, 0, 4, st));
     const unsigned blocks = (unsigned)std::min<uint64_t>((n + 255) / 256, 148ull * 16);
-    k_merge_check<<<blocks, 256, 0, st>>>(d_offs, nchars, d_ids, n, d_err);
     // with the runs' LCP arrays every round is LCP-aware and carries the
     // merged LCP array to the next one (the last round writes d_lcp_out, if
     // any). Its sequential reads take 16 bytes at a time, from the library's
-    // own buffers (aligned, padded): the caller's ids and LCPs are copied in.
+    // own buffers (aligned, padded): the caller's ids (as handles, or as
+    // they are) and LCPs are copied in; round 0 writes tv[0] and tlcp[0].
     const bool with_lcp = d_lcp != nullptr;
-    const uint32_t* in_ids = d_ids;
+    const unsigned char* in_v = (const unsigned char*)d_ids;
     const uint32_t* in_lcp = d_lcp;
+    if (packed) {
+        k_merge_pack<<<blocks, 256, 0, st>>>(d_offs, nchars, d_ids, n, hbits, (uint64_t*)tv[1], d_err);
+        in_v = tv[1];
+    } else {
+        k_merge_check<<<blocks, 256, 0, st>>>(d_offs, nchars, d_ids, n, d_err);
+        if (with_lcp) {
+            PSS_CUDA(cudaMemcpyAsync(tv[1], d_ids, 4 * n, cudaMemcpyDeviceToDevice, st));
+            in_v = tv[1];
+        }
+    }
     if (with_lcp) {
-        // round 0 writes tid[0], so the copies go to the other buffers
-        PSS_CUDA(cudaMemcpyAsync(tid[1], d_ids, 4 * n, cudaMemcpyDeviceToDevice, st));
         PSS_CUDA(cudaMemcpyAsync(tlcp[1], d_lcp, 4 * n, cudaMemcpyDeviceToDevice, st));
-        in_ids = tid[1];
         in_lcp = tlcp[1];
     }
+    const MergeByIds by_ids{d_offs};
+    const MergeByHandles by_h{(1ull << hbits) - 1};
     for (size_t i = 0; i < rounds; ++i) {
         const bool lastr = i + 1 == rounds;
-        uint32_t* out_ids = lastr ? d_ids_out : tid[i & 1];
+        // the last round writes the caller's ids directly unless it merges handles
+        unsigned char* out_v = lastr && !packed ? (unsigned char*)d_ids_out : tv[i & 1];
         uint32_t* out_lcp = lastr ? d_lcp_out : tlcp[i & 1];
         const MergePair* pairs = reinterpret_cast<const MergePair*>(d_flat + at_pairs[i]);
         const uint64_t* first = d_flat + at_first[i];
         const uint32_t np = (uint32_t)npairs[i];
         const uint32_t pc = c->merge_piece;
-        for (int coarse = 1; coarse >= 0; --coarse)
-            k_merge_split<<<blocks, 256, 0, st>>>(d_chars, nchars, d_offs, pairs, first, np, in_ids,
-                                                  split, pc, coarse);
-        if (with_lcp)
-            k_merge_lcp_seq<<<blocks, 256, 0, st>>>(d_chars, nchars, d_offs, pairs, first, np, split,
-                                                    in_ids, in_lcp, out_ids, out_lcp, pc);
-        else
-            k_merge_seq<<<blocks, 256, 0, st>>>(d_chars, nchars, d_offs, pairs, first, np, split,
-                                                in_ids, out_ids, pc);
+        if (packed) {
+            const uint64_t* in = (const uint64_t*)in_v;
+            uint64_t* out = (uint64_t*)out_v;
+            for (int coarse = 1; coarse >= 0; --coarse)
+                k_merge_split<MergeByHandles><<<blocks, 256, 0, st>>>(d_chars, nchars, by_h, pairs, first, np, in,
+                                                                      split, pc, coarse);
+            if (with_lcp)
+                k_merge_lcp_seq<MergeByHandles><<<blocks, 256, 0, st>>>(d_chars, nchars, by_h, pairs, first, np,
+                                                                        split, in, in_lcp, out, out_lcp, pc);
+            else
+                k_merge_seq<MergeByHandles><<<blocks, 256, 0, st>>>(d_chars, nchars, by_h, pairs, first, np,
+                                                                    split, in, out, pc);
+        } else {
+            const uint32_t* in = (const uint32_t*)in_v;
+            uint32_t* out = (uint32_t*)out_v;
+            for (int coarse = 1; coarse >= 0; --coarse)
+                k_merge_split<MergeByIds><<<blocks, 256, 0, st>>>(d_chars, nchars, by_ids, pairs, first, np, in,
+                                                                  split, pc, coarse);
+            if (with_lcp)
+                k_merge_lcp_seq<MergeByIds><<<blocks, 256, 0, st>>>(d_chars, nchars, by_ids, pairs, first, np,
+                                                                    split, in, in_lcp, out, out_lcp, pc);
+            else
+                k_merge_seq<MergeByIds><<<blocks, 256, 0, st>>>(d_chars, nchars, by_ids, pairs, first, np,
+                                                                split, in, out, pc);
+        }
         PSS_CUDA(cudaGetLastError());
-        in_ids = out_ids;
+        in_v = out_v;
         in_lcp = out_lcp;
     }
+    if (packed)
+        k_merge_unpack<<<blocks, 256, 0, st>>>((const uint64_t*)in_v, n, hbits, d_ids_out);
     uint32_t err = 0;
     PSS_CUDA(cudaMemcpyAsync(&err, d_err, 4, cudaMemcpyDeviceToHost, st));
     PSS_CUDA(cudaStreamSynchronize(st));

@@ -525,6 +525,35 @@ def test_merge_lcp(pkg, orc, ctx, K, case):
         check_against_oracle(orc, chars, offs, perm, dlo.cpu().numpy().view(np.uint32))
 
 
+@pytest.mark.parametrize("K,case", [(3, "rand"), (4, "deep"), (2, "no_lcp"), (6, "no_lcp_input")])
+def test_merge_lcp_ids_path(pkg, orc, K, case):
+    """The merge rounds on string ids with offsets gathered at each use (the
+    form an arena over 4 GiB takes; PSSGPU_OPT_INDIRECT_HANDLES forces it
+    here) give the same results as the handle form."""
+    import torch
+    chars, offs = pkg.pack_strings(_merge_strings("deep" if case == "deep" else "rand"))
+    nchars = chars.shape[0]
+    ids, lcp, runs = _oracle_runs(orc, chars, offs, K, 190 + K)
+    dc = torch.from_numpy(np.concatenate([chars, np.zeros(16, np.uint8)])).cuda()
+    do = torch.from_numpy(offs.view(np.int64)).cuda()
+    di = torch.from_numpy(ids.view(np.int32)).cuda()
+    dl = torch.from_numpy(lcp.view(np.int32)).cuda() if case != "no_lcp_input" else None
+    dio = torch.empty_like(di)
+    dlo = torch.zeros_like(di) if case not in ("no_lcp", "no_lcp_input") else None
+    c = pkg.Context(0)
+    try:
+        c.set_option(c.OPT_INDIRECT_HANDLES, 1)
+        c.merge_lcp_device(dc, nchars, do, runs, di, dl, dio, dlo)
+    finally:
+        c.close()
+    perm = dio.cpu().numpy().view(np.uint32)
+    if dlo is None:
+        assert orc.check_permutation(perm)
+        assert orc.check_order(chars, offs, perm) == -1
+    else:
+        check_against_oracle(orc, chars, offs, perm, dlo.cpu().numpy().view(np.uint32))
+
+
 def test_merge_rejects_offsets_outside_the_arena(pkg, orc, ctx):
     import torch
     chars, offs = pkg.pack_strings([b"b", b"a", b"c", b"a"])

@@ -151,6 +151,7 @@ __global__ void k_merge_split(const uint8_t* __restrict__ chars, uint64_t nchars
         // left-run strings among the first d outputs: the first i with
         // A[i] > B[d - i - 1] (ties go to the left run)
         int64_t lo = d > nb ? (int64_t)(d - nb) : 0, hi = (int64_t)min(d, na);
+        uint32_t depth = 0;  // chars every compared pair shares
         if (!coarse) {
             const uint64_t k0 = k - k % MERGE_SPLIT_COARSE, k1 = k0 + MERGE_SPLIT_COARSE;
             const uint64_t D0 = k0 * piece, i0 = split[first[p] + k0];
@@ -158,12 +159,26 @@ __global__ void k_merge_split(const uint8_t* __restrict__ chars, uint64_t nchars
             const uint64_t D1 = last ? na + nb : k1 * piece, i1 = last ? na : split[first[p] + k1];
             lo = max(lo, max((int64_t)i0, (int64_t)d - (int64_t)D1 + (int64_t)i1));
             hi = min(hi, min((int64_t)i1, (int64_t)(d - D0 + i0)));
+            if (hi - lo > 2) {
+                // the search compares A[x], x in [lo, hi), with B[y], y in
+                // [d - hi, d - lo): a sorted run's extremes share no more
+                // than anything between them, so every such pair shares
+                // min(LCP(A[lo], A[hi - 1]), LCP(A[lo], B[d - hi]),
+                // LCP(B[d - hi], B[d - lo - 1])) chars
+                const uint64_t a_lo = view.off(in[pr.a0 + lo]), a_hi = view.off(in[pr.a0 + hi - 1]);
+                const uint64_t b_lo = view.off(in[pr.a1 + d - hi]), b_hi = view.off(in[pr.a1 + d - lo - 1]);
+                uint32_t l1, l2, l3;
+                compare_from(chars, nchars, a_lo, a_hi, 0, &l1);
+                compare_from(chars, nchars, b_lo, b_hi, 0, &l2);
+                compare_from(chars, nchars, a_lo, b_lo, 0, &l3);
+                depth = min(min(l1, l2), l3);
+            }
         }
         while (lo < hi) {
             const int64_t mid = (lo + hi) >> 1;
             uint32_t l;
-            const int c = compare_lcp(chars, nchars, view.off(in[pr.a0 + mid]),
-                                      view.off(in[pr.a1 + d - mid - 1]), &l);
+            const int c = compare_from(chars, nchars, view.off(in[pr.a0 + mid]),
+                                       view.off(in[pr.a1 + d - mid - 1]), depth, &l);
             if (c <= 0) lo = mid + 1; else hi = mid;
         }
         split[t] = (uint64_t)lo;

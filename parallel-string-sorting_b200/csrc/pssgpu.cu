@@ -1149,17 +1149,27 @@ static int sort_pointer_array(unsigned char** strings, unsigned char** out, uint
     std::lock_guard<std::mutex> lk(c->mu);
     const size_t parts = host_slices(n);
     // offsets, permutation and LCPs in the context's pinned buffer (copies at
-    // full PCIe speed, no page faults per call)
+    // full PCIe speed, no page faults per call), or in ordinary host memory
+    // when that much cannot be pinned
     const uint64_t need = 8ull * n + 4ull * n + (lcp_out ? 4ull * n : 0ull);
+    std::vector<uint64_t> unpinned;
+    unsigned char* hbuf = c->ptr_host;
     if (!c->ptr_host || c->ptr_host_bytes < need) {
         if (c->ptr_host) cudaFreeHost(c->ptr_host);
         c->ptr_host = nullptr;
         c->ptr_host_bytes = 0;
-        PSS_CUDA(cudaHostAlloc((void**)&c->ptr_host, need, cudaHostAllocDefault));
-        c->ptr_host_bytes = need;
+        if (cudaHostAlloc((void**)&c->ptr_host, need, cudaHostAllocDefault) == cudaSuccess) {
+            c->ptr_host_bytes = need;
+            hbuf = c->ptr_host;
+        } else {
+            cudaGetLastError();
+            c->ptr_host = nullptr;
+            unpinned.resize((need + 7) / 8);
+            hbuf = reinterpret_cast<unsigned char*>(unpinned.data());
+        }
     }
-    uint64_t* const offs = reinterpret_cast<uint64_t*>(c->ptr_host);
-    uint32_t* const perm = reinterpret_cast<uint32_t*>(c->ptr_host + 8ull * n);
+    uint64_t* const offs = reinterpret_cast<uint64_t*>(hbuf);
+    uint32_t* const perm = reinterpret_cast<uint32_t*>(hbuf + 8ull * n);
     uint32_t* const lcp32 = lcp_out ? perm + n : nullptr;
     std::vector<uint8_t> packed;
     const uint8_t* arena;

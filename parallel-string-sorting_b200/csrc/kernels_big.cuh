@@ -597,6 +597,43 @@ __device__ __forceinline__ void push_seg(Work& w, int nxt, Seg c)
     }
 }
 
+// push_seg for a whole warp: lanes with push set append c. One reservation
+// per class and warp, and the class's tile or string count added once (a
+// launch that pushes many segments would otherwise serialise on these few
+// counters).
+__device__ __forceinline__ void push_seg_warp(Work& w, int nxt, bool push, const Seg& c)
+{
+    const uint32_t lane = threadIdx.x & 31;
+    int cls = -1;
+    if (push)
+        cls = c.size > SMALL_MAX ? L_BIG : c.size > 256 ? L_SMALLB : c.size > WARP_GROUP_MAX ? L_SMALLA : L_TINY;
+#pragma unroll
+    for (int k = 0; k < L_NCLASS; ++k) {
+        const uint32_t m = __ballot_sync(0xffffffffu, cls == k);
+        if (!m) continue;
+        const int leader = __ffs(m) - 1;
+        const uint32_t tiles = cls == k && k == L_BIG ? (c.size + TILE - 1) / TILE : 0u;
+        const uint32_t amount = __reduce_add_sync(0xffffffffu, cls != k ? 0u : k == L_BIG ? tiles : c.size);
+        const uint32_t multi = __reduce_add_sync(0xffffffffu, tiles > (uint32_t)CHUNK ? 1u : 0u);
+        uint32_t base = 0;
+        if (lane == (uint32_t)leader) {
+            base = atomicAdd(w.counters + C_PAR * nxt + k, (uint32_t)__popc(m));
+            if (k == L_BIG) {
+                atomicAdd(w.counters + C_PAR * nxt + C_NTILES, amount);
+                if (multi) atomicAdd(w.counters + C_MULTI + nxt, multi);
+            } else {
+                atomicAdd(w.counters + C_PAR * nxt + C_NSTR + k, amount);
+            }
+        }
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (cls == k) {
+            const uint32_t at = base + __popc(m & ((1u << lane) - 1u));
+            if (at >= w.cap[k]) set_error(w.counters + C_ERR, ERR_OVERFLOW);
+            else w.list[k][nxt][at] = c;
+        }
+    }
+}
+
 // Children of each bucket, after the scatter has placed them (hpp:1492-1584):
 // '<' buckets keep their depth and keys, '=' buckets go 8 chars deeper or
 // are finished when their splitter ends the string. Behind a common-prefix

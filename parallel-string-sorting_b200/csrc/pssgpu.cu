@@ -62,23 +62,31 @@ __global__ void k_roots(Work w, const uint64_t* __restrict__ inst, uint32_t nins
         if (blockIdx.x == 0 && threadIdx.x == 0) push_seg(w, 0, Seg{0u, w.n, 0u, 0u});
         return;
     }
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < ninst; k += gridDim.x * blockDim.x) {
-        const uint32_t b = (uint32_t)inst[k], e = (uint32_t)inst[k + 1];
-        if (e - b >= 2) push_seg(w, 0, Seg{b, e - b, 0u, 0u});
-        else if (e - b == 1) w.perm[b] = b;
+    // warp-uniform trips, so that the list appends aggregate per warp
+    for (uint32_t k0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); k0 < ninst;
+         k0 += gridDim.x * blockDim.x) {
+        const uint32_t k = k0 + (threadIdx.x & 31);
+        uint32_t b = 0, e = 0;
+        if (k < ninst) {
+            b = (uint32_t)inst[k];
+            e = (uint32_t)inst[k + 1];
+        }
+        if (e - b == 1) w.perm[b] = b;
+        push_seg_warp(w, 0, e - b >= 2, Seg{b, e - b, 0u, 0u});
     }
 }
 
-// Batch output: ids relative to their instance.
 // Batch output: ids relative to their instance; the first LCP of every
-// instance is 0.
+// instance is 0. One warp per instance.
 __global__ void k_localize(uint32_t* __restrict__ perm, uint32_t* __restrict__ lcp,
                            const uint64_t* __restrict__ inst, uint32_t ninst)
 {
-    for (uint32_t k = blockIdx.x; k < ninst; k += gridDim.x) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < ninst; k += nw) {
         const uint32_t b = (uint32_t)inst[k], e = (uint32_t)inst[k + 1];
-        for (uint32_t p = b + threadIdx.x; p < e; p += blockDim.x) perm[p] -= b;
-        if (lcp && threadIdx.x == 0 && e > b) lcp[b] = 0;
+        for (uint32_t p = b + lane; p < e; p += 32) perm[p] -= b;
+        if (lcp && lane == 0 && e > b) lcp[b] = 0;
     }
 }
 
@@ -519,7 +527,8 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
         PSS_CUDA(cudaMemsetAsync(w.counters, 0, 4 * C_COUNT, st));
         kt.begin(K_INIT);
         k_init<<<1184, 256, 0, st>>>(w);
-        k_roots<<<d_inst ? 148 : 1, 256, 0, st>>>(w, d_inst, ninst);
+        k_roots<<<d_inst ? std::max(1u, std::min((ninst + 255) / 256, 148u * 16u)) : 1u, 256, 0, st>>>(
+            w, d_inst, ninst);
         // every string a suffix of one text (n == nchars is necessary)?
         if (suffix_try) k_suffix_check<<<1184, 256, 0, st>>>(chars, offs, n, w.counters + C_SFX);
         kt.end(K_INIT);
@@ -738,7 +747,7 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
         stats.kernel_launches += 1;
     }
     if (!err && d_inst) {
-        k_localize<<<1184, 256, 0, st>>>(perm, lcp, d_inst, ninst);
+        k_localize<<<std::max(1u, std::min((ninst + 7) / 8, 148u * 64u)), 256, 0, st>>>(perm, lcp, d_inst, ninst);
         stats.kernel_launches += 1;
     }
     PSS_CUDA(cudaEventRecord(c->ev1, st));

@@ -77,16 +77,41 @@ __global__ void k_roots(Work w, const uint64_t* __restrict__ inst, uint32_t nins
 }
 
 // Batch output: ids relative to their instance; the first LCP of every
-// instance is 0. One warp per instance.
-__global__ void k_localize(uint32_t* __restrict__ perm, uint32_t* __restrict__ lcp,
-                           const uint64_t* __restrict__ inst, uint32_t ninst)
+// instance is 0. Blocks take chunks of LOC_CHUNK positions (work follows
+// the strings, whether a batch holds many small instances or a few large
+// ones): the instances overlapping a chunk are found once, and each position
+// finds its own among them.
+constexpr uint32_t LOC_CHUNK = 4096;
+
+// last k in [lo, hi] with inst[k] <= p (inst[lo] <= p)
+__device__ __forceinline__ uint32_t last_inst_at_or_below(const uint64_t* inst, uint32_t lo, uint32_t hi,
+                                                          uint64_t p)
 {
-    const uint32_t lane = threadIdx.x & 31;
-    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < ninst; k += nw) {
-        const uint32_t b = (uint32_t)inst[k], e = (uint32_t)inst[k + 1];
-        for (uint32_t p = b + lane; p < e; p += 32) perm[p] -= b;
-        if (lcp && lane == 0 && e > b) lcp[b] = 0;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (inst[mid] <= p) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void k_localize(uint32_t* __restrict__ perm, uint32_t* __restrict__ lcp,
+                           const uint64_t* __restrict__ inst, uint32_t ninst, uint32_t n)
+{
+    __shared__ uint32_t kr[2];
+    for (uint64_t c0 = (uint64_t)blockIdx.x * LOC_CHUNK; c0 < n; c0 += (uint64_t)gridDim.x * LOC_CHUNK) {
+        const uint64_t c1 = min(c0 + LOC_CHUNK, (uint64_t)n);
+        if (threadIdx.x == 0) {
+            kr[0] = last_inst_at_or_below(inst, 0, ninst - 1, c0);
+            kr[1] = last_inst_at_or_below(inst, kr[0], ninst - 1, c1 - 1);
+        }
+        __syncthreads();
+        const uint32_t klo = kr[0], khi = kr[1];
+        for (uint64_t p = c0 + threadIdx.x; p < c1; p += blockDim.x) {
+            const uint64_t b = inst[last_inst_at_or_below(inst, klo, khi, p)];
+            perm[p] -= (uint32_t)b;
+            if (lcp && p == b) lcp[p] = 0;
+        }
+        __syncthreads();
     }
 }
 
@@ -747,7 +772,8 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
         stats.kernel_launches += 1;
     }
     if (!err && d_inst) {
-        k_localize<<<std::max(1u, std::min((ninst + 7) / 8, 148u * 64u)), 256, 0, st>>>(perm, lcp, d_inst, ninst);
+        k_localize<<<std::max(1u, std::min((n + LOC_CHUNK - 1) / LOC_CHUNK, 148u * 8u)), 256, 0, st>>>(
+            perm, lcp, d_inst, ninst, n);
         stats.kernel_launches += 1;
     }
     PSS_CUDA(cudaEventRecord(c->ev1, st));

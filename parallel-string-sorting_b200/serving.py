@@ -127,9 +127,34 @@ def make_stream(pools, rate: float = 2000.0, duration: float = 60.0, min_bytes: 
     return out
 
 
-def run_stream(server: Server, pools, reqs: List[Req], want_lcp: bool = False) -> dict:
+class ResultRing:
+    """Result buffers carved from one reused host buffer (pinned when alloc
+    pins), as a serving client with a fixed result area hands them out: a
+    request's slot is overwritten once `entries` more results have been
+    handed out, so the results must be read before then."""
+
+    def __init__(self, entries: int, alloc: Callable = workloads._alloc_np):
+        self.buf = alloc(4 * entries, np.uint32)
+        self.buf.fill(0)  # resident before the first copy lands in it
+        self.pos = 0
+
+    def take(self, n: int) -> np.ndarray:
+        if n > self.buf.shape[0]:
+            raise ValueError("request larger than the result ring")
+        if self.pos + n > self.buf.shape[0]:
+            self.pos = 0
+        out = self.buf[self.pos:self.pos + n]
+        self.pos += n
+        return out
+
+
+def run_stream(server: Server, pools, reqs: List[Req], want_lcp: bool = False,
+               results: ResultRing = None) -> dict:
     """Submit every request at its arrival time (relative to now); a second
-    thread waits for completions in order. Returns latency figures."""
+    thread waits for completions in order. Returns latency figures. Results
+    go to fresh arrays, or to slots of `results` (perm only)."""
+    if results is not None and want_lcp:
+        raise ValueError("a result ring holds permutations only")
     submitted: "queue.Queue[Req]" = queue.Queue()
 
     def waiter():
@@ -146,7 +171,7 @@ def run_stream(server: Server, pools, reqs: List[Req], want_lcp: bool = False) -
             time.sleep(delay)
         pool = pools[r.alphabet]
         n = r.i1 - r.i0
-        r.perm = np.empty(n, dtype=np.uint32)
+        r.perm = results.take(n) if results is not None else np.empty(n, dtype=np.uint32)
         r.lcp = np.zeros(n, dtype=np.uint32) if want_lcp else None
         r.ticket = server.submit(pool.chars.ctypes.data + r.start, r.nchars,
                                  pool.offs[r.i0:r.i1], r.start, r.perm, r.lcp)

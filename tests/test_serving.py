@@ -98,3 +98,4 @@ def test_refuses_requests_beyond_the_budget(pkg, serving):
         assert e.value.status == 6  # PSSGPU_EBUDGET
     finally:
         srv.close()
+

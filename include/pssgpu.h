@@ -130,7 +130,9 @@ int pssgpu_ctx_set_option(pssgpu_ctx* ctx, int option, int64_t value);
  * either way. Pinned host buffers let the copies overlap the host work.
  *
  * pssgpu_sort_device: device buffers on the context's device. d_chars must
- * be 8-byte aligned and readable for nchars + PSSGPU_ARENA_PAD bytes;
+ * be 8-byte aligned and readable for nchars + PSSGPU_ARENA_PAD bytes (the
+ * kernels read whole 16-byte blocks, so the block holding d_chars[0] is read
+ * from its start: any device allocation satisfies this);
  * `stream` is a cudaStream_t or NULL for the context's stream, which orders
  * with the legacy default stream (work the caller queued there before the
  * call is done before the sort starts). The call returns after the sort has

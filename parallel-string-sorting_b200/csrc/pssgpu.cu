@@ -77,10 +77,10 @@ __global__ void k_roots(Work w, const uint64_t* __restrict__ inst, uint32_t nins
 }
 
 // Batch output: ids relative to their instance; the first LCP of every
-// instance is 0. Blocks take chunks of LOC_CHUNK positions (work follows
+// instance is 0. One block per chunk of LOC_CHUNK positions (work follows
 // the strings, whether a batch holds many small instances or a few large
-// ones): the instances overlapping a chunk are found once, and each position
-// finds its own among them.
+// ones); a thread finds the instance of its first position by a search and
+// then only moves forward, as its positions increase.
 constexpr uint32_t LOC_CHUNK = 4096;
 
 // last k in [lo, hi] with inst[k] <= p (inst[lo] <= p)
@@ -97,21 +97,17 @@ __device__ __forceinline__ uint32_t last_inst_at_or_below(const uint64_t* inst, 
 __global__ void k_localize(uint32_t* __restrict__ perm, uint32_t* __restrict__ lcp,
                            const uint64_t* __restrict__ inst, uint32_t ninst, uint32_t n)
 {
-    __shared__ uint32_t kr[2];
     for (uint64_t c0 = (uint64_t)blockIdx.x * LOC_CHUNK; c0 < n; c0 += (uint64_t)gridDim.x * LOC_CHUNK) {
         const uint64_t c1 = min(c0 + LOC_CHUNK, (uint64_t)n);
-        if (threadIdx.x == 0) {
-            kr[0] = last_inst_at_or_below(inst, 0, ninst - 1, c0);
-            kr[1] = last_inst_at_or_below(inst, kr[0], ninst - 1, c1 - 1);
-        }
-        __syncthreads();
-        const uint32_t klo = kr[0], khi = kr[1];
-        for (uint64_t p = c0 + threadIdx.x; p < c1; p += blockDim.x) {
-            const uint64_t b = inst[last_inst_at_or_below(inst, klo, khi, p)];
+        uint64_t p = c0 + threadIdx.x;
+        if (p >= c1) continue;
+        uint32_t k = last_inst_at_or_below(inst, 0, ninst - 1, p);
+        for (; p < c1; p += blockDim.x) {
+            while (k + 1 < ninst && inst[k + 1] <= p) ++k;
+            const uint64_t b = inst[k];
             perm[p] -= (uint32_t)b;
             if (lcp && p == b) lcp[p] = 0;
         }
-        __syncthreads();
     }
 }
 
@@ -772,8 +768,7 @@ static int run_sort(Ctx* c, const uint8_t* chars, uint64_t nchars, const uint64_
         stats.kernel_launches += 1;
     }
     if (!err && d_inst) {
-        k_localize<<<std::max(1u, std::min((n + LOC_CHUNK - 1) / LOC_CHUNK, 148u * 8u)), 256, 0, st>>>(
-            perm, lcp, d_inst, ninst, n);
+        k_localize<<<std::max(1u, (n + LOC_CHUNK - 1) / LOC_CHUNK), 256, 0, st>>>(perm, lcp, d_inst, ninst, n);
         stats.kernel_launches += 1;
     }
     PSS_CUDA(cudaEventRecord(c->ev1, st));

@@ -44,6 +44,88 @@ __device__ __forceinline__ int compare_lcp(const uint8_t* chars, uint64_t nchars
     return compare_from(chars, nchars, oa, ob, 0, lcp);
 }
 
+// compare_from that also returns the last 8-char windows it read (*wa, *wb,
+// both from depth *wd; the LCP lies in [*wd, *wd + 7]).
+__device__ __forceinline__ int compare_from_win(const uint8_t* chars, uint64_t nchars, uint64_t oa,
+                                                uint64_t ob, uint32_t d, uint32_t* lcp, uint64_t* wa,
+                                                uint64_t* wb, uint32_t* wd)
+{
+    while (true) {
+        const uint64_t ka = load_key(chars, nchars, oa + d), kb = load_key(chars, nchars, ob + d);
+        if (ka != kb || key_terminated(ka)) {
+            *wa = ka;
+            *wb = kb;
+            *wd = d;
+            if (ka != kb) {
+                *lcp = d + lcp_key_type(ka, kb);
+                return ka < kb ? -1 : 1;
+            }
+            *lcp = d + lcp_key_depth(ka);
+            return 0;
+        }
+        d += 8;
+    }
+}
+
+// Char cache of a run head (the reference's LCP + char-cache form, with
+// more than one char): the chars of the string from depth h, its LCP with
+// the last output, big-endian in bits 63..8 (7 chars, NUL past the string's
+// end) and in bits 7..0 how many of them are known (1..7). A run's cache
+// array holds, for every entry but its first, the chars at the depth of its
+// LCP with its predecessor, so a head taken from the run brings them along.
+__device__ __forceinline__ uint64_t cache_of_key(uint64_t key) { return (key & ~0xFFull) | 7u; }
+
+// The cache of the same string j chars deeper (j < known).
+__device__ __forceinline__ uint64_t cache_shift(uint64_t c, uint32_t j)
+{
+    return (((c & ~0xFFull) << (8u * j)) & ~0xFFull) | ((c & 0xFFu) - j);
+}
+
+// Order of heads a and b that both share h chars with the last output, from
+// their caches first and from the arena past the chars both know. Returns
+// whether a comes first (equal strings: a, the left run's); the loser's LCP
+// with the winner, the new last output, replaces its h and its cache moves
+// to that depth.
+__device__ __forceinline__ bool cached_tie(const uint8_t* chars, uint64_t nchars, uint64_t oa,
+                                           uint64_t ob, uint32_t& ha, uint64_t& ca, uint32_t& hb,
+                                           uint64_t& cb)
+{
+    const uint32_t h = ha;
+    const uint32_t m = min((uint32_t)(ca & 0xFFu), (uint32_t)(cb & 0xFFu));
+    const uint64_t mask = ~0ull << (64u - 8u * m);
+    const uint64_t ka = ca & mask, kb = cb & mask;
+    uint32_t j;
+    bool take_a;
+    if (ka != kb) {  // differ within the known chars
+        j = lcp_key_type(ka, kb);
+        take_a = ka < kb;
+    } else if ((j = lcp_key_depth(ka)) < m) {  // both end within them: equal
+        take_a = true;
+    } else {  // the arena past the known chars
+        uint32_t l, wd;
+        uint64_t wa, wb;
+        take_a = compare_from_win(chars, nchars, oa, ob, h + m, &l, &wa, &wb, &wd) <= 0;
+        const uint32_t sft = l - wd;  // 0..7
+        const uint64_t nc = (((take_a ? wb : wa) << (8u * sft)) & ~0xFFull) | min(7u, 8u - sft);
+        if (take_a) {
+            hb = l;
+            cb = nc;
+        } else {
+            ha = l;
+            ca = nc;
+        }
+        return take_a;
+    }
+    if (take_a) {
+        hb = h + j;
+        cb = cache_shift(cb, j);
+    } else {
+        ha = h + j;
+        ca = cache_shift(ca, j);
+    }
+    return take_a;
+}
+
 // Merge-path form of a round. A pair is (a0, a1, b1): left run [a0, a1),
 // right run [a1, b1) (empty for an unpaired last run), merged into [a0, b1).
 // Its output is cut into pieces of `piece` positions (MERGE_PIECE by
@@ -71,7 +153,7 @@ __device__ __forceinline__ uint32_t pair_of(const uint64_t* first, uint32_t npai
 // How a round reads its runs. MergeByIds: the entries are string ids and
 // a string's arena offset is gathered through offs at each use.
 // MergeByHandles: the entries are handles (id << hbits | offset), made once
-// by k_merge_pack, so the offset comes with the entry a round reads in order
+// by k_merge_prep, so the offset comes with the entry a round reads in order
 // and no round gathers offsets.
 struct MergeByIds {
     using T = uint32_t;
@@ -84,45 +166,6 @@ struct MergeByHandles {
     __device__ __forceinline__ uint64_t off(uint64_t v) const { return v & hmask; }
 };
 
-// Sequential reads of an array 16 bytes at a time: a thread that walks its
-// own stretch of entries or LCPs keeps the last aligned 16-byte block in
-// registers instead of fetching a sector per entry (the threads' streams are
-// too many for the caches to keep their lines). The array must be 16-byte
-// aligned and readable up to the next 16-byte boundary past its end.
-template <class T>
-struct SeqRead;
-template <>
-struct SeqRead<uint32_t> {
-    const uint32_t* base;
-    uint64_t blk = ~0ull;
-    uint4 v{};
-    __device__ __forceinline__ uint32_t get(uint64_t i)
-    {
-        const uint64_t b = i >> 2;
-        if (b != blk) {
-            v = __ldg(reinterpret_cast<const uint4*>(base + (b << 2)));
-            blk = b;
-        }
-        const uint32_t k = (uint32_t)(i & 3);
-        return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w;
-    }
-};
-template <>
-struct SeqRead<uint64_t> {
-    const uint64_t* base;
-    uint64_t blk = ~0ull;
-    ulonglong2 v{};
-    __device__ __forceinline__ uint64_t get(uint64_t i)
-    {
-        const uint64_t b = i >> 1;
-        if (b != blk) {
-            v = __ldg(reinterpret_cast<const ulonglong2*>(base + (b << 1)));
-            blk = b;
-        }
-        return (i & 1) ? v.y : v.x;
-    }
-};
-using SeqRead4 = SeqRead<uint32_t>;
 
 // Splits in two launches: coarse = 1 searches every MERGE_SPLIT_COARSE-th
 // piece of a pair over the whole diagonal; coarse = 0 searches the other
@@ -220,28 +263,160 @@ __global__ void k_merge_seq(const uint8_t* __restrict__ chars, uint64_t nchars, 
     }
 }
 
-// LCP-aware piece merge (the reference's LCP loser-tree rule for two runs).
-// Runs A = in[a0, a1) and B = in[a1, b1) with their LCP arrays in lcp_in
-// (entries at a run's first position are not read). ha / hb are the LCPs of
-// the heads A[i] / B[j] with the last output. A piece that does not start
-// the pair first finds its previous output (the larger of A[i0 - 1] and
-// B[j0 - 1]; equal strings: B's, as A's comes first) and the heads' LCPs
-// with it. lcp_out (may be null) receives the LCP of every output but the
-// pair's first.
+// Shared-memory staging of the LCP-aware piece merge. A thread's heads come
+// from two runs it reads in order, and its outputs go to one stretch: per
+// run and stream (entries, LCPs, caches) two chunks of MS_CH entries, the
+// next one in flight (cp.async) while the current one is read, and per
+// output stream the 32-byte sector being filled, written at once when full.
+// Every byte a thread fetches is then one it uses, and no output sector is
+// written in parts (a partial sector costs a fill read from DRAM).
+constexpr uint32_t MS_THREADS = 128;
+constexpr uint32_t MS_CH = 4;
+
+template <class T>
+struct alignas(32) MergeStage {
+    T v[2][2][MS_THREADS][MS_CH];           // run, slot, thread, entry
+    uint64_t ck[2][2][MS_THREADS][MS_CH];
+    uint32_t lcp[2][2][MS_THREADS][MS_CH];
+    T ov[MS_THREADS][32 / sizeof(T)];       // output sectors
+    uint64_t ock[MS_THREADS][4];
+    uint32_t olcp[MS_THREADS][8];
+};
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
+{
+    const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+// One 32-byte sector from shared memory to an aligned global address.
+__device__ __forceinline__ void store_sector(void* gdst, const void* ssrc)
+{
+    const ulonglong2 x = *reinterpret_cast<const ulonglong2*>(ssrc);
+    const ulonglong2 y = *(reinterpret_cast<const ulonglong2*>(ssrc) + 1);
+    asm volatile("st.global.v4.u64 [%0], {%1, %2, %3, %4};\n" ::"l"(gdst), "l"(x.x), "l"(x.y), "l"(y.x),
+                 "l"(y.y)
+                 : "memory");
+}
+
+// Chunk c (entries [c * MS_CH, c * MS_CH + MS_CH) of the round's arrays) of
+// run r into its slot, as one cp.async group. The arrays are 16-byte
+// aligned and padded past their last chunk.
+template <class T>
+__device__ __forceinline__ void stage_chunk(MergeStage<T>& sm, uint32_t r, uint64_t c, const T* in,
+                                            const uint32_t* lcp_in, const uint64_t* ck_in)
+{
+    const uint32_t tid = threadIdx.x, sl = (uint32_t)(c & 1);
+    const uint64_t q = c * MS_CH;
+    cp_async16(&sm.v[r][sl][tid][0], in + q);
+    if (sizeof(T) == 8) cp_async16(&sm.v[r][sl][tid][2], in + q + 2);
+    cp_async16(&sm.ck[r][sl][tid][0], ck_in + q);
+    cp_async16(&sm.ck[r][sl][tid][2], ck_in + q + 2);
+    cp_async16(&sm.lcp[r][sl][tid][0], lcp_in + q);
+    cp_async_commit();
+}
+
+// Run R's head moved to position q (< its end q1): on entering a chunk,
+// wait for it (it was staged one ahead; the other run's chunk in flight is
+// not waited for when it went out later) and stage the next one into the
+// slot just read. mine / other: whether run R's / the other run's chunk is
+// in flight; last_b: whether run B staged the latest group.
+template <uint32_t R, class T>
+__device__ __forceinline__ void stage_next(MergeStage<T>& sm, uint64_t q, uint64_t q1, const T* in,
+                                           const uint32_t* lcp_in, const uint64_t* ck_in, bool& mine,
+                                           bool& other, bool& last_b)
+{
+    if (q % MS_CH != 0) return;
+    const bool other_later = R == 0 ? last_b : !last_b;
+    if (other && other_later) {
+        cp_async_wait1();
+    } else {
+        cp_async_wait0();
+        other = false;
+    }
+    mine = false;
+    const uint64_t c = q / MS_CH;
+    if ((c + 1) * MS_CH < q1) {
+        stage_chunk(sm, R, c + 1, in, lcp_in, ck_in);
+        mine = true;
+        last_b = R == 1;
+    }
+}
+
+// An output stream: entries written to base[o] for o in [lo, hi) in order,
+// collected per 32-byte sector in shared memory (buf, E entries of U) and
+// written per sector; a sector the stretch covers only in part is written
+// entry by entry.
+template <class U>
+struct SectorOut {
+    static constexpr uint32_t E = 32 / sizeof(U);
+    U* base;
+    U* buf;
+    uint64_t lo;
+    uint32_t phase;  // sector position of base[0]
+    __device__ __forceinline__ void init(U* b, U* sbuf, uint64_t lo_)
+    {
+        base = b;
+        buf = sbuf;
+        lo = lo_;
+        phase = (uint32_t)((reinterpret_cast<uintptr_t>(b) / sizeof(U)) & (E - 1));
+    }
+    __device__ __forceinline__ void put(uint64_t o, U x)
+    {
+        const uint32_t s = (uint32_t)((o + phase) & (E - 1));
+        buf[s] = x;
+        if (s == E - 1) {
+            if (o + 1 >= lo + E) {
+                store_sector(base + (o + 1 - E), buf);
+            } else {
+                for (uint64_t k = lo; k <= o; ++k) base[k] = buf[(uint32_t)((k + phase) & (E - 1))];
+            }
+        }
+    }
+    // the entries of [lo, hi) after the last full sector
+    __device__ __forceinline__ void finish(uint64_t hi)
+    {
+        if (hi <= lo) return;
+        const uint32_t s = (uint32_t)((hi - 1 + phase) & (E - 1));
+        if (s == E - 1) return;  // written by put
+        uint64_t k = hi - 1 - s;  // the last sector's first entry
+        if (k < lo) k = lo;
+        for (; k < hi; ++k) base[k] = buf[(uint32_t)((k + phase) & (E - 1))];
+    }
+};
+
+// LCP-aware piece merge (the reference's LCP loser-tree rule for two runs,
+// with char caches). Runs A = in[a0, a1) and B = in[a1, b1) with their LCP
+// arrays in lcp_in and char caches in ck_in (entries at a run's first
+// position are not read). ha / hb are the LCPs of the heads A[i] / B[j] with
+// the last output, ca / cb their chars from there: heads with different
+// LCPs order by them, equal ones by their caches, and only chars neither
+// cache holds are read from the arena. A piece that does not start the pair
+// first finds its previous output (the larger of A[i0 - 1] and B[j0 - 1];
+// equal strings: B's, as A's comes first) and the heads' LCPs with it, and
+// reads its heads' chars from the arena. lcp_out (may be null) receives the
+// LCP of every output but the pair's first, ck_out (may be null) every
+// output's cache. MS_THREADS threads per block, sizeof(MergeStage<T>) bytes
+// of dynamic shared memory.
 template <class V>
-__global__ void __launch_bounds__(256, 4) k_merge_lcp_seq(const uint8_t* __restrict__ chars, uint64_t nchars, V view,
+__global__ void __launch_bounds__(MS_THREADS) k_merge_lcp_seq(const uint8_t* __restrict__ chars, uint64_t nchars, V view,
                                 const MergePair* __restrict__ pairs,
                                 const uint64_t* __restrict__ first, uint32_t npair,
                                 const uint64_t* __restrict__ split,
                                 const typename V::T* __restrict__ in,
-                                const uint32_t* __restrict__ lcp_in,
+                                const uint32_t* __restrict__ lcp_in, const uint64_t* __restrict__ ck_in,
                                 typename V::T* __restrict__ out, uint32_t* __restrict__ lcp_out,
-                                uint32_t piece)
+                                uint64_t* __restrict__ ck_out, uint32_t piece)
 {
     using T = typename V::T;
+    extern __shared__ __align__(32) unsigned char merge_smem[];
+    MergeStage<T>& sm = *reinterpret_cast<MergeStage<T>*>(merge_smem);
+    const uint32_t tid = threadIdx.x;
     const uint64_t ntask = first[npair];
-    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ntask;
-         t += (uint64_t)gridDim.x * blockDim.x) {
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + tid; t < ntask; t += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t p = pair_of(first, npair, t);
         const MergePair pr = pairs[p];
         const uint64_t na = pr.a1 - pr.a0, nb = pr.b1 - pr.a1;
@@ -254,80 +429,128 @@ __global__ void __launch_bounds__(256, 4) k_merge_lcp_seq(const uint8_t* __restr
         const uint64_t i0 = split[t];
         const uint64_t i1 = t + 1 < first[p + 1] ? split[t + 1] : na;
         const uint64_t j0 = d0 - i0, j1 = d1 - i1;
-        uint64_t i = i0, j = j0;
+        // absolute positions of the heads and their ends
+        uint64_t qa = pr.a0 + i0, qb = pr.a1 + j0;
+        const uint64_t qa1 = pr.a0 + i1, qb1 = pr.a1 + j1;
+        // the first chunks of both runs in flight while the heads' LCPs
+        // with the previous output are found
+        bool pend_a = false, pend_b = false, last_b = false;
+        if (qa < qa1) {
+            stage_chunk(sm, 0, qa / MS_CH, in, lcp_in, ck_in);
+            if ((qa / MS_CH + 1) * MS_CH < qa1) stage_chunk(sm, 0, qa / MS_CH + 1, in, lcp_in, ck_in);
+        }
+        if (qb < qb1) {
+            stage_chunk(sm, 1, qb / MS_CH, in, lcp_in, ck_in);
+            if ((qb / MS_CH + 1) * MS_CH < qb1) stage_chunk(sm, 1, qb / MS_CH + 1, in, lcp_in, ck_in);
+        }
         uint32_t ha = 0, hb = 0;
-        if (d0 > 0) {
-            if (i0 == 0) {  // previous output B[j0 - 1]
-                hb = j < nb ? LB[j] : 0u;
-                if (i < na) compare_from(chars, nchars, view.off(A[i]), view.off(B[j - 1]), 0, &ha);
-            } else if (j0 == 0) {  // previous output A[i0 - 1]
-                ha = i < na ? LA[i] : 0u;
-                if (j < nb) compare_from(chars, nchars, view.off(B[j]), view.off(A[i - 1]), 0, &hb);
-            } else {
-                uint32_t l;
-                const int c = compare_from(chars, nchars, view.off(A[i - 1]), view.off(B[j - 1]), 0, &l);
-                // LCP(x, z) >= min(LCP(x, y), LCP(y, z)): start from that depth
-                if (c <= 0) {  // previous output B[j0 - 1]
+        {
+            const uint64_t i = i0, j = j0;
+            if (d0 > 0) {
+                if (i0 == 0) {  // previous output B[j0 - 1]
                     hb = j < nb ? LB[j] : 0u;
-                    if (i < na)
-                        compare_from(chars, nchars, view.off(A[i]), view.off(B[j - 1]), min(LA[i], l), &ha);
-                } else {       // previous output A[i0 - 1]
+                    if (i < na) compare_from(chars, nchars, view.off(A[i]), view.off(B[j - 1]), 0, &ha);
+                } else if (j0 == 0) {  // previous output A[i0 - 1]
                     ha = i < na ? LA[i] : 0u;
-                    if (j < nb)
-                        compare_from(chars, nchars, view.off(B[j]), view.off(A[i - 1]), min(LB[j], l), &hb);
+                    if (j < nb) compare_from(chars, nchars, view.off(B[j]), view.off(A[i - 1]), 0, &hb);
+                } else {
+                    uint32_t l;
+                    const int c = compare_from(chars, nchars, view.off(A[i - 1]), view.off(B[j - 1]), 0, &l);
+                    // LCP(x, z) >= min(LCP(x, y), LCP(y, z)): start from that depth
+                    if (c <= 0) {  // previous output B[j0 - 1]
+                        hb = j < nb ? LB[j] : 0u;
+                        if (i < na)
+                            compare_from(chars, nchars, view.off(A[i]), view.off(B[j - 1]), min(LA[i], l), &ha);
+                    } else {       // previous output A[i0 - 1]
+                        ha = i < na ? LA[i] : 0u;
+                        if (j < nb)
+                            compare_from(chars, nchars, view.off(B[j]), view.off(A[i - 1]), min(LB[j], l), &hb);
+                    }
                 }
             }
         }
-        // the heads' entries and arena offsets stay in registers: a compare
-        // reads chars only; the runs' entries and LCPs are read 16 bytes at
-        // a time
-        SeqRead<T> ra{in}, rb{in};
-        SeqRead4 la{lcp_in}, lb{lcp_in};
-        T va = i < i1 ? ra.get(pr.a0 + i) : T(0), vb = j < j1 ? rb.get(pr.a1 + j) : T(0);
-        uint64_t oa = i < i1 ? view.off(va) : 0ull, ob = j < j1 ? view.off(vb) : 0ull;
-        for (uint64_t d = d0; d < d1; ++d) {
+        cp_async_wait0();
+        T va = T(0), vb = T(0);
+        uint64_t oa = 0, ob = 0, ca = 0, cb = 0;
+        if (qa < qa1) {
+            va = sm.v[0][(qa / MS_CH) & 1][tid][qa % MS_CH];
+            oa = view.off(va);
+            ca = cache_of_key(load_key(chars, nchars, oa + ha));
+        }
+        if (qb < qb1) {
+            vb = sm.v[1][(qb / MS_CH) & 1][tid][qb % MS_CH];
+            ob = view.off(vb);
+            cb = cache_of_key(load_key(chars, nchars, ob + hb));
+        }
+        const uint64_t o0 = pr.a0 + d0, o1 = pr.a0 + d1;
+        SectorOut<T> wv;
+        SectorOut<uint32_t> wl;
+        SectorOut<uint64_t> wc;
+        wv.init(out, sm.ov[tid], o0);
+        if (lcp_out) wl.init(lcp_out, sm.olcp[tid], d0 == 0 ? o0 + 1 : o0);
+        if (ck_out) wc.init(ck_out, sm.ock[tid], o0);
+        for (uint64_t o = o0; o < o1; ++o) {
             bool take_a;
-            if (i >= i1) take_a = false;
-            else if (j >= j1) take_a = true;
+            if (qa >= qa1) take_a = false;
+            else if (qb >= qb1) take_a = true;
             else if (ha != hb) take_a = ha > hb;
-            else {
-                uint32_t l;
-                take_a = compare_from(chars, nchars, oa, ob, ha, &l) <= 0;
-                if (take_a) hb = l; else ha = l;  // the loser's LCP with the new last output
-            }
-            out[pr.a0 + d] = take_a ? va : vb;
-            if (lcp_out && d > 0) lcp_out[pr.a0 + d] = take_a ? ha : hb;
+            else take_a = cached_tie(chars, nchars, oa, ob, ha, ca, hb, cb);
+            wv.put(o, take_a ? va : vb);
+            if (lcp_out && o >= wl.lo) wl.put(o, take_a ? ha : hb);
+            if (ck_out) wc.put(o, take_a ? ca : cb);
             if (take_a) {
-                ++i;
-                ha = i < na ? la.get(pr.a0 + i) : 0u;  // against its predecessor, the last output
-                if (i < i1) {
-                    va = ra.get(pr.a0 + i);
+                if (++qa < qa1) {
+                    stage_next<0>(sm, qa, qa1, in, lcp_in, ck_in, pend_a, pend_b, last_b);
+                    const uint32_t sl = (uint32_t)((qa / MS_CH) & 1), e = (uint32_t)(qa % MS_CH);
+                    va = sm.v[0][sl][tid][e];
+                    ha = sm.lcp[0][sl][tid][e];
+                    ca = sm.ck[0][sl][tid][e];
                     oa = view.off(va);
                 }
             } else {
-                ++j;
-                hb = j < nb ? lb.get(pr.a1 + j) : 0u;
-                if (j < j1) {
-                    vb = rb.get(pr.a1 + j);
+                if (++qb < qb1) {
+                    stage_next<1>(sm, qb, qb1, in, lcp_in, ck_in, pend_b, pend_a, last_b);
+                    const uint32_t sl = (uint32_t)((qb / MS_CH) & 1), e = (uint32_t)(qb % MS_CH);
+                    vb = sm.v[1][sl][tid][e];
+                    hb = sm.lcp[1][sl][tid][e];
+                    cb = sm.ck[1][sl][tid][e];
                     ob = view.off(vb);
                 }
             }
         }
+        wv.finish(o1);
+        if (lcp_out) wl.finish(o1);
+        if (ck_out) wc.finish(o1);
+        cp_async_wait0();  // nothing of this piece left in flight
     }
 }
 
-// Handles of the runs' strings (32-bit id << hbits | arena offset, offsets
-// below 2^hbits <= 2^32), with the arena check of k_merge_check.
-__global__ void k_merge_pack(const uint64_t* __restrict__ offs, uint64_t nchars,
-                             const uint32_t* __restrict__ ids, uint64_t n, uint32_t hbits,
-                             uint64_t* __restrict__ out, uint32_t* err)
+// Round 0's inputs in the library's own buffers (aligned, padded, so that
+// the rounds stage them in 16-byte copies), with the arena check: every
+// id's offset must lie inside the arena (else *err). PACK: handles (32-bit
+// id << hbits | arena offset, offsets below 2^hbits <= 2^32) into out; else
+// the ids as they are (out may be null: no copy). With the runs' LCP arrays
+// (lcp not null) their copy and every entry's cache at the depth of its LCP.
+template <bool PACK>
+__global__ void k_merge_prep(const uint8_t* __restrict__ chars, uint64_t nchars,
+                             const uint64_t* __restrict__ offs, const uint32_t* __restrict__ ids,
+                             const uint32_t* __restrict__ lcp, uint64_t n, uint32_t hbits, void* out,
+                             uint32_t* __restrict__ lcp_out, uint64_t* __restrict__ ck_out, uint32_t* err)
 {
     for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n;
          q += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t id = ids[q];
         const uint64_t o = __ldg(offs + id);
-        if (o >= nchars) atomicOr(err, ERR_OFFSET);
-        out[q] = ((uint64_t)id << hbits) | (o < nchars ? o : 0ull);
+        const bool bad = o >= nchars;
+        if (bad) atomicOr(err, ERR_OFFSET);
+        if (PACK) static_cast<uint64_t*>(out)[q] = ((uint64_t)id << hbits) | (bad ? 0ull : o);
+        else if (out) static_cast<uint32_t*>(out)[q] = id;
+        if (lcp) {
+            // a run's first LCP is any value: its cache is not read
+            const uint32_t l = lcp[q];
+            lcp_out[q] = l;
+            ck_out[q] = bad ? 7u : cache_of_key(load_key(chars, nchars, o + l));
+        }
     }
 }
 
@@ -338,15 +561,6 @@ __global__ void k_merge_unpack(const uint64_t* __restrict__ h, uint64_t n, uint3
     for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n;
          q += (uint64_t)gridDim.x * blockDim.x)
         ids[q] = (uint32_t)(h[q] >> hbits);
-}
-
-// Every id's offset must lie inside the arena (offsets >= nchars: *err).
-__global__ void k_merge_check(const uint64_t* __restrict__ offs, uint64_t nchars,
-                              const uint32_t* __restrict__ ids, uint64_t n, uint32_t* err)
-{
-    for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n;
-         q += (uint64_t)gridDim.x * blockDim.x)
-        if (__ldg(offs + ids[q]) >= nchars) atomicOr(err, ERR_OFFSET);
 }
 
 }  // namespace pssgpu

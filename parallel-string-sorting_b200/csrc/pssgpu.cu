@@ -1681,46 +1681,59 @@ int pssgpu_merge_lcp_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nc
     // entries instead of gathering them; else as ids
     const uint32_t hbits = std::max<uint32_t>(1, bit_length(nchars - 1));
     const bool packed = hbits <= 32 && !c->indirect_handles;
-    const uint64_t b_v = align256(4 * n + 16), b_h = align256(8 * n + 16);
+    // padded past the last entry: the piece merge stages whole chunks of
+    // MS_CH entries
+    const uint64_t b_v = align256(4 * n + 8 * MS_CH), b_h = align256(8 * n + 8 * MS_CH);
     const uint64_t b_runs = align256(8 * flat.size()), b_split = align256(8 * (max_tasks + 1));
-    if ((rc = ensure_buf(&c->mbuf, &c->mbuf_bytes, 2 * b_h + 2 * b_v + b_runs + b_split + 256))) return rc;
+    const bool with_lcp = d_lcp != nullptr;
+    const uint64_t b_ck = with_lcp ? b_h : 0;
+    if ((rc = ensure_buf(&c->mbuf, &c->mbuf_bytes, 2 * b_h + 2 * b_v + 2 * b_ck + b_runs + b_split + 256)))
+        return rc;
     unsigned char* tv[2] = {c->mbuf, c->mbuf + b_h};  // ids or handles, by round parity
     uint32_t* tlcp[2] = {(uint32_t*)(c->mbuf + 2 * b_h), (uint32_t*)(c->mbuf + 2 * b_h + b_v)};
-    uint64_t* d_flat = (uint64_t*)(c->mbuf + 2 * b_h + 2 * b_v);
-    uint64_t* split = (uint64_t*)(c->mbuf + 2 * b_h + 2 * b_v + b_runs);
-    uint32_t* d_err = (uint32_t*)(c->mbuf + 2 * b_h + 2 * b_v + b_runs + b_split);
+    unsigned char* const rest = c->mbuf + 2 * b_h + 2 * b_v;
+    uint64_t* tck[2] = {(uint64_t*)rest, (uint64_t*)(rest + b_ck)};  // char caches
+    uint64_t* d_flat = (uint64_t*)(rest + 2 * b_ck);
+    uint64_t* split = (uint64_t*)(rest + 2 * b_ck + b_runs);
+    uint32_t* d_err = (uint32_t*)(rest + 2 * b_ck + b_runs + b_split);
     PSS_CUDA(cudaMemcpyAsync(d_flat, flat.data(), 8 * flat.size(), cudaMemcpyHostToDevice, st));
     PSS_CUDA(cudaMemsetAsync(d_err, 0, 4, st));
     const unsigned blocks = (unsigned)std::min<uint64_t>((n + 255) / 256, 148ull * 16);
     // with the runs' LCP arrays every round is LCP-aware and carries the
-    // merged LCP array to the next one (the last round writes d_lcp_out, if
-    // any). Its sequential reads take 16 bytes at a time, from the library's
-    // own buffers (aligned, padded): the caller's ids (as handles, or as
-    // they are) and LCPs are copied in; round 0 writes tv[0] and tlcp[0].
-    const bool with_lcp = d_lcp != nullptr;
+    // merged LCP array and the char caches to the next one (the last round
+    // writes d_lcp_out, if any). Its reads are staged in 16-byte copies from
+    // the library's own buffers (aligned, padded): k_merge_prep copies the
+    // caller's ids (as handles, or as they are) and LCPs in and makes the
+    // caches; round 0 writes tv[0], tlcp[0] and tck[0].
     const unsigned char* in_v = (const unsigned char*)d_ids;
-    const uint32_t* in_lcp = d_lcp;
+    const uint32_t* in_lcp = with_lcp ? tlcp[1] : nullptr;
+    const uint64_t* in_ck = with_lcp ? tck[1] : nullptr;
     if (packed) {
-        k_merge_pack<<<blocks, 256, 0, st>>>(d_offs, nchars, d_ids, n, hbits, (uint64_t*)tv[1], d_err);
+        k_merge_prep<true><<<blocks, 256, 0, st>>>(d_chars, nchars, d_offs, d_ids, d_lcp, n, hbits, tv[1],
+                                                   tlcp[1], tck[1], d_err);
         in_v = tv[1];
     } else {
-        k_merge_check<<<blocks, 256, 0, st>>>(d_offs, nchars, d_ids, n, d_err);
-        if (with_lcp) {
-            PSS_CUDA(cudaMemcpyAsync(tv[1], d_ids, 4 * n, cudaMemcpyDeviceToDevice, st));
-            in_v = tv[1];
-        }
-    }
-    if (with_lcp) {
-        PSS_CUDA(cudaMemcpyAsync(tlcp[1], d_lcp, 4 * n, cudaMemcpyDeviceToDevice, st));
-        in_lcp = tlcp[1];
+        k_merge_prep<false><<<blocks, 256, 0, st>>>(d_chars, nchars, d_offs, d_ids, d_lcp, n, hbits,
+                                                    with_lcp ? tv[1] : nullptr, tlcp[1], tck[1], d_err);
+        if (with_lcp) in_v = tv[1];
     }
     const MergeByIds by_ids{d_offs};
     const MergeByHandles by_h{(1ull << hbits) - 1};
+    // the piece merge: MS_THREADS threads and their staging per block
+    const uint32_t smem_h = sizeof(MergeStage<uint64_t>), smem_i = sizeof(MergeStage<uint32_t>);
+    if (with_lcp) {  // per device: set on every call
+        PSS_CUDA(cudaFuncSetAttribute(packed ? (const void*)k_merge_lcp_seq<MergeByHandles>
+                                             : (const void*)k_merge_lcp_seq<MergeByIds>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(packed ? smem_h : smem_i)));
+    }
+    const unsigned ms_blocks =
+        (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((max_tasks + MS_THREADS - 1) / MS_THREADS, 148ull * 8));
     for (size_t i = 0; i < rounds; ++i) {
         const bool lastr = i + 1 == rounds;
         // the last round writes the caller's ids directly unless it merges handles
         unsigned char* out_v = lastr && !packed ? (unsigned char*)d_ids_out : tv[i & 1];
         uint32_t* out_lcp = lastr ? d_lcp_out : tlcp[i & 1];
+        uint64_t* out_ck = lastr || !with_lcp ? nullptr : tck[i & 1];
         const MergePair* pairs = reinterpret_cast<const MergePair*>(d_flat + at_pairs[i]);
         const uint64_t* first = d_flat + at_first[i];
         const uint32_t np = (uint32_t)npairs[i];
@@ -1732,8 +1745,8 @@ int pssgpu_merge_lcp_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nc
                 k_merge_split<MergeByHandles><<<blocks, 256, 0, st>>>(d_chars, nchars, by_h, pairs, first, np, in,
                                                                       split, pc, coarse);
             if (with_lcp)
-                k_merge_lcp_seq<MergeByHandles><<<blocks, 256, 0, st>>>(d_chars, nchars, by_h, pairs, first, np,
-                                                                        split, in, in_lcp, out, out_lcp, pc);
+                k_merge_lcp_seq<MergeByHandles><<<ms_blocks, MS_THREADS, smem_h, st>>>(
+                    d_chars, nchars, by_h, pairs, first, np, split, in, in_lcp, in_ck, out, out_lcp, out_ck, pc);
             else
                 k_merge_seq<MergeByHandles><<<blocks, 256, 0, st>>>(d_chars, nchars, by_h, pairs, first, np,
                                                                     split, in, out, pc);
@@ -1744,8 +1757,8 @@ int pssgpu_merge_lcp_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nc
                 k_merge_split<MergeByIds><<<blocks, 256, 0, st>>>(d_chars, nchars, by_ids, pairs, first, np, in,
                                                                   split, pc, coarse);
             if (with_lcp)
-                k_merge_lcp_seq<MergeByIds><<<blocks, 256, 0, st>>>(d_chars, nchars, by_ids, pairs, first, np,
-                                                                    split, in, in_lcp, out, out_lcp, pc);
+                k_merge_lcp_seq<MergeByIds><<<ms_blocks, MS_THREADS, smem_i, st>>>(
+                    d_chars, nchars, by_ids, pairs, first, np, split, in, in_lcp, in_ck, out, out_lcp, out_ck, pc);
             else
                 k_merge_seq<MergeByIds><<<blocks, 256, 0, st>>>(d_chars, nchars, by_ids, pairs, first, np,
                                                                 split, in, out, pc);
@@ -1753,6 +1766,7 @@ int pssgpu_merge_lcp_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nc
         PSS_CUDA(cudaGetLastError());
         in_v = out_v;
         in_lcp = out_lcp;
+        in_ck = out_ck;
     }
     if (packed)
         k_merge_unpack<<<blocks, 256, 0, st>>>((const uint64_t*)in_v, n, hbits, d_ids_out);

@@ -525,6 +525,40 @@ def test_merge_lcp(pkg, orc, ctx, K, case):
         check_against_oracle(orc, chars, offs, perm, dlo.cpu().numpy().view(np.uint32))
 
 
+@pytest.mark.parametrize("piece", [1, 3, 8, 128])
+@pytest.mark.parametrize("indirect", [0, 1])
+def test_merge_lcp_char_caches(pkg, orc, piece, indirect):
+    """The piece merge orders heads with equal LCPs from the 7 chars each
+    carries from that depth, and reads the arena only past them: strings that
+    differ inside the cached chars, after them (a 12-char shared stem then
+    variants up to 20 chars deeper), end inside them (duplicates, prefixes of
+    one another, empty strings), over several rounds and with a piece start
+    (heads read from the arena) at every few outputs."""
+    import torch
+    rng = np.random.default_rng(31 + piece)
+    stem = b"abbabaabbaba"
+    strs = [bytes(rng.integers(97, 99, int(rng.integers(0, 30)), dtype=np.uint8)) for _ in range(3000)]
+    strs += [stem + bytes(rng.integers(97, 99, int(rng.integers(0, 21)), dtype=np.uint8)) for _ in range(3000)]
+    strs += [stem] * 40 + [stem[:5]] * 30 + [b""] * 20
+    chars, offs = pkg.pack_strings(strs)
+    nchars = chars.shape[0]
+    ids, lcp, runs = _oracle_runs(orc, chars, offs, 5, 300 + piece)
+    dc = torch.from_numpy(np.concatenate([chars, np.zeros(16, np.uint8)])).cuda()
+    do = torch.from_numpy(offs.view(np.int64)).cuda()
+    di = torch.from_numpy(ids.view(np.int32)).cuda()
+    dl = torch.from_numpy(lcp.view(np.int32)).cuda()
+    dio = torch.empty_like(di)
+    dlo = torch.zeros_like(di)
+    c = pkg.Context(0)
+    try:
+        c.set_option(c.OPT_MERGE_PIECE, piece)
+        c.set_option(c.OPT_INDIRECT_HANDLES, indirect)
+        c.merge_lcp_device(dc, nchars, do, runs, di, dl, dio, dlo)
+    finally:
+        c.close()
+    check_against_oracle(orc, chars, offs, dio.cpu().numpy().view(np.uint32), dlo.cpu().numpy().view(np.uint32))
+
+
 @pytest.mark.parametrize("K,case", [(3, "rand"), (4, "deep"), (2, "no_lcp"), (6, "no_lcp_input")])
 def test_merge_lcp_ids_path(pkg, orc, K, case):
     """The merge rounds on string ids with offsets gathered at each use (the

@@ -133,7 +133,7 @@ __device__ __forceinline__ bool cached_tie(const uint8_t* chars, uint64_t nchars
 // piece how many left-run strings precede it (a binary search along the
 // piece's diagonal), k_merge_lcp_seq (or k_merge_seq without LCP arrays)
 // merges each piece sequentially from there.
-constexpr uint32_t MERGE_PIECE = 128;
+constexpr uint32_t MERGE_PIECE = 256;
 constexpr uint32_t MERGE_PIECE_MAX = 4096;
 
 struct MergePair {
@@ -159,63 +159,116 @@ struct MergeByIds {
     using T = uint32_t;
     const uint64_t* offs;
     __device__ __forceinline__ uint64_t off(uint32_t v) const { return __ldg(offs + v); }
+    __device__ __forceinline__ uint32_t id(uint32_t v) const { return v; }
 };
 struct MergeByHandles {
     using T = uint64_t;
     uint64_t hmask;
+    uint32_t hbits;
     __device__ __forceinline__ uint64_t off(uint64_t v) const { return v & hmask; }
+    __device__ __forceinline__ uint32_t id(uint64_t v) const { return (uint32_t)(v >> hbits); }
 };
 
 
-// Splits in two launches: coarse = 1 searches every MERGE_SPLIT_COARSE-th
-// piece of a pair over the whole diagonal; coarse = 0 searches the other
-// pieces between the two coarse splits around them. The merge path is a
-// monotone staircase, so for a diagonal d between coarse diagonals D0 < D1
-// with splits i0, i1: i0 <= i(d) <= i1 and d - D1 + i1 <= i(d) <= d - D0 + i0,
-// a window of at most MERGE_SPLIT_COARSE * piece positions.
+// Splits in two launches: k_merge_split_coarse searches every
+// MERGE_SPLIT_COARSE-th piece of a pair over the whole diagonal;
+// k_merge_split searches the other pieces between the two coarse splits
+// around them. The merge path is a monotone staircase, so for a diagonal d
+// between coarse diagonals D0 < D1 with splits i0, i1: i0 <= i(d) <= i1 and
+// d - D1 + i1 <= i(d) <= d - D0 + i0, a window of at most
+// MERGE_SPLIT_COARSE * piece positions. A split is the number of left-run
+// strings among the first d outputs: the first i with A[i] > B[d - i - 1]
+// (ties go to the left run).
 constexpr uint32_t MERGE_SPLIT_COARSE = 32;
+
+// One warp per coarse split (cfirst[p]: the pair's first coarse split; a
+// pair of P pieces has ceil(P / MERGE_SPLIT_COARSE)): each step probes 32
+// positions of the window at once, one per lane, and keeps the 33rd part
+// between the last probe below the split and the first at or above it, so a
+// diagonal of 2^22 positions takes 5 steps of parallel compares where a
+// binary search takes 22 dependent ones. Blocks of whole warps.
+template <class V>
+__global__ void k_merge_split_coarse(const uint8_t* __restrict__ chars, uint64_t nchars, V view,
+                                     const MergePair* __restrict__ pairs,
+                                     const uint64_t* __restrict__ first,
+                                     const uint64_t* __restrict__ cfirst, uint32_t npair,
+                                     const typename V::T* __restrict__ in, uint64_t* __restrict__ split,
+                                     uint32_t piece)
+{
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t ncoarse = cfirst[npair];
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < ncoarse; w += nwarps) {
+        const uint32_t p = pair_of(cfirst, npair, w);
+        const uint64_t k = (w - cfirst[p]) * MERGE_SPLIT_COARSE;
+        const MergePair pr = pairs[p];
+        const uint64_t na = pr.a1 - pr.a0, nb = pr.b1 - pr.a1;
+        const int64_t d = (int64_t)(k * piece);
+        // the split lies in [lo, hi]; positions >= hi count as above it
+        int64_t lo = d > (int64_t)nb ? d - (int64_t)nb : 0, hi = min(d, (int64_t)na);
+        auto above = [&](int64_t x) {
+            uint32_t l;
+            return compare_from(chars, nchars, view.off(in[pr.a0 + x]), view.off(in[pr.a1 + d - x - 1]), 0,
+                                &l) > 0;
+        };
+        while (hi - lo > 32) {
+            // probes x_i = lo + floor((i + 1) * len / 33), strictly
+            // increasing inside [lo, hi) for len > 32
+            const int64_t len = hi - lo;
+            const int64_t x = lo + ((int64_t)(lane + 1) * len) / 33;
+            const uint32_t m = __ballot_sync(0xFFFFFFFFu, above(x));
+            if (m == 0) {
+                lo = lo + (32 * len) / 33 + 1;
+            } else {
+                const int f = __ffs(m) - 1;
+                const int64_t xf = lo + ((int64_t)(f + 1) * len) / 33;
+                lo = f ? lo + ((int64_t)f * len) / 33 + 1 : lo;
+                hi = xf;
+            }
+        }
+        const int64_t x = lo + lane;
+        const uint32_t m = __ballot_sync(0xFFFFFFFFu, x < hi ? above(x) : true);
+        if (lane == 0) split[first[p] + k] = (uint64_t)(m ? min(lo + (int64_t)(__ffs(m) - 1), hi) : hi);
+    }
+}
 
 template <class V>
 __global__ void k_merge_split(const uint8_t* __restrict__ chars, uint64_t nchars, V view,
                               const MergePair* __restrict__ pairs,
                               const uint64_t* __restrict__ first, uint32_t npair,
                               const typename V::T* __restrict__ in, uint64_t* __restrict__ split,
-                              uint32_t piece, int coarse)
+                              uint32_t piece)
 {
     const uint64_t ntask = first[npair];
     for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ntask;
          t += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t p = pair_of(first, npair, t);
         const uint64_t k = t - first[p];
-        if ((k % MERGE_SPLIT_COARSE == 0) != (coarse != 0)) continue;
+        if (k % MERGE_SPLIT_COARSE == 0) continue;
         const MergePair pr = pairs[p];
         const uint64_t na = pr.a1 - pr.a0, nb = pr.b1 - pr.a1;
         const uint64_t d = k * piece;
-        // left-run strings among the first d outputs: the first i with
-        // A[i] > B[d - i - 1] (ties go to the left run)
         int64_t lo = d > nb ? (int64_t)(d - nb) : 0, hi = (int64_t)min(d, na);
         uint32_t depth = 0;  // chars every compared pair shares
-        if (!coarse) {
-            const uint64_t k0 = k - k % MERGE_SPLIT_COARSE, k1 = k0 + MERGE_SPLIT_COARSE;
-            const uint64_t D0 = k0 * piece, i0 = split[first[p] + k0];
-            const bool last = first[p] + k1 >= first[p + 1];
-            const uint64_t D1 = last ? na + nb : k1 * piece, i1 = last ? na : split[first[p] + k1];
-            lo = max(lo, max((int64_t)i0, (int64_t)d - (int64_t)D1 + (int64_t)i1));
-            hi = min(hi, min((int64_t)i1, (int64_t)(d - D0 + i0)));
-            if (hi - lo > 2) {
-                // the search compares A[x], x in [lo, hi), with B[y], y in
-                // [d - hi, d - lo): a sorted run's extremes share no more
-                // than anything between them, so every such pair shares
-                // min(LCP(A[lo], A[hi - 1]), LCP(A[lo], B[d - hi]),
-                // LCP(B[d - hi], B[d - lo - 1])) chars
-                const uint64_t a_lo = view.off(in[pr.a0 + lo]), a_hi = view.off(in[pr.a0 + hi - 1]);
-                const uint64_t b_lo = view.off(in[pr.a1 + d - hi]), b_hi = view.off(in[pr.a1 + d - lo - 1]);
-                uint32_t l1, l2, l3;
-                compare_from(chars, nchars, a_lo, a_hi, 0, &l1);
-                compare_from(chars, nchars, b_lo, b_hi, 0, &l2);
-                compare_from(chars, nchars, a_lo, b_lo, 0, &l3);
-                depth = min(min(l1, l2), l3);
-            }
+        const uint64_t k0 = k - k % MERGE_SPLIT_COARSE, k1 = k0 + MERGE_SPLIT_COARSE;
+        const uint64_t D0 = k0 * piece, i0 = split[first[p] + k0];
+        const bool last = first[p] + k1 >= first[p + 1];
+        const uint64_t D1 = last ? na + nb : k1 * piece, i1 = last ? na : split[first[p] + k1];
+        lo = max(lo, max((int64_t)i0, (int64_t)d - (int64_t)D1 + (int64_t)i1));
+        hi = min(hi, min((int64_t)i1, (int64_t)(d - D0 + i0)));
+        if (hi - lo > 2) {
+            // the search compares A[x], x in [lo, hi), with B[y], y in
+            // [d - hi, d - lo): a sorted run's extremes share no more than
+            // anything between them, so every such pair shares
+            // min(LCP(A[lo], A[hi - 1]), LCP(A[lo], B[d - hi]),
+            // LCP(B[d - hi], B[d - lo - 1])) chars
+            const uint64_t a_lo = view.off(in[pr.a0 + lo]), a_hi = view.off(in[pr.a0 + hi - 1]);
+            const uint64_t b_lo = view.off(in[pr.a1 + d - hi]), b_hi = view.off(in[pr.a1 + d - lo - 1]);
+            uint32_t l1, l2, l3;
+            compare_from(chars, nchars, a_lo, a_hi, 0, &l1);
+            compare_from(chars, nchars, b_lo, b_hi, 0, &l2);
+            compare_from(chars, nchars, a_lo, b_lo, 0, &l3);
+            depth = min(min(l1, l2), l3);
         }
         while (lo < hi) {
             const int64_t mid = (lo + hi) >> 1;
@@ -311,11 +364,12 @@ __device__ __forceinline__ void stage_chunk(MergeStage<T>& sm, uint32_t r, uint6
 {
     const uint32_t tid = threadIdx.x, sl = (uint32_t)(c & 1);
     const uint64_t q = c * MS_CH;
-    cp_async16(&sm.v[r][sl][tid][0], in + q);
-    if (sizeof(T) == 8) cp_async16(&sm.v[r][sl][tid][2], in + q + 2);
-    cp_async16(&sm.ck[r][sl][tid][0], ck_in + q);
-    cp_async16(&sm.ck[r][sl][tid][2], ck_in + q + 2);
-    cp_async16(&sm.lcp[r][sl][tid][0], lcp_in + q);
+#pragma unroll
+    for (uint32_t k = 0; k < MS_CH; k += 16 / sizeof(T)) cp_async16(&sm.v[r][sl][tid][k], in + q + k);
+#pragma unroll
+    for (uint32_t k = 0; k < MS_CH; k += 2) cp_async16(&sm.ck[r][sl][tid][k], ck_in + q + k);
+#pragma unroll
+    for (uint32_t k = 0; k < MS_CH; k += 4) cp_async16(&sm.lcp[r][sl][tid][k], lcp_in + q + k);
     cp_async_commit();
 }
 
@@ -399,24 +453,27 @@ struct SectorOut {
 // equal strings: B's, as A's comes first) and the heads' LCPs with it, and
 // reads its heads' chars from the arena. lcp_out (may be null) receives the
 // LCP of every output but the pair's first, ck_out (may be null) every
-// output's cache. MS_THREADS threads per block, sizeof(MergeStage<T>) bytes
+// output's cache; with ids_out (the last round) the outputs' string ids go
+// there instead of their entries to out. MS_THREADS threads per block, sizeof(MergeStage<T>) bytes
 // of dynamic shared memory.
 template <class V>
-__global__ void __launch_bounds__(MS_THREADS) k_merge_lcp_seq(const uint8_t* __restrict__ chars, uint64_t nchars, V view,
+__global__ void __launch_bounds__(MS_THREADS)
+    k_merge_lcp_seq(const uint8_t* __restrict__ chars, uint64_t nchars, V view,
                                 const MergePair* __restrict__ pairs,
                                 const uint64_t* __restrict__ first, uint32_t npair,
                                 const uint64_t* __restrict__ split,
                                 const typename V::T* __restrict__ in,
                                 const uint32_t* __restrict__ lcp_in, const uint64_t* __restrict__ ck_in,
                                 typename V::T* __restrict__ out, uint32_t* __restrict__ lcp_out,
-                                uint64_t* __restrict__ ck_out, uint32_t piece)
+                                uint64_t* __restrict__ ck_out, uint32_t* __restrict__ ids_out, uint32_t piece)
 {
     using T = typename V::T;
     extern __shared__ __align__(32) unsigned char merge_smem[];
     MergeStage<T>& sm = *reinterpret_cast<MergeStage<T>*>(merge_smem);
     const uint32_t tid = threadIdx.x;
     const uint64_t ntask = first[npair];
-    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + tid; t < ntask; t += (uint64_t)gridDim.x * blockDim.x) {
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + tid; t < ntask;
+         t += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t p = pair_of(first, npair, t);
         const MergePair pr = pairs[p];
         const uint64_t na = pr.a1 - pr.a0, nb = pr.b1 - pr.a1;
@@ -484,9 +541,10 @@ __global__ void __launch_bounds__(MS_THREADS) k_merge_lcp_seq(const uint8_t* __r
         }
         const uint64_t o0 = pr.a0 + d0, o1 = pr.a0 + d1;
         SectorOut<T> wv;
-        SectorOut<uint32_t> wl;
+        SectorOut<uint32_t> wi, wl;
         SectorOut<uint64_t> wc;
-        wv.init(out, sm.ov[tid], o0);
+        if (ids_out) wi.init(ids_out, reinterpret_cast<uint32_t*>(sm.ov[tid]), o0);
+        else wv.init(out, sm.ov[tid], o0);
         if (lcp_out) wl.init(lcp_out, sm.olcp[tid], d0 == 0 ? o0 + 1 : o0);
         if (ck_out) wc.init(ck_out, sm.ock[tid], o0);
         for (uint64_t o = o0; o < o1; ++o) {
@@ -495,7 +553,8 @@ __global__ void __launch_bounds__(MS_THREADS) k_merge_lcp_seq(const uint8_t* __r
             else if (qb >= qb1) take_a = true;
             else if (ha != hb) take_a = ha > hb;
             else take_a = cached_tie(chars, nchars, oa, ob, ha, ca, hb, cb);
-            wv.put(o, take_a ? va : vb);
+            if (ids_out) wi.put(o, view.id(take_a ? va : vb));
+            else wv.put(o, take_a ? va : vb);
             if (lcp_out && o >= wl.lo) wl.put(o, take_a ? ha : hb);
             if (ck_out) wc.put(o, take_a ? ca : cb);
             if (take_a) {
@@ -518,7 +577,8 @@ __global__ void __launch_bounds__(MS_THREADS) k_merge_lcp_seq(const uint8_t* __r
                 }
             }
         }
-        wv.finish(o1);
+        if (ids_out) wi.finish(o1);
+        else wv.finish(o1);
         if (lcp_out) wl.finish(o1);
         if (ck_out) wc.finish(o1);
         cp_async_wait0();  // nothing of this piece left in flight
@@ -530,12 +590,11 @@ __global__ void __launch_bounds__(MS_THREADS) k_merge_lcp_seq(const uint8_t* __r
 // id's offset must lie inside the arena (else *err). PACK: handles (32-bit
 // id << hbits | arena offset, offsets below 2^hbits <= 2^32) into out; else
 // the ids as they are (out may be null: no copy). With the runs' LCP arrays
-// (lcp not null) their copy and every entry's cache at the depth of its LCP.
+// (lcp not null) their copy into lcp_out.
 template <bool PACK>
-__global__ void k_merge_prep(const uint8_t* __restrict__ chars, uint64_t nchars,
-                             const uint64_t* __restrict__ offs, const uint32_t* __restrict__ ids,
-                             const uint32_t* __restrict__ lcp, uint64_t n, uint32_t hbits, void* out,
-                             uint32_t* __restrict__ lcp_out, uint64_t* __restrict__ ck_out, uint32_t* err)
+__global__ void k_merge_prep(const uint64_t* __restrict__ offs, uint64_t nchars,
+                             const uint32_t* __restrict__ ids, const uint32_t* __restrict__ lcp, uint64_t n,
+                             uint32_t hbits, void* out, uint32_t* __restrict__ lcp_out, uint32_t* err)
 {
     for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n;
          q += (uint64_t)gridDim.x * blockDim.x) {
@@ -545,13 +604,21 @@ __global__ void k_merge_prep(const uint8_t* __restrict__ chars, uint64_t nchars,
         if (bad) atomicOr(err, ERR_OFFSET);
         if (PACK) static_cast<uint64_t*>(out)[q] = ((uint64_t)id << hbits) | (bad ? 0ull : o);
         else if (out) static_cast<uint32_t*>(out)[q] = id;
-        if (lcp) {
-            // a run's first LCP is any value: its cache is not read
-            const uint32_t l = lcp[q];
-            lcp_out[q] = l;
-            ck_out[q] = bad ? 7u : cache_of_key(load_key(chars, nchars, o + l));
-        }
+        if (lcp) lcp_out[q] = lcp[q];
     }
+}
+
+// Every entry's cache at the depth of its LCP (round 0's ck_in; a run's
+// first LCP is any value, its cache is not read). Needed by round 0's piece
+// merge only, so it runs beside round 0's splits.
+template <class V>
+__global__ void k_merge_caches(const uint8_t* __restrict__ chars, uint64_t nchars, V view,
+                               const typename V::T* __restrict__ in, const uint32_t* __restrict__ lcp,
+                               uint64_t n, uint64_t* __restrict__ ck_out)
+{
+    for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n;
+         q += (uint64_t)gridDim.x * blockDim.x)
+        ck_out[q] = cache_of_key(load_key(chars, nchars, view.off(in[q]) + lcp[q]));
 }
 
 // The ids of merged handles.

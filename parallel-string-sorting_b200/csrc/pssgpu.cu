@@ -1651,9 +1651,9 @@ int pssgpu_merge_lcp_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nc
         level.push_back(std::move(b));
     }
     const size_t rounds = level.size() - 1;
-    std::vector<uint64_t> flat;  // per round: pairs, piece starts
-    std::vector<uint64_t> at_pairs, at_first, npairs;
-    uint64_t max_tasks = 0;
+    std::vector<uint64_t> flat;  // per round: pairs, piece starts, coarse-split starts
+    std::vector<uint64_t> at_pairs, at_first, at_cfirst, npairs;
+    uint64_t max_tasks = 0, max_coarse = 0;
     for (size_t i = 0; i < rounds; ++i) {
         const std::vector<uint64_t>& a = level[i];
         const uint32_t K = (uint32_t)a.size() - 1, np = (K + 1) / 2;
@@ -1673,8 +1673,17 @@ int pssgpu_merge_lcp_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nc
             t += (m + c->merge_piece - 1) / c->merge_piece;
         }
         flat.push_back(t);
+        at_cfirst.push_back(flat.size());
+        uint64_t tc = 0;
+        for (uint32_t p = 0; p < np; ++p) {
+            flat.push_back(tc);
+            const uint64_t pieces = flat[at_first.back() + p + 1] - flat[at_first.back() + p];
+            tc += (pieces + MERGE_SPLIT_COARSE - 1) / MERGE_SPLIT_COARSE;
+        }
+        flat.push_back(tc);
         npairs.push_back(np);
         max_tasks = std::max(max_tasks, t);
+        max_coarse = std::max(max_coarse, tc);
     }
     // runs as handles (32-bit id << hbits | offset) when the offsets fit 32
     // bits: made once, then every round reads offsets in order with the
@@ -1703,62 +1712,93 @@ int pssgpu_merge_lcp_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nc
     // merged LCP array and the char caches to the next one (the last round
     // writes d_lcp_out, if any). Its reads are staged in 16-byte copies from
     // the library's own buffers (aligned, padded): k_merge_prep copies the
-    // caller's ids (as handles, or as they are) and LCPs in and makes the
-    // caches; round 0 writes tv[0], tlcp[0] and tck[0].
+    // caller's ids (as handles, or as they are) and LCPs in; round 0 writes
+    // tv[0], tlcp[0] and tck[0].
     const unsigned char* in_v = (const unsigned char*)d_ids;
     const uint32_t* in_lcp = with_lcp ? tlcp[1] : nullptr;
     const uint64_t* in_ck = with_lcp ? tck[1] : nullptr;
     if (packed) {
-        k_merge_prep<true><<<blocks, 256, 0, st>>>(d_chars, nchars, d_offs, d_ids, d_lcp, n, hbits, tv[1],
-                                                   tlcp[1], tck[1], d_err);
+        k_merge_prep<true><<<blocks, 256, 0, st>>>(d_offs, nchars, d_ids, d_lcp, n, hbits, tv[1], tlcp[1],
+                                                   d_err);
         in_v = tv[1];
     } else {
-        k_merge_prep<false><<<blocks, 256, 0, st>>>(d_chars, nchars, d_offs, d_ids, d_lcp, n, hbits,
-                                                    with_lcp ? tv[1] : nullptr, tlcp[1], tck[1], d_err);
+        k_merge_prep<false><<<blocks, 256, 0, st>>>(d_offs, nchars, d_ids, d_lcp, n, hbits,
+                                                    with_lcp ? tv[1] : nullptr, tlcp[1], d_err);
         if (with_lcp) in_v = tv[1];
     }
     const MergeByIds by_ids{d_offs};
-    const MergeByHandles by_h{(1ull << hbits) - 1};
+    const MergeByHandles by_h{(1ull << hbits) - 1, hbits};
+    if (with_lcp) {
+        // round 0's caches on a side stream, beside round 0's splits (which
+        // do not read them); round 0's piece merge waits for them
+        PSS_CUDA(cudaEventRecord(c->fork_ev, st));
+        PSS_CUDA(cudaStreamWaitEvent(c->side[0], c->fork_ev, 0));
+        cudaStream_t s = c->side[0];
+        if (packed)
+            k_merge_caches<MergeByHandles><<<blocks, 256, 0, s>>>(d_chars, nchars, by_h, (const uint64_t*)in_v,
+                                                                  tlcp[1], n, tck[1]);
+        else
+            k_merge_caches<MergeByIds><<<blocks, 256, 0, s>>>(d_chars, nchars, by_ids, (const uint32_t*)in_v,
+                                                              tlcp[1], n, tck[1]);
+        PSS_CUDA(cudaEventRecord(c->join_ev[0], c->side[0]));
+    }
     // the piece merge: MS_THREADS threads and their staging per block
     const uint32_t smem_h = sizeof(MergeStage<uint64_t>), smem_i = sizeof(MergeStage<uint32_t>);
     if (with_lcp) {  // per device: set on every call
-        PSS_CUDA(cudaFuncSetAttribute(packed ? (const void*)k_merge_lcp_seq<MergeByHandles>
-                                             : (const void*)k_merge_lcp_seq<MergeByIds>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(packed ? smem_h : smem_i)));
+        const void* fn = packed ? (const void*)k_merge_lcp_seq<MergeByHandles>
+                                : (const void*)k_merge_lcp_seq<MergeByIds>;
+        PSS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(packed ? smem_h : smem_i)));
     }
     const unsigned ms_blocks =
-        (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((max_tasks + MS_THREADS - 1) / MS_THREADS, 148ull * 8));
+        (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((max_tasks + MS_THREADS - 1) / MS_THREADS, 148 * 8));
+    // coarse splits: one warp each, 8 per block
+    const unsigned cs_blocks =
+        (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((max_coarse + 7) / 8, 148ull * 16));
     for (size_t i = 0; i < rounds; ++i) {
         const bool lastr = i + 1 == rounds;
-        // the last round writes the caller's ids directly unless it merges handles
+        // the last round writes the caller's ids directly unless it merges
+        // handles (then the piece merge writes them through ids_out, or
+        // k_merge_unpack after a merge without LCPs)
         unsigned char* out_v = lastr && !packed ? (unsigned char*)d_ids_out : tv[i & 1];
         uint32_t* out_lcp = lastr ? d_lcp_out : tlcp[i & 1];
         uint64_t* out_ck = lastr || !with_lcp ? nullptr : tck[i & 1];
         const MergePair* pairs = reinterpret_cast<const MergePair*>(d_flat + at_pairs[i]);
         const uint64_t* first = d_flat + at_first[i];
+        const uint64_t* cfirst = d_flat + at_cfirst[i];
         const uint32_t np = (uint32_t)npairs[i];
+        // the last round of handles with LCPs writes the caller's ids itself
+        uint32_t* ids_out = lastr && packed && with_lcp ? d_ids_out : nullptr;
         const uint32_t pc = c->merge_piece;
+        // the piece merge of round 0 reads the caches of the side stream
+        const bool wait_caches = i == 0 && with_lcp;
         if (packed) {
             const uint64_t* in = (const uint64_t*)in_v;
             uint64_t* out = (uint64_t*)out_v;
-            for (int coarse = 1; coarse >= 0; --coarse)
-                k_merge_split<MergeByHandles><<<blocks, 256, 0, st>>>(d_chars, nchars, by_h, pairs, first, np, in,
-                                                                      split, pc, coarse);
+            k_merge_split_coarse<MergeByHandles><<<cs_blocks, 256, 0, st>>>(
+                d_chars, nchars, by_h, pairs, first, cfirst, np, in, split, pc);
+            k_merge_split<MergeByHandles><<<blocks, 256, 0, st>>>(d_chars, nchars, by_h, pairs, first, np, in,
+                                                                  split, pc);
+            if (wait_caches) PSS_CUDA(cudaStreamWaitEvent(st, c->join_ev[0], 0));
             if (with_lcp)
                 k_merge_lcp_seq<MergeByHandles><<<ms_blocks, MS_THREADS, smem_h, st>>>(
-                    d_chars, nchars, by_h, pairs, first, np, split, in, in_lcp, in_ck, out, out_lcp, out_ck, pc);
+                    d_chars, nchars, by_h, pairs, first, np, split, in, in_lcp, in_ck, out, out_lcp, out_ck,
+                    ids_out, pc);
             else
                 k_merge_seq<MergeByHandles><<<blocks, 256, 0, st>>>(d_chars, nchars, by_h, pairs, first, np,
                                                                     split, in, out, pc);
         } else {
             const uint32_t* in = (const uint32_t*)in_v;
             uint32_t* out = (uint32_t*)out_v;
-            for (int coarse = 1; coarse >= 0; --coarse)
-                k_merge_split<MergeByIds><<<blocks, 256, 0, st>>>(d_chars, nchars, by_ids, pairs, first, np, in,
-                                                                  split, pc, coarse);
+            k_merge_split_coarse<MergeByIds><<<cs_blocks, 256, 0, st>>>(
+                d_chars, nchars, by_ids, pairs, first, cfirst, np, in, split, pc);
+            k_merge_split<MergeByIds><<<blocks, 256, 0, st>>>(d_chars, nchars, by_ids, pairs, first, np, in,
+                                                              split, pc);
+            if (wait_caches) PSS_CUDA(cudaStreamWaitEvent(st, c->join_ev[0], 0));
             if (with_lcp)
                 k_merge_lcp_seq<MergeByIds><<<ms_blocks, MS_THREADS, smem_i, st>>>(
-                    d_chars, nchars, by_ids, pairs, first, np, split, in, in_lcp, in_ck, out, out_lcp, out_ck, pc);
+                    d_chars, nchars, by_ids, pairs, first, np, split, in, in_lcp, in_ck, out, out_lcp, out_ck,
+                    ids_out, pc);
             else
                 k_merge_seq<MergeByIds><<<blocks, 256, 0, st>>>(d_chars, nchars, by_ids, pairs, first, np,
                                                                 split, in, out, pc);
@@ -1768,7 +1808,7 @@ int pssgpu_merge_lcp_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nc
         in_lcp = out_lcp;
         in_ck = out_ck;
     }
-    if (packed)
+    if (packed && !with_lcp)
         k_merge_unpack<<<blocks, 256, 0, st>>>((const uint64_t*)in_v, n, hbits, d_ids_out);
     uint32_t err = 0;
     PSS_CUDA(cudaMemcpyAsync(&err, d_err, 4, cudaMemcpyDeviceToHost, st));

@@ -360,16 +360,24 @@ def run_merge(args):
 
     def step():
         ctx.merge_lcp_device(dc, nchars, do, bounds, ids, lcp, out, out_lcp, stream=stream)
-    for _ in range(max(args.warmup, 3)):
-        step()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        step()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / args.steps
+
+    def sort_all():  # the same strings sorted outright, with their LCP array
+        ctx.sort_device(dc, nchars, do, sort_ids, sort_lcp, stream=stream)
+
+    def timed(fn):
+        for _ in range(max(args.warmup, 3)):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps
+    ms = timed(step)
+    sort_ids, sort_lcp = torch.empty_like(ids), torch.zeros_like(lcp)
+    sort_ms = timed(sort_all)
     print(json.dumps({
         "mode": "merge", "metric": "merged char GB/s", "value": nchars / (ms / 1e3) / 1e9,
         "unit": "GB/s", "ms_per_step": ms, "steps": args.steps, "warmup": max(args.warmup, 3),
@@ -377,7 +385,8 @@ def run_merge(args):
         "config": {"workload": f"prefixes-{n}", "strings": n, "chars": nchars,
                    "shards": args.shards, "lcp_output": True,
                    "merge_piece": args.merge_piece or "default"},
-        "strings_per_s": n / (ms / 1e3)}))
+        "strings_per_s": n / (ms / 1e3),
+        "sort_with_lcp_ms": sort_ms, "merge_over_sort": ms / sort_ms}))
     ctx.close()
 
 

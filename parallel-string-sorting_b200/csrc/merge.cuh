@@ -341,6 +341,24 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
     const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem)
+{
+    const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+// MS_CH entries of X (aligned to their size) in 16-byte copies, or one
+// 8-byte copy
+template <class X>
+__device__ __forceinline__ void cp_async_chunk(X* smem, const X* gmem)
+{
+    if constexpr (MS_CH * sizeof(X) >= 16) {
+#pragma unroll
+        for (uint32_t k = 0; k < MS_CH; k += 16 / sizeof(X)) cp_async16(smem + k, gmem + k);
+    } else {
+        static_assert(MS_CH * sizeof(X) == 8, "chunks of 8 or a multiple of 16 bytes");
+        cp_async8(smem, gmem);
+    }
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
@@ -364,12 +382,9 @@ __device__ __forceinline__ void stage_chunk(MergeStage<T>& sm, uint32_t r, uint6
 {
     const uint32_t tid = threadIdx.x, sl = (uint32_t)(c & 1);
     const uint64_t q = c * MS_CH;
-#pragma unroll
-    for (uint32_t k = 0; k < MS_CH; k += 16 / sizeof(T)) cp_async16(&sm.v[r][sl][tid][k], in + q + k);
-#pragma unroll
-    for (uint32_t k = 0; k < MS_CH; k += 2) cp_async16(&sm.ck[r][sl][tid][k], ck_in + q + k);
-#pragma unroll
-    for (uint32_t k = 0; k < MS_CH; k += 4) cp_async16(&sm.lcp[r][sl][tid][k], lcp_in + q + k);
+    cp_async_chunk(&sm.v[r][sl][tid][0], in + q);
+    cp_async_chunk(&sm.ck[r][sl][tid][0], ck_in + q);
+    cp_async_chunk(&sm.lcp[r][sl][tid][0], lcp_in + q);
     cp_async_commit();
 }
 

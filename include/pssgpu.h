@@ -191,7 +191,10 @@ int pssgpu_sort_text_host(pssgpu_ctx* ctx, const uint8_t* text, uint64_t size,
  * id in d_ids must index d_offs (the call cannot check that: it does not
  * know the length of d_offs); an offset outside the arena returns
  * PSSGPU_EINVAL, with d_ids_out / d_lcp_out unspecified. With d_lcp the
- * merge is LCP-aware (compares start at the known common prefix). */
+ * merge is LCP-aware (compares start at the known common prefix, and each
+ * run head carries the next 7 chars from there). The context keeps about
+ * 40 bytes per string of merge scratch (entries, LCPs and char caches, two
+ * of each) between calls. */
 int pssgpu_merge_lcp_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nchars,
                             const uint64_t* d_offs, const uint64_t* runs, uint32_t nruns,
                             const uint32_t* d_ids, const uint32_t* d_lcp,

@@ -388,17 +388,16 @@ __device__ __forceinline__ void stage_chunk(MergeStage<T>& sm, uint32_t r, uint6
     cp_async_commit();
 }
 
-// Run R's head moved to position q (< its end q1): on entering a chunk,
-// wait for it (it was staged one ahead; the other run's chunk in flight is
-// not waited for when it went out later) and stage the next one into the
-// slot just read. mine / other: whether run R's / the other run's chunk is
-// in flight; last_b: whether run B staged the latest group.
+// Run R's head entered chunk c (its end: q1): wait for the chunk (it was
+// staged one ahead; the other run's chunk in flight is not waited for when
+// it went out later) and stage the next one into the slot just read. mine /
+// other: whether run R's / the other run's chunk is in flight; last_b:
+// whether run B staged the latest group.
 template <uint32_t R, class T>
-__device__ __forceinline__ void stage_next(MergeStage<T>& sm, uint64_t q, uint64_t q1, const T* in,
+__device__ __forceinline__ void next_chunk(MergeStage<T>& sm, uint64_t c, uint64_t q1, const T* in,
                                            const uint32_t* lcp_in, const uint64_t* ck_in, bool& mine,
                                            bool& other, bool& last_b)
 {
-    if (q % MS_CH != 0) return;
     const bool other_later = R == 0 ? last_b : !last_b;
     if (other && other_later) {
         cp_async_wait1();
@@ -407,7 +406,6 @@ __device__ __forceinline__ void stage_next(MergeStage<T>& sm, uint64_t q, uint64
         other = false;
     }
     mine = false;
-    const uint64_t c = q / MS_CH;
     if ((c + 1) * MS_CH < q1) {
         stage_chunk(sm, R, c + 1, in, lcp_in, ck_in);
         mine = true;
@@ -418,42 +416,42 @@ __device__ __forceinline__ void stage_next(MergeStage<T>& sm, uint64_t q, uint64
 // An output stream: entries written to base[o] for o in [lo, hi) in order,
 // collected per 32-byte sector in shared memory (buf, E entries of U) and
 // written per sector; a sector the stretch covers only in part is written
-// entry by entry.
+// entry by entry. s: the sector slot of the next entry.
 template <class U>
 struct SectorOut {
     static constexpr uint32_t E = 32 / sizeof(U);
     U* base;
     U* buf;
     uint64_t lo;
-    uint32_t phase;  // sector position of base[0]
+    uint32_t s;
     __device__ __forceinline__ void init(U* b, U* sbuf, uint64_t lo_)
     {
         base = b;
         buf = sbuf;
         lo = lo_;
-        phase = (uint32_t)((reinterpret_cast<uintptr_t>(b) / sizeof(U)) & (E - 1));
+        s = (uint32_t)((reinterpret_cast<uintptr_t>(b + lo_) / sizeof(U)) & (E - 1));
     }
     __device__ __forceinline__ void put(uint64_t o, U x)
     {
-        const uint32_t s = (uint32_t)((o + phase) & (E - 1));
         buf[s] = x;
         if (s == E - 1) {
             if (o + 1 >= lo + E) {
                 store_sector(base + (o + 1 - E), buf);
             } else {
-                for (uint64_t k = lo; k <= o; ++k) base[k] = buf[(uint32_t)((k + phase) & (E - 1))];
+                for (uint64_t k = lo; k <= o; ++k) base[k] = buf[(uint32_t)(k + E - 1 - o)];
             }
+            s = 0;
+        } else {
+            ++s;
         }
     }
-    // the entries of [lo, hi) after the last full sector
+    // the entries of [lo, hi) after the last full sector (slots [0, s))
     __device__ __forceinline__ void finish(uint64_t hi)
     {
-        if (hi <= lo) return;
-        const uint32_t s = (uint32_t)((hi - 1 + phase) & (E - 1));
-        if (s == E - 1) return;  // written by put
-        uint64_t k = hi - 1 - s;  // the last sector's first entry
+        if (s == 0 || hi <= lo) return;
+        uint64_t k = hi - s;
         if (k < lo) k = lo;
-        for (; k < hi; ++k) base[k] = buf[(uint32_t)((k + phase) & (E - 1))];
+        for (; k < hi; ++k) base[k] = buf[(uint32_t)(k + s - hi)];
     }
 };
 
@@ -562,32 +560,56 @@ __global__ void __launch_bounds__(MS_THREADS)
         else wv.init(out, sm.ov[tid], o0);
         if (lcp_out) wl.init(lcp_out, sm.olcp[tid], d0 == 0 ? o0 + 1 : o0);
         if (ck_out) wc.init(ck_out, sm.ock[tid], o0);
-        for (uint64_t o = o0; o < o1; ++o) {
+        // per run: heads left in the piece (the current one included), the
+        // current chunk, its slot and the head's entry in it; the thread's
+        // staging of each run
+        uint32_t na_left = (uint32_t)(qa1 - qa), nb_left = (uint32_t)(qb1 - qb);
+        uint64_t cha = qa / MS_CH, chb = qb / MS_CH;
+        uint32_t sla = (uint32_t)(cha & 1), slb = (uint32_t)(chb & 1);
+        uint32_t ea = (uint32_t)(qa % MS_CH), eb = (uint32_t)(qb % MS_CH);
+        constexpr uint32_t SLOT = MS_THREADS * MS_CH;  // entries from one slot to the next
+        const T* svA = &sm.v[0][0][tid][0];
+        const T* svB = &sm.v[1][0][tid][0];
+        const uint32_t* slA = &sm.lcp[0][0][tid][0];
+        const uint32_t* slB = &sm.lcp[1][0][tid][0];
+        const uint64_t* skA = &sm.ck[0][0][tid][0];
+        const uint64_t* skB = &sm.ck[1][0][tid][0];
+        const uint32_t plen = (uint32_t)(d1 - d0);
+        for (uint32_t k = 0; k < plen; ++k) {
+            const uint64_t o = o0 + k;
             bool take_a;
-            if (qa >= qa1) take_a = false;
-            else if (qb >= qb1) take_a = true;
+            if (!na_left) take_a = false;
+            else if (!nb_left) take_a = true;
             else if (ha != hb) take_a = ha > hb;
             else take_a = cached_tie(chars, nchars, oa, ob, ha, ca, hb, cb);
             if (ids_out) wi.put(o, view.id(take_a ? va : vb));
             else wv.put(o, take_a ? va : vb);
-            if (lcp_out && o >= wl.lo) wl.put(o, take_a ? ha : hb);
+            if (lcp_out && (k | d0)) wl.put(o, take_a ? ha : hb);
             if (ck_out) wc.put(o, take_a ? ca : cb);
             if (take_a) {
-                if (++qa < qa1) {
-                    stage_next<0>(sm, qa, qa1, in, lcp_in, ck_in, pend_a, pend_b, last_b);
-                    const uint32_t sl = (uint32_t)((qa / MS_CH) & 1), e = (uint32_t)(qa % MS_CH);
-                    va = sm.v[0][sl][tid][e];
-                    ha = sm.lcp[0][sl][tid][e];
-                    ca = sm.ck[0][sl][tid][e];
+                if (--na_left) {  // against its predecessor, the last output
+                    if (++ea == MS_CH) {
+                        ea = 0;
+                        sla ^= 1;
+                        next_chunk<0>(sm, ++cha, qa1, in, lcp_in, ck_in, pend_a, pend_b, last_b);
+                    }
+                    const uint32_t at = sla * SLOT + ea;
+                    va = svA[at];
+                    ha = slA[at];
+                    ca = skA[at];
                     oa = view.off(va);
                 }
             } else {
-                if (++qb < qb1) {
-                    stage_next<1>(sm, qb, qb1, in, lcp_in, ck_in, pend_b, pend_a, last_b);
-                    const uint32_t sl = (uint32_t)((qb / MS_CH) & 1), e = (uint32_t)(qb % MS_CH);
-                    vb = sm.v[1][sl][tid][e];
-                    hb = sm.lcp[1][sl][tid][e];
-                    cb = sm.ck[1][sl][tid][e];
+                if (--nb_left) {
+                    if (++eb == MS_CH) {
+                        eb = 0;
+                        slb ^= 1;
+                        next_chunk<1>(sm, ++chb, qb1, in, lcp_in, ck_in, pend_b, pend_a, last_b);
+                    }
+                    const uint32_t at = slb * SLOT + eb;
+                    vb = svB[at];
+                    hb = slB[at];
+                    cb = skB[at];
                     ob = view.off(vb);
                 }
             }

@@ -5,14 +5,19 @@
 // LCP-aware K-way merge of src/parallel/eberle-parallel-lcp-merge*.hpp over
 // src/sequential/bingmann-lcp_losertree.hpp).
 //
-// Here the runs merge pairwise, ceil(log2 K) rounds of two launches: the
-// merge-path split of every piece of MERGE_PIECE outputs, then the merge of
-// each piece by one thread. With the runs' LCP arrays the piece merge is
-// LCP-aware, as the reference's loser tree is
-// (src/sequential/bingmann-lcp_losertree.hpp:61-110, 156-185): each head
-// carries its LCP with the last output, the head with the larger one is the
-// smaller string without reading a char, equal ones compare from that depth
-// only, and every output's LCP falls out of the same step.
+// Here the runs merge pairwise, ceil(log2 K) rounds of three launches: the
+// merge-path splits of every MERGE_SPLIT_COARSE-th piece of MERGE_PIECE
+// outputs (a warp each), those of the other pieces (a thread each, inside
+// the window the coarse ones leave), then the merge of each piece by one
+// thread. With the runs' LCP arrays the piece merge is LCP-aware, as the
+// reference's loser tree is (src/sequential/bingmann-lcp_losertree.hpp:61-110,
+// 156-185): each head carries its LCP with the last output, the head with
+// the larger one is the smaller string without reading a char, equal ones
+// compare from that depth only, and every output's LCP falls out of the same
+// step. Each head also carries the 7 chars that follow its LCP (a wider form
+// of the char cache of the reference's LCP + cache sorts), so most equal
+// LCPs are settled without reading the arena; a thread's runs are staged in
+// shared memory a chunk ahead and its outputs written per 32-byte sector.
 #pragma once
 
 #include "device_common.cuh"

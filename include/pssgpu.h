@@ -99,8 +99,9 @@ int pssgpu_ctx_kernel_stats(pssgpu_ctx* ctx, pssgpu_kernel_stats* out, int max);
  * 0 sends every sort through the multi-launch pass loop.
  * PSSGPU_OPT_WAIT_LIMIT (default 4,194,304): polls of a grid-barrier wait in
  * that kernel before it gives up and the sort returns PSSGPU_ETIMEOUT.
- * PSSGPU_OPT_MERGE_PIECE (default 256, at most 4096): outputs one GPU thread
- * merges in each round of pssgpu_merge_lcp_device.
+ * PSSGPU_OPT_MERGE_PIECE (1..4096; by default chosen per merge, 64..256,
+ * so that the pieces fill whole waves of the GPU's resident merge threads):
+ * outputs one GPU thread merges in each round of pssgpu_merge_lcp_device.
  * PSSGPU_OPT_SUFFIX_DOUBLING (default 1): when the strings of a sort are all
  * suffixes of one text (n == nchars, offs[i] == i, no NUL before the last
  * char: psstest --suffix, src/psstest.cpp:502-518), groups that share 8 or

@@ -133,12 +133,15 @@ __device__ __forceinline__ bool cached_tie(const uint8_t* chars, uint64_t nchars
 
 // Merge-path form of a round. A pair is (a0, a1, b1): left run [a0, a1),
 // right run [a1, b1) (empty for an unpaired last run), merged into [a0, b1).
-// Its output is cut into pieces of `piece` positions (MERGE_PIECE by
-// default); task t of the round is piece t - first[pair] of its pair. k_merge_split finds for every
-// piece how many left-run strings precede it (a binary search along the
-// piece's diagonal), k_merge_lcp_seq (or k_merge_seq without LCP arrays)
-// merges each piece sequentially from there.
+// Its output is cut into pieces of `piece` positions (unless the caller
+// sets it: MERGE_PIECE_MIN..MERGE_PIECE, sized to fill whole waves of the
+// GPU's resident piece-merge threads); task t of the round is piece
+// t - first[pair] of its pair. The splits find for every piece how many
+// left-run strings precede it (a search along the piece's diagonal),
+// k_merge_lcp_seq (or k_merge_seq without LCP arrays) merges each piece
+// sequentially from there.
 constexpr uint32_t MERGE_PIECE = 256;
+constexpr uint32_t MERGE_PIECE_MIN = 64;
 constexpr uint32_t MERGE_PIECE_MAX = 4096;
 
 struct MergePair {

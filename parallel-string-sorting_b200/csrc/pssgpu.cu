@@ -224,8 +224,9 @@ struct Ctx {
     bool single_launch = true;
     // polls of a grid-barrier wait in k_wave before it gives up
     uint32_t wait_limit = 1u << 22;
-    // outputs one thread merges in a round of pssgpu_merge_lcp_device
-    uint32_t merge_piece = MERGE_PIECE;
+    // outputs one thread merges in a round of pssgpu_merge_lcp_device (0:
+    // chosen per merge, merge_piece_for)
+    uint32_t merge_piece = 0;
     // suffix sets finish their deep groups by rank doubling (off: the string
     // passes sort them like any strings)
     bool suffix_doubling = true;
@@ -1607,6 +1608,18 @@ int pssgpu_sort_text_host(pssgpu_ctx* ctx, const uint8_t* text, uint64_t size, i
     return sort_text_host_locked(c, text, size, mode, perm, lcp, cap, n_out);
 }
 
+// Outputs per piece of a merge of n strings when the caller set none: at
+// most MERGE_PIECE, and as few waves of `wave` pieces (the piece-merge
+// threads the GPU holds at once) as that allows, filled evenly, so that no
+// wave runs part-empty; at least MERGE_PIECE_MIN (every piece costs a split).
+static uint32_t merge_piece_for(uint64_t n, uint64_t wave)
+{
+    const uint64_t per_wave = (uint64_t)MERGE_PIECE * wave;
+    const uint64_t waves = std::max<uint64_t>(1, (n + per_wave - 1) / per_wave);
+    const uint64_t p = (n + waves * wave - 1) / (waves * wave);
+    return (uint32_t)std::min<uint64_t>(MERGE_PIECE, std::max<uint64_t>(MERGE_PIECE_MIN, p));
+}
+
 int pssgpu_merge_lcp_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nchars,
                             const uint64_t* d_offs, const uint64_t* runs, uint32_t nruns,
                             const uint32_t* d_ids, const uint32_t* d_lcp, uint32_t* d_ids_out,
@@ -1639,6 +1652,29 @@ int pssgpu_merge_lcp_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nc
         PSS_CUDA(cudaStreamSynchronize(st));
         return PSSGPU_OK;
     }
+    // runs as handles (32-bit id << hbits | offset) when the offsets fit 32
+    // bits: made once, then every round reads offsets in order with the
+    // entries instead of gathering them; else as ids
+    const uint32_t hbits = std::max<uint32_t>(1, bit_length(nchars - 1));
+    const bool packed = hbits <= 32 && !c->indirect_handles;
+    const bool with_lcp = d_lcp != nullptr;
+    // the piece merge: MS_THREADS threads and their staging per block
+    const uint32_t smem_h = sizeof(MergeStage<uint64_t>), smem_i = sizeof(MergeStage<uint32_t>);
+    const void* piece_fn = packed ? (const void*)k_merge_lcp_seq<MergeByHandles>
+                                  : (const void*)k_merge_lcp_seq<MergeByIds>;
+    uint32_t pc = c->merge_piece;
+    if (with_lcp) {  // per device: set on every call
+        PSS_CUDA(cudaFuncSetAttribute(piece_fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(packed ? smem_h : smem_i)));
+        if (!pc) {
+            int sms = 0, per_sm = 0;
+            PSS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+            PSS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, piece_fn, MS_THREADS,
+                                                                   packed ? smem_h : smem_i));
+            pc = merge_piece_for(n, (uint64_t)std::max(sms, 1) * std::max(per_sm, 1) * MS_THREADS);
+        }
+    }
+    if (!pc) pc = MERGE_PIECE;
     // pairs and piece counts of every round, uploaded at once: round i
     // merges the runs of level i into those of level i + 1
     std::vector<std::vector<uint64_t>> level{std::vector<uint64_t>(runs, runs + nruns + 1)};
@@ -1670,7 +1706,7 @@ int pssgpu_merge_lcp_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nc
         for (uint32_t p = 0; p < np; ++p) {
             flat.push_back(t);
             const uint64_t m = flat[at_pairs.back() + 3 * p + 2] - flat[at_pairs.back() + 3 * p];
-            t += (m + c->merge_piece - 1) / c->merge_piece;
+            t += (m + pc - 1) / pc;
         }
         flat.push_back(t);
         at_cfirst.push_back(flat.size());
@@ -1685,16 +1721,10 @@ int pssgpu_merge_lcp_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nc
         max_tasks = std::max(max_tasks, t);
         max_coarse = std::max(max_coarse, tc);
     }
-    // runs as handles (32-bit id << hbits | offset) when the offsets fit 32
-    // bits: made once, then every round reads offsets in order with the
-    // entries instead of gathering them; else as ids
-    const uint32_t hbits = std::max<uint32_t>(1, bit_length(nchars - 1));
-    const bool packed = hbits <= 32 && !c->indirect_handles;
     // padded past the last entry: the piece merge stages whole chunks of
     // MS_CH entries
     const uint64_t b_v = align256(4 * n + 8 * MS_CH), b_h = align256(8 * n + 8 * MS_CH);
     const uint64_t b_runs = align256(8 * flat.size()), b_split = align256(8 * (max_tasks + 1));
-    const bool with_lcp = d_lcp != nullptr;
     const uint64_t b_ck = with_lcp ? b_h : 0;
     if ((rc = ensure_buf(&c->mbuf, &c->mbuf_bytes, 2 * b_h + 2 * b_v + 2 * b_ck + b_runs + b_split + 256)))
         return rc;
@@ -1742,14 +1772,6 @@ int pssgpu_merge_lcp_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nc
                                                               tlcp[1], n, tck[1]);
         PSS_CUDA(cudaEventRecord(c->join_ev[0], c->side[0]));
     }
-    // the piece merge: MS_THREADS threads and their staging per block
-    const uint32_t smem_h = sizeof(MergeStage<uint64_t>), smem_i = sizeof(MergeStage<uint32_t>);
-    if (with_lcp) {  // per device: set on every call
-        const void* fn = packed ? (const void*)k_merge_lcp_seq<MergeByHandles>
-                                : (const void*)k_merge_lcp_seq<MergeByIds>;
-        PSS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)(packed ? smem_h : smem_i)));
-    }
     const unsigned ms_blocks =
         (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((max_tasks + MS_THREADS - 1) / MS_THREADS, 148 * 8));
     // coarse splits: one warp each, 8 per block
@@ -1769,7 +1791,6 @@ int pssgpu_merge_lcp_device(pssgpu_ctx* ctx, const uint8_t* d_chars, uint64_t nc
         const uint32_t np = (uint32_t)npairs[i];
         // the last round of handles with LCPs writes the caller's ids itself
         uint32_t* ids_out = lastr && packed && with_lcp ? d_ids_out : nullptr;
-        const uint32_t pc = c->merge_piece;
         // the piece merge of round 0 reads the caches of the side stream
         const bool wait_caches = i == 0 && with_lcp;
         if (packed) {
